@@ -1,0 +1,135 @@
+/*
+ * b200tau: B200-native (sm_100a) multiple-scattering tau00 solve for LSMS.
+ *
+ * C ABI of the drop-in for LSMS's per-atom, per-energy solve
+ *   M = 1 - t G0 over the local interaction zone (LIZ),
+ *   tau00 = [M^-1]_00 t_0  (central kkrsz_ns x kkrsz_ns block),
+ * returned as the reference returns it in tau00_l: (tau00 - t_0), rotated into
+ * the local spin frame when n_spin_cant == 2.
+ *
+ * Reference interfaces replaced (paths inside mstsuite/lsms):
+ *   calculateTauMatrix      src/MultipleScattering/calculateTauMatrix.cpp:320-837
+ *   calculateAllTauMatrices src/MultipleScattering/calculateTauMatrix.cpp:841-945
+ *   buildKKRMatrix*         src/MultipleScattering/buildKKRMatrix_CPU.cpp:621-646,
+ *                           src/MultipleScattering/buildKKRMatrix_CUDA.cu:958-991
+ *   solveTau00*             src/MultipleScattering/linearSolvers_CPU.cpp:76-331,
+ *                           src/MultipleScattering/linearSolvers_CUDA.cu:182-469
+ *   DeviceStorage / DeviceAtom uploads
+ *                           src/Accelerator/DeviceStorage.cu:284-303,341-404
+ *
+ * Conventions
+ *   - Complex numbers are interleaved (re, im) doubles, layout-compatible with
+ *     std::complex<double>.  Matrices are column-major like Matrix<Complex>.
+ *   - Every function returns B200TAU_OK (0) or an error code; the message of
+ *     the last failure of a context is b200tau_last_error(ctx).  Nothing calls
+ *     exit() or abort().
+ *   - Host pointers passed in are read during the call only; nothing retains
+ *     them after it returns.
+ *   - One context per host thread (a context owns one CUDA stream); calls on
+ *     one context are serialised by the caller.
+ */
+#ifndef B200TAU_H
+#define B200TAU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define B200TAU_OK 0
+#define B200TAU_ERR_ARG 1       /* bad argument (size, index, NULL pointer) */
+#define B200TAU_ERR_CUDA 2      /* CUDA runtime error */
+#define B200TAU_ERR_OOM 3       /* device allocation failed */
+#define B200TAU_ERR_SINGULAR 4  /* zero pivot in a diagonal block or in 1 - Delta */
+#define B200TAU_ERR_TIMEOUT 5   /* a device-side wait exceeded its bound */
+#define B200TAU_ERR_STATE 6     /* call order (e.g. solve before upload) */
+
+#define B200TAU_PREC_FP64 0  /* all arithmetic in FP64 */
+#define B200TAU_PREC_MIXED 1 /* FP32/TF32 trailing updates + FP64 refinement */
+
+typedef struct b200tau_ctx b200tau_ctx;
+
+/* One solve: what calculateTauMatrix receives besides the shared state
+ * (calculateTauMatrix.cpp:320-323: localAtomIndex, ispin, energy, prel, iie). */
+typedef struct b200tau_job {
+  int atom;         /* index previously given to b200tau_set_atom */
+  int iie;          /* energy index inside the uploaded tmatStore group */
+  int ispin;        /* spin channel (collinear spin-polarised: 0 or 1) */
+  int reserved;     /* must be 0 */
+  double energy[2]; /* complex energy, Ry */
+  double prel[2];   /* sqrt(E (1 + E c2inv)), calculateTauMatrix.cpp:846 */
+} b200tau_job;
+
+/* Create a context on CUDA device `device` for maxlmax `lmax` (<= 3 supported
+ * in this build), n_spin_cant in {1,2}, n_spin_pola in {1,2}
+ * (LSMSSystemParameters fields, SystemParameters.hpp:126,76-77).  Builds the
+ * Gaunt / i^l / Legendre tables (Coeficients.hpp:21-107) on the device. */
+int b200tau_create(b200tau_ctx **ctx, int device, int lmax, int n_spin_cant,
+                   int n_spin_pola);
+void b200tau_destroy(b200tau_ctx *ctx);
+const char *b200tau_last_error(const b200tau_ctx *ctx);
+
+/* The context's CUDA stream (cudaStream_t) for callers that order their own
+ * work against device-resident solves. */
+void *b200tau_stream(b200tau_ctx *ctx);
+
+/* Upload LocalTypeInfo::tmatStore (SystemParameters.hpp:260-262): column-major
+ * (ld x nstore) complex, ld = blk_size * group_size, blk_size =
+ * (2 (lmax+1)^2)^2 (buildLIZandCommLists.cpp:552-555).  Replaces
+ * DeviceStorage::copyTmatStoreToDevice (DeviceStorage.cu:284-303). */
+int b200tau_upload_tmat(b200tau_ctx *ctx, const double *tmat_store, long ld,
+                        int nstore, int blk_size);
+
+/* Register atom `atom`'s LIZ (AtomData fields, AtomData.hpp:440-445,466):
+ * liz_pos 3 x num_liz column-major (LIZPos), liz_lmax and liz_store_idx
+ * (LIZlmax, LIZStoreIdx), and the spin frame ubr/ubrd (4 complex each, may
+ * be NULL when n_spin_cant == 1).  Replaces DeviceAtom::copyFromAtom
+ * (DeviceStorage.cu:341-404). */
+int b200tau_set_atom(b200tau_ctx *ctx, int atom, int num_liz,
+                     const double *liz_pos, const int *liz_lmax,
+                     const int *liz_store_idx, const double *ubr,
+                     const double *ubrd);
+
+/* Solve `njobs` (atom, energy, spin) problems in one batched device pass and
+ * write each job's tau00_l (kkrsz_ns^2 complex, the layout calculateTauMatrix
+ * writes through its tau00_l argument) to host memory at
+ * tau00_l + 2 * kkrsz_ns^2 * j.  `prec` is B200TAU_PREC_*. */
+int b200tau_solve(b200tau_ctx *ctx, const b200tau_job *jobs, int njobs,
+                  int prec, double *tau00_l);
+
+/* As b200tau_solve, but tau00_l_dev is device memory and the call returns
+ * once the work is enqueued on the context's stream (inputs already resident
+ * from upload_tmat / set_atom).  Errors detected on the device are reported by
+ * the next b200tau_sync. */
+int b200tau_solve_device(b200tau_ctx *ctx, const b200tau_job *jobs, int njobs,
+                         int prec, double *tau00_l_dev);
+int b200tau_sync(b200tau_ctx *ctx);
+
+/* Solver-only entry, the contract of solveTau00zblocklu_cpp / solveTau00zgesv
+ * (linearSolvers_CPU.cpp:76-96,261-331): given a host KKR matrix m (n x n,
+ * column-major, leading dimension ldm, central site first) and the central
+ * t-matrix t0 (b x b), write tau00 = [m^-1 [t0; 0]]_00 (b x b, NOT minus t0,
+ * unrotated) to host memory. */
+int b200tau_solve_dense(b200tau_ctx *ctx, const double *m, int n, int ldm,
+                        const double *t0, int b, int prec, double *tau00);
+
+/* Build only: the KKR matrix M = 1 - t G for one job in the reference's site
+ * order (central site first), written to host memory (n x n, ld = n) where
+ * n = n_spin_cant * nrmat.  Parity hook for buildKKRMatrix*; not on the hot
+ * path.  Returns B200TAU_ERR_ARG if m_out's n does not match. */
+int b200tau_build_kkr(b200tau_ctx *ctx, const b200tau_job *job, double *m_out,
+                      int n);
+
+/* The Gaunt numbers this library builds its G0 tables from (host-only, no GPU needed):
+ * cgnt[l3/2 + (lmax+1) * (j1 + kk * j2)], kk = (lmax+1)^2, the layout of the reference's
+ * GauntCoeficients::cgnt (Coeficients.hpp:37-92, cgaunt_c.f90:31).  cgnt must hold
+ * (lmax+1) * kk * kk doubles; entries outside the l3 range are 0. */
+int b200tau_gaunt_numbers(int lmax, double *cgnt);
+
+/* Number of kernel launches the last solve issued (for launch accounting). */
+long b200tau_last_launch_count(const b200tau_ctx *ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* B200TAU_H */

@@ -1,0 +1,286 @@
+// KKR matrix build M = 1 - t G0 on the device (FP64).
+//
+// Restates, for one (atom, energy, spin) job per grid row:
+//   buildBGijCPU            src/MultipleScattering/buildKKRMatrix_CPU.cpp:96-176
+//     (Hankel :23-40, sin/cos powers :42-59, D_lm :127-140, Gaunt sum :148-176),
+//   setBGijCPU / setgij     buildKKRMatrix_CPU.cpp:61-94, setgij.f:29-38 (spin-diagonal G),
+//   M_ij = -t_i G_ij        buildKKRMatrix_CPU.cpp:388-412, calculateTauMatrix.cpp:156-183,240-242
+//                           (t gathered with the F77 build's per-site lmax semantics).
+// The reference's CUDA build (buildGijCudaKernel, buildKKRMatrix_CUDA.cu:215-381) runs one CTA
+// per site pair with a serial thread-0 prologue and global read-modify-writes of a second N x N
+// matrix.  Here one CTA owns one block column of M (one LIZ site j) for one job: the angular
+// gather tables arrive in shared memory by one bulk-async (TMA) copy, each warp builds whole
+// -t_i G_ij blocks for a row site i with G held in shared memory, and every store writes
+// contiguous 256-byte column segments of M.  No N x N scratch is written besides M itself.
+//
+// Site order in M: LIZ sites 1..L-1 then the central site 0 (JobDev::perm), so the
+// elimination leaves 1 - Delta in the trailing block.
+
+#include <cuda_runtime.h>
+
+#include "common.cuh"
+
+namespace b200 {
+namespace {
+
+constexpr int kWarps = 8;
+constexpr int kThreads = kWarps * 32;
+
+struct BuildSmem {
+  AngularTables tab;
+  double2 D[kWarps][kNdlj];
+  double2 G[kWarps][kMaxKK * kMaxKK];
+  double2 H[kWarps][kMaxLend + 2];
+  double P[kWarps][kNdlm + 4];
+  double C[kWarps][kMaxLend + 2];
+  double S[kWarps][kMaxLend + 2];
+  unsigned long long bar;
+};
+
+__device__ __forceinline__ unsigned smem_u32(const void *p) {
+  return static_cast<unsigned>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
+  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ double2 cfma(double2 a, double2 b, double2 c) {  // c + a*b
+  c.x = fma(a.x, b.x, c.x);
+  c.x = fma(-a.y, b.y, c.x);
+  c.y = fma(a.x, b.y, c.y);
+  c.y = fma(a.y, b.x, c.y);
+  return c;
+}
+__device__ __forceinline__ double2 cdiv(double2 a, double2 b) {
+  const double d = b.x * b.x + b.y * b.y;
+  return make_double2((a.x * b.x + a.y * b.y) / d, (a.y * b.x - a.x * b.y) / d);
+}
+
+// Stage the angular tables with one bulk copy (cp.async.bulk, completion on an mbarrier).
+// The wait is bounded; on expiry the CTA records an error and keeps waiting (bounded again)
+// so that it never exits with a copy into its shared memory still in flight.
+__device__ bool stage_tables(BuildSmem &sm, const AngularTables *src, int *err) {
+  const unsigned bar = smem_u32(&sm.bar);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar),
+                 "r"((unsigned)sizeof(AngularTables))
+                 : "memory");
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(smem_u32(&sm.tab)),
+        "l"(src), "r"((unsigned)sizeof(AngularTables)), "r"(bar)
+        : "memory");
+  }
+  __syncthreads();
+  bool ok = false;
+  for (long it = 0; it < (1L << 24); ++it) {
+    unsigned done;
+    asm volatile(
+        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
+        : "=r"(done)
+        : "r"(bar)
+        : "memory");
+    if (done) {
+      ok = true;
+      break;
+    }
+  }
+  if (!ok) {
+    if (threadIdx.x == 0) atomicExch(err, 1);
+    for (long it = 0; it < (1L << 26); ++it) {
+      unsigned done;
+      asm volatile(
+          "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
+          : "=r"(done)
+          : "r"(bar)
+          : "memory");
+      if (done) break;
+    }
+  }
+  return ok;
+}
+
+__global__ void __launch_bounds__(kThreads)
+    kkr_build_kernel(const JobDev *__restrict__ jobs, BuildParams p, int *err) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  BuildSmem &sm = *reinterpret_cast<BuildSmem *>(smem_raw);
+  const JobDev &J = jobs[blockIdx.y];
+  const int pc = blockIdx.x;
+  if (pc >= J.L) return;
+  if (!stage_tables(sm, p.tables, err)) return;
+  const AngularTables &T = sm.tab;
+
+  const int warp = threadIdx.x >> 5;
+  const int lane = threadIdx.x & 31;
+  const int ns = p.ns;
+  const int kkrsz = p.kkrsz;
+  const int bstore = ns * kkrsz;  // leading dimension of a stored t block
+  const int j = J.perm[pc];
+  const int lj = J.lmax[j];
+  const int kkj = (lj + 1) * (lj + 1);
+  const int col0 = J.off[pc];
+  const int ld = J.ld;
+  double2 *__restrict__ M = J.M;
+  const double2 prel = J.prel;
+  // collinear spin-polarised: spin block offset kkrsz^2 * ispin (buildKKRMatrix_CPU.cpp:402)
+  const long jsm = (p.npola != p.ns) ? (long)kkrsz * kkrsz * J.ispin : 0;
+
+  for (int pr = warp; pr < J.L; pr += kWarps) {
+    const int i = J.perm[pr];
+    const int li = J.lmax[i];
+    const int kki = (li + 1) * (li + 1);
+    const int row0 = J.off[pr];
+    const int nr = ns * kki, nc = ns * kkj;
+    if (pr == pc) {  // diagonal block: identity (buildKKRMatrix_CPU.cpp:266-268)
+      for (int c = 0; c < nc; ++c)
+        for (int r = lane; r < nr; r += 32)
+          M[(size_t)(row0 + r) + (size_t)(col0 + c) * ld] =
+              make_double2(r == c ? 1.0 : 0.0, 0.0);
+      continue;
+    }
+    // rij = pos(ir1) - pos(ir2), ir1 = row site (calculateTauMatrix.cpp:206-208)
+    const double rx = J.pos[3 * i + 0] - J.pos[3 * j + 0];
+    const double ry = J.pos[3 * i + 1] - J.pos[3 * j + 1];
+    const double rz = J.pos[3 * i + 2] - J.pos[3 * j + 2];
+    const double r = sqrt(rx * rx + ry * ry + rz * rz);
+    const int lend = li + lj;
+    if (lane == 0) {
+      // spherical Hankel recursion, hfn_l = -i^(l+1) h_l(kR) e^{ikR}/R (:23-40)
+      double2 *H = sm.H[warp];
+      const double2 z = make_double2(prel.x * r, prel.y * r);
+      const double2 zi = cdiv(make_double2(1.0, 0.0), z);
+      H[0] = make_double2(0.0, -1.0);
+      if (lend >= 1) {
+        const double2 t = cmul(make_double2(0.0, 1.0), zi);
+        H[1] = make_double2(-1.0 - t.x, -t.y);
+      }
+      for (int l = 1; l < lend; ++l) {
+        const double2 a = cmul(H[l], zi);
+        H[l + 1] = make_double2((2.0 * l + 1.0) * a.x - H[l - 1].x, (2.0 * l + 1.0) * a.y - H[l - 1].y);
+      }
+      double s, c;
+      sincos(z.x, &s, &c);
+      const double e = exp(-z.y) / r;
+      const double2 f = make_double2(e * c, e * s);  // e^{iz}/r
+      for (int l = 0; l <= lend; ++l) {
+        double2 h = cmul(H[l], f);
+        h = cmul(h, make_double2(T.ilp1_re[l], T.ilp1_im[l]));
+        H[l] = make_double2(-h.x, -h.y);
+      }
+    } else if (lane == 1) {
+      // normalised P_lm(cos theta) (associatedLegendreFunction.hpp:33-69)
+      double *P = sm.P[warp];
+      const double x = rz / r;
+      const double y = sqrt(1.0 - x * x);
+      P[0] = sqrt(1.0 / (4.0 * 3.14159265358979323846));
+      for (int m = 1; m <= lend; ++m) {
+        const int mm = m * (m + 1) / 2 + m, pm = (m - 1) * m / 2 + (m - 1);
+        P[mm] = -T.plm_mm[m] * y * P[pm];
+        P[mm - 1] = T.plm_m1[m] * x * P[pm];
+      }
+      for (int m = 0; m < lend; ++m)
+        for (int l = m + 2; l <= lend; ++l) {
+          const int k = l * (l + 1) / 2 + m;
+          P[k] = T.plm_a[k] * (x * P[(l - 1) * l / 2 + m] - T.plm_b[k] * P[(l - 2) * (l - 1) / 2 + m]);
+        }
+    } else if (lane == 2) {
+      // cos(m phi), sin(m phi) (:42-59)
+      double *C = sm.C[warp];
+      double *S = sm.S[warp];
+      const double pmag = sqrt(rx * rx + ry * ry);
+      C[0] = 1.0;
+      S[0] = 0.0;
+      double c1 = 0.0, s1 = 0.0;
+      if (pmag > 1.0e-6) {
+        c1 = rx / pmag;
+        s1 = ry / pmag;
+      }
+      if (lend >= 1) {
+        C[1] = c1;
+        S[1] = s1;
+      }
+      for (int m = 2; m <= lend; ++m) {
+        C[m] = C[m - 1] * c1 - S[m - 1] * s1;
+        S[m] = S[m - 1] * c1 + C[m - 1] * s1;
+      }
+    }
+    __syncwarp();
+    // D_{l,m} = hfn_l P_l|m| (cos m phi -/+ i sin m phi), (-1)^m for m < 0 (:127-140)
+    for (int q = lane; q < (lend + 1) * (lend + 1); q += 32) {
+      int l = 0;
+      while ((l + 1) * (l + 1) <= q) ++l;
+      const int m = q - l * (l + 1);
+      const int am = m < 0 ? -m : m;
+      const double pl = sm.P[warp][l * (l + 1) / 2 + am];
+      const double2 h = sm.H[warp][l];
+      double2 f = make_double2(pl * sm.C[warp][am], -pl * sm.S[warp][am]);
+      if (m < 0) {
+        const double sg = (am & 1) ? -1.0 : 1.0;
+        f = make_double2(sg * pl * sm.C[warp][am], sg * pl * sm.S[warp][am]);
+      }
+      sm.D[warp][q] = cmul(h, f);
+    }
+    __syncwarp();
+    // G(lm2, lm1) = pi4 i^(l2-l1) sum_l3 cgnt(l3/2, lm1, lm2) D(l3, m2-m1) (:148-176)
+    for (int e = lane; e < kki * kkj; e += 32) {
+      const int lm2 = e / kkj, lm1 = e - lm2 * kkj;
+      const int te = lm2 * kMaxKK + lm1;
+      double2 acc = make_double2(0.0, 0.0);
+      const int nt = T.nterm[te];
+      for (int q = 0; q < nt; ++q) {
+        const double cg = T.coef[te * kMaxTerms + q];
+        const double2 d = sm.D[warp][T.didx[te * kMaxTerms + q]];
+        acc.x += cg * d.x;
+        acc.y += cg * d.y;
+      }
+      acc.x *= T.pi4;
+      acc.y *= T.pi4;
+      const int rot = T.rot[te];
+      double2 g = acc;
+      if (rot == 1) g = make_double2(-acc.y, acc.x);
+      else if (rot == 2) g = make_double2(-acc.x, -acc.y);
+      else if (rot == 3) g = make_double2(acc.y, -acc.x);
+      sm.G[warp][lm2 * kMaxKK + lm1] = g;
+    }
+    __syncwarp();
+    // M block = -t_i * diag_s(G): rows (s_r, r'), columns (s_c, c') (setgij.f:29-38)
+    const double2 *__restrict__ tb =
+        p.tmat + (long)J.store[i] * p.tmat_ld + (long)J.iie * p.blk + jsm;
+    const int r_lo = lane & 15;
+    const int c_par = lane >> 4;
+    for (int rr = r_lo; rr < nr; rr += 16) {
+      const int trow = (rr / kki) * kkrsz + (rr % kki);
+      for (int sc = 0; sc < ns; ++sc) {
+        double2 trow_v[kMaxKK];
+#pragma unroll
+        for (int k = 0; k < kMaxKK; ++k)
+          trow_v[k] = (k < kki) ? __ldg(tb + trow + (long)(sc * kkrsz + k) * bstore)
+                                : make_double2(0.0, 0.0);
+        for (int cp = c_par; cp < kkj; cp += 2) {
+          double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+          for (int k = 0; k < kMaxKK; ++k)
+            if (k < kki) acc = cfma(trow_v[k], sm.G[warp][k * kMaxKK + cp], acc);
+          M[(size_t)(row0 + rr) + (size_t)(col0 + sc * kkj + cp) * ld] = make_double2(-acc.x, -acc.y);
+        }
+      }
+    }
+    __syncwarp();
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_kkr_build(const JobDev *jobs, int njobs, int max_L, const BuildParams &p,
+                             int *err_flags, cudaStream_t s) {
+  const int smem = (int)sizeof(BuildSmem);
+  cudaError_t e = cudaFuncSetAttribute(kkr_build_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return e;
+  dim3 grid(max_L, njobs);
+  kkr_build_kernel<<<grid, kThreads, smem, s>>>(jobs, p, err_flags);
+  return cudaGetLastError();
+}
+
+}  // namespace b200

@@ -1,0 +1,232 @@
+"""Python host side of b200tau, mirroring the reference's tau00 call surface.
+
+The names follow src/MultipleScattering/calculateTauMatrix.cpp and linearSolvers_CPU.cpp:
+
+* ``TauSolver.calculate_tau_matrix``   <- ``calculateTauMatrix(lsms, local, atom,
+  localAtomIndex, ispin, energy, prel, tau00_l, m, iie)`` (calculateTauMatrix.cpp:320-837)
+* ``TauSolver.calculate_all_tau_matrices`` <- ``calculateAllTauMatrices`` (:841-945), batched over
+  every (atom, energy, spin) of an energy group in one device pass
+* ``TauSolver.solve_tau00_dense``      <- ``solveTau00zblocklu_cpp`` / ``solveTau00zgesv``
+  (linearSolvers_CPU.cpp:76-96,261-331)
+* ``TauSolver.upload_tmat`` / ``set_atom`` <- ``DeviceStorage::copyTmatStoreToDevice`` and
+  ``DeviceAtom::copyFromAtom`` (src/Accelerator/DeviceStorage.cu:284-303,341-404)
+
+Everything goes through the C ABI of ``lsms_b200/_lib/libb200tau.so`` (include/b200tau.h).  There
+is no CPU fallback: if the library or a GPU is missing, construction raises.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+from . import workloads
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libb200tau.so")
+
+OK = 0
+ERR_ARG = 1
+ERR_CUDA = 2
+ERR_OOM = 3
+ERR_SINGULAR = 4
+ERR_TIMEOUT = 5
+ERR_STATE = 6
+PREC_FP64 = 0
+PREC_MIXED = 1
+
+# Symbols declared in include/b200tau.h.
+EXPORTS = (
+    "b200tau_create", "b200tau_destroy", "b200tau_last_error", "b200tau_stream",
+    "b200tau_upload_tmat", "b200tau_set_atom", "b200tau_solve", "b200tau_solve_device",
+    "b200tau_sync", "b200tau_solve_dense", "b200tau_build_kkr", "b200tau_last_launch_count",
+    "b200tau_gaunt_numbers",
+)
+
+
+class B200TauError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"b200tau error {code}: {msg}")
+        self.code = code
+
+
+class Job(ctypes.Structure):
+    """``b200tau_job``: one (atom, energy, spin) solve."""
+    _fields_ = [("atom", ctypes.c_int), ("iie", ctypes.c_int), ("ispin", ctypes.c_int),
+                ("reserved", ctypes.c_int), ("energy", ctypes.c_double * 2),
+                ("prel", ctypes.c_double * 2)]
+
+
+_lib = None
+
+
+def load_library():
+    """Load the CUDA library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError(f"b200tau CUDA library not built: {LIB_PATH} (python -m lsms_b200.build)")
+    lib = ctypes.CDLL(LIB_PATH)
+    P, I, L, D = ctypes.c_void_p, ctypes.c_int, ctypes.c_long, ctypes.c_double
+    lib.b200tau_create.argtypes = [ctypes.POINTER(P), I, I, I, I]
+    lib.b200tau_destroy.argtypes = [P]
+    lib.b200tau_destroy.restype = None
+    lib.b200tau_last_error.argtypes = [P]
+    lib.b200tau_last_error.restype = ctypes.c_char_p
+    lib.b200tau_stream.argtypes = [P]
+    lib.b200tau_stream.restype = P
+    lib.b200tau_upload_tmat.argtypes = [P, P, L, I, I]
+    lib.b200tau_set_atom.argtypes = [P, I, I, P, P, P, P, P]
+    lib.b200tau_solve.argtypes = [P, P, I, I, P]
+    lib.b200tau_solve_device.argtypes = [P, P, I, I, P]
+    lib.b200tau_sync.argtypes = [P]
+    lib.b200tau_solve_dense.argtypes = [P, P, I, I, P, I, I, P]
+    lib.b200tau_build_kkr.argtypes = [P, P, P, I]
+    lib.b200tau_last_launch_count.argtypes = [P]
+    lib.b200tau_last_launch_count.restype = L
+    lib.b200tau_gaunt_numbers.argtypes = [I, P]
+    _lib = lib
+    return lib
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def gaunt_numbers(lmax: int = 3) -> np.ndarray:
+    """The library's Gaunt table as cgnt[l3/2, j1, j2] (host-only call)."""
+    kk = (lmax + 1) ** 2
+    out = np.zeros(((lmax + 1) * kk * kk,), np.float64)
+    rc = load_library().b200tau_gaunt_numbers(lmax, _ptr(out))
+    if rc != OK:
+        raise B200TauError(rc, "b200tau_gaunt_numbers")
+    return out.reshape(kk, kk, lmax + 1).transpose(2, 1, 0).copy()
+
+
+def make_jobs(specs) -> ctypes.Array:
+    """specs: iterable of (atom, iie, ispin, energy) -> b200tau_job array (prel computed as
+    calculateTauMatrix.cpp:846)."""
+    specs = list(specs)
+    arr = (Job * max(len(specs), 1))()
+    for k, (atom, iie, ispin, energy) in enumerate(specs):
+        e = complex(energy)
+        p = workloads.prel_of(e)
+        arr[k].atom, arr[k].iie, arr[k].ispin, arr[k].reserved = int(atom), int(iie), int(ispin), 0
+        arr[k].energy[0], arr[k].energy[1] = e.real, e.imag
+        arr[k].prel[0], arr[k].prel[1] = p.real, p.imag
+    return arr
+
+
+class TauSolver:
+    """A b200tau context on one GPU (LSMSSystemParameters: maxlmax, n_spin_cant, n_spin_pola)."""
+
+    def __init__(self, lmax: int = 3, n_spin_cant: int = 1, n_spin_pola: int = 1, device: int = 0):
+        self.lib = load_library()
+        self.ctx = ctypes.c_void_p()
+        rc = self.lib.b200tau_create(ctypes.byref(self.ctx), device, lmax, n_spin_cant, n_spin_pola)
+        if rc != OK:
+            raise B200TauError(rc, "b200tau_create failed (no CUDA device or bad parameters)")
+        self.lmax, self.n_spin_cant, self.n_spin_pola = lmax, n_spin_cant, n_spin_pola
+        self.kkrsz = (lmax + 1) ** 2
+        self.kkrsz_ns = n_spin_cant * self.kkrsz
+
+    # -- plumbing -------------------------------------------------------------------------
+    def close(self):
+        if self.ctx:
+            self.lib.b200tau_destroy(self.ctx)
+            self.ctx = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int):
+        if rc != OK:
+            raise B200TauError(rc, self.lib.b200tau_last_error(self.ctx).decode())
+
+    @property
+    def stream(self) -> int:
+        return int(self.lib.b200tau_stream(self.ctx) or 0)
+
+    @property
+    def last_launch_count(self) -> int:
+        return int(self.lib.b200tau_last_launch_count(self.ctx))
+
+    # -- uploads (DeviceStorage / DeviceAtom) ----------------------------------------------
+    def upload_tmat(self, tmat_store: np.ndarray):
+        """tmat_store: (nstore, group_size, blk) complex128 == column-major (blk*group, nstore)."""
+        ts = np.ascontiguousarray(tmat_store, np.complex128)
+        nstore, group, blk = ts.shape
+        self._check(self.lib.b200tau_upload_tmat(self.ctx, _ptr(ts), blk * group, nstore, blk))
+
+    def set_atom(self, atom: int, liz_pos: np.ndarray, liz_lmax, liz_store_idx, ubr=None, ubrd=None):
+        pos = np.ascontiguousarray(np.asarray(liz_pos, np.float64).T)  # (L, 3) == column-major 3 x L
+        lm = np.ascontiguousarray(liz_lmax, np.int32)
+        si = np.ascontiguousarray(liz_store_idx, np.int32)
+        u = None if ubr is None else np.ascontiguousarray(ubr, np.complex128)
+        ud = None if ubrd is None else np.ascontiguousarray(ubrd, np.complex128)
+        self._check(self.lib.b200tau_set_atom(self.ctx, atom, pos.shape[0], _ptr(pos), _ptr(lm), _ptr(si),
+                                              None if u is None else _ptr(u),
+                                              None if ud is None else _ptr(ud)))
+
+    def load_problem(self, prob: workloads.Problem, atom: int = 0, upload_tmat: bool = True):
+        if upload_tmat:
+            self.upload_tmat(prob.tmat_store)
+        self.set_atom(atom, prob.liz_pos, prob.liz_lmax, prob.liz_store_idx, prob.ubr, prob.ubrd)
+
+    # -- solves ---------------------------------------------------------------------------
+    def solve_jobs(self, jobs, prec: int = PREC_FP64) -> np.ndarray:
+        """Batched solve; returns (njobs, kkrsz_ns^2) complex tau00_l (column-major blocks)."""
+        n = len(jobs)
+        out = np.zeros((max(n, 1), self.kkrsz_ns * self.kkrsz_ns), np.complex128)
+        self._check(self.lib.b200tau_solve(self.ctx, ctypes.cast(jobs, ctypes.c_void_p), n, prec, _ptr(out)))
+        return out[:n]
+
+    def solve_jobs_device(self, jobs, out_dev_ptr: int, prec: int = PREC_FP64):
+        """Enqueue a batched solve writing to device memory (no host synchronisation)."""
+        self._check(self.lib.b200tau_solve_device(self.ctx, ctypes.cast(jobs, ctypes.c_void_p), len(jobs), prec,
+                                                  ctypes.c_void_p(out_dev_ptr)))
+
+    def sync(self):
+        self._check(self.lib.b200tau_sync(self.ctx))
+
+    def calculate_tau_matrix(self, atom: int, ispin: int, energy: complex, iie: int,
+                             prec: int = PREC_FP64) -> np.ndarray:
+        """tau00_l of one (atom, energy, spin) as calculateTauMatrix writes it (flat, kkrsz_ns^2)."""
+        return self.solve_jobs(make_jobs([(atom, iie, ispin, energy)]), prec)[0]
+
+    def calculate_all_tau_matrices(self, atoms, energies, iies=None, prec: int = PREC_FP64) -> np.ndarray:
+        """tau00_l for every local atom x energy (x spin when collinear-polarised), batched.
+        Returns (n_energies, n_spin, n_atoms, kkrsz_ns^2)."""
+        atoms = list(atoms)
+        energies = np.asarray(energies, np.complex128).reshape(-1)
+        iies = list(range(energies.size)) if iies is None else list(iies)
+        nspin = 2 if (self.n_spin_pola != self.n_spin_cant) else 1
+        specs = [(a, iie, s, e) for iie, e in zip(iies, energies) for s in range(nspin) for a in atoms]
+        out = self.solve_jobs(make_jobs(specs), prec)
+        return out.reshape(energies.size, nspin, len(atoms), -1)
+
+    def solve_tau00_dense(self, m: np.ndarray, t0: np.ndarray, prec: int = PREC_FP64) -> np.ndarray:
+        """tau00 = [m^-1 [t0; 0]]_00 for a KKR matrix m (numpy [row, col], central block first)."""
+        m = np.asarray(m, np.complex128)
+        n = m.shape[0]
+        b = t0.shape[0]
+        mf = np.asfortranarray(m)
+        t0f = np.asfortranarray(np.asarray(t0, np.complex128))
+        out = np.zeros((b, b), np.complex128, order="F")
+        self._check(self.lib.b200tau_solve_dense(self.ctx, mf.ctypes.data_as(ctypes.c_void_p), n, n,
+                                                 t0f.ctypes.data_as(ctypes.c_void_p), b, prec,
+                                                 out.ctypes.data_as(ctypes.c_void_p)))
+        return np.array(out)
+
+    def build_kkr(self, atom: int, iie: int, ispin: int, energy: complex, n: int) -> np.ndarray:
+        """The device-built KKR matrix in the reference's site order (numpy [row, col])."""
+        jobs = make_jobs([(atom, iie, ispin, energy)])
+        out = np.zeros((n * n,), np.complex128)
+        self._check(self.lib.b200tau_build_kkr(self.ctx, ctypes.cast(jobs, ctypes.c_void_p), _ptr(out), n))
+        return out.reshape(n, n).T.copy()
