@@ -1,0 +1,333 @@
+"""Benchmark: tau00 solves/s at N = 2160 (complex), mixed precision vs plain FP64.
+
+Workload (one step): one atom's fcc LIZ of 135 sites (a = 6.82 bohr, lmax 3, N = 2160,
+kkrsz_ns = 16, binary alloy t-matrices from seeded phase shifts) solved at every point of a
+31-point semicircle energy contour (-0.3 .. 0.7 Ry): 31 tau00 solves = build M = 1 - t G0, block
+elimination, refinement, tau00_l.  Each rank (GPU) solves its own atom's contour (independent
+atoms, no data-path collective: weak scaling).  Inputs are synthetic (seeded), see
+lsms_b200/workloads.py.
+
+JSON keys beyond the driver contract:
+  value        mixed-precision solves/s (refined to <= 1e-10 of FP64), all ranks
+  fp64         the plain-FP64 path on the same workload (solves/s), and the mixed/FP64 ratio
+  err_mixed_vs_fp64   max relative tau00 difference between the two paths on this workload
+  roofline     the dominant kernel (trailing update of the block elimination), algorithmic
+               FLOPs / CUDA-event device time, against the peak named in `peak_source`
+  e2e          the same metric through the public API with host buffers (tmatStore and LIZ
+               uploaded from pinned host memory and tau00_l copied back every step)
+  cpu_baseline the reference's own calculateTauMatrix (oracle/_ref) on the host cores
+
+--impl reference times the reference's CPU implementation (oracle/_ref/libtauref.so, build
+0x2000 + solver 0x2005, OpenBLAS on all host threads) on the same workload, one solve per step.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "tau00 solves/s at N=2160 c128: mixed vs plain FP64 at <=1e-10 rel err; %peak"
+N_ENERGIES = 31
+# DRAM bytes (read + write) per tc_update_kernel launch, from the ncu capture summarised in
+# profiles/ (None until captured).
+TRAFFIC_PER_LAUNCH = None
+
+
+def algorithmic_flops(N: int, b: int, L: int) -> float:
+    """F = 8/3 n^3 + 8 n^2 b + 8 n b^2 + 8/3 b^3 + 8 b^3 + 8 b^3 L (L-1), n = N - b."""
+    n = N - b
+    return (8.0 / 3.0 * n ** 3 + 8.0 * n * n * b + 8.0 * n * b * b + 8.0 / 3.0 * b ** 3 + 8.0 * b ** 3
+            + 8.0 * b ** 3 * L * (L - 1))
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.samples = []
+        self._stop = threading.Event()
+        self._proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self._proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self._proc = None
+        return self
+
+    def _read(self):
+        for line in self._proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 7:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self._proc:
+            self._proc.terminate()
+            try:
+                self._proc.wait(timeout=5)
+            except Exception:
+                self._proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return json.load(f), "MEASURED_PEAKS.json"
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0}, "fallback"
+
+
+def run_reference(args, world, rank):
+    """Reference CPU implementation timed on the host cores (rank 0 only)."""
+    if rank != 0:
+        return
+    from lsms_b200 import workloads as W
+    from oracle import reflib
+    if not reflib.available():
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libtauref.so was not built"}))
+        return
+    cores = os.cpu_count() or 1
+    reflib.set_num_threads(cores)
+    prob = W.config_n2160(npts=N_ENERGIES)
+    for i in range(args.warmup):
+        reflib.calculate_tau(prob, i % N_ENERGIES, 0, reflib.ZBLOCKLU_CPP)
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        reflib.calculate_tau(prob, i % N_ENERGIES, 0, reflib.ZBLOCKLU_CPP)
+    dt = (time.perf_counter() - t0) / args.steps
+    value = 1.0 / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+        "config": {"workload": "fcc LIZ 135 sites, lmax 3, N=2160, 31-point contour; one solve per step",
+                   "solver": "reference calculateTauMatrix build 0x2000 + zblocklu_cpp 0x2005"},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "reference",
+                         "sample": f"{args.steps} solves at N=2160 (energies cycled)"},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+
+
+def cpu_baseline(prob, seconds_budget=20.0):
+    from oracle import reflib
+    if not reflib.available():
+        return None
+    cores = os.cpu_count() or 1
+    reflib.set_num_threads(cores)
+    reflib.calculate_tau(prob, 0, 0, reflib.ZBLOCKLU_CPP)  # warm-up
+    n, t0 = 0, time.perf_counter()
+    while n < 3 or (time.perf_counter() - t0 < seconds_budget and n < N_ENERGIES):
+        reflib.calculate_tau(prob, n % N_ENERGIES, 0, reflib.ZBLOCKLU_CPP)
+        n += 1
+        if time.perf_counter() - t0 > seconds_budget:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": n / dt, "unit": "solves/s", "cores": cores, "kind": "reference",
+            "sample": f"{n} of the 31 contour solves at N=2160, one after another, OpenBLAS on {cores} threads"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    world, rank, local = dist_setup()
+
+    if args.impl == "reference":
+        run_reference(args, world, rank)
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    pg = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        pg = dist
+
+    from lsms_b200 import tau as T
+    from lsms_b200 import workloads as W
+
+    # each rank its own atom (seed) -> independent solves
+    prob = W.config_n2160(seed=2 + rank, npts=N_ENERGIES)
+    N, b, L = prob.nrmat_ns, prob.kkrsz_ns, prob.num_liz
+    flops_per_solve = algorithmic_flops(N, b, L)
+    s = T.TauSolver(prob.lmax, prob.n_spin_cant, prob.n_spin_pola, device=local)
+    s.load_problem(prob)
+    jobs = T.make_jobs([(0, i, 0, prob.energies[i]) for i in range(N_ENERGIES)])
+    out = torch.empty(N_ENERGIES * b * b * 2, dtype=torch.float64, device=f"cuda:{local}")
+    stream = torch.cuda.ExternalStream(s.stream, device=f"cuda:{local}")
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if pg is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        return float(t.item())
+
+    def timed(prec, steps, warmup, sampler=None):
+        for _ in range(warmup):
+            s.solve_jobs_device(jobs, out.data_ptr(), prec)
+        s.sync()
+        torch.cuda.synchronize()
+        barrier()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        launches = 0
+        cm = sampler if sampler is not None else _Null()
+        with cm:
+            e0.record(stream)
+            for _ in range(steps):
+                s.solve_jobs_device(jobs, out.data_ptr(), prec)
+                launches += s.last_launch_count
+            e1.record(stream)
+            s.sync()
+        torch.cuda.synchronize()
+        barrier()
+        ms = e0.elapsed_time(e1) / steps
+        return max_over_ranks(ms), launches
+
+    # --- mixed precision (the headline), device-resident inputs -------------------------------
+    sampler = ClockSampler(local)
+    ms_mixed, launches = timed(T.PREC_MIXED, args.steps, args.warmup, sampler)
+    mixed_out = out.clone()
+    # --- plain FP64 on the same workload ---------------------------------------------------------
+    ms_fp64, _ = timed(T.PREC_FP64, max(2, args.steps // 2), 1)
+    fp64_out = out.clone()
+    a = mixed_out.cpu().numpy().view(np.complex128).reshape(N_ENERGIES, -1)
+    f = fp64_out.cpu().numpy().view(np.complex128).reshape(N_ENERGIES, -1)
+    t0l = np.stack([prob.t_block(int(prob.liz_store_idx[0]), i).T.reshape(-1) for i in range(N_ENERGIES)])
+    err = float(max(np.abs(a[i] - f[i]).max() / np.abs(f[i] + t0l[i]).max() for i in range(N_ENERGIES)))
+
+    # --- roofline of the dominant kernel (trailing update), CUDA events on the library stream ---
+    s.set_profiling(True)
+    for _ in range(2):
+        s.solve_jobs_device(jobs, out.data_ptr(), T.PREC_MIXED)
+    s.sync()
+    k_ms, k_launches, k_flops = s.profile_read()
+    s.set_profiling(False)
+    peaks, peak_src = measured_peaks()
+    achieved = k_flops / (k_ms * 1e-3) / 1e12 if k_ms > 0 else None
+    tf32_peak = float(peaks.get("bf16_tflops", 1590.0)) / 2.0
+
+    # --- end to end through the public API with host buffers ------------------------------------
+    tm_host = torch.from_numpy(np.ascontiguousarray(prob.tmat_store).view(np.float64)).pin_memory()
+    tm_np = tm_host.numpy().view(np.complex128).reshape(prob.tmat_store.shape)
+    h2d = tm_np.nbytes + prob.liz_pos.nbytes + prob.liz_lmax.nbytes + prob.liz_store_idx.nbytes
+    d2h = N_ENERGIES * b * b * 16
+    for _ in range(2):
+        s.upload_tmat(tm_np)
+        s.set_atom(0, prob.liz_pos, prob.liz_lmax, prob.liz_store_idx, prob.ubr, prob.ubrd)
+        s.solve_jobs(jobs, T.PREC_MIXED)
+    barrier()
+    e2e_steps = max(2, args.steps // 2)
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        s.upload_tmat(tm_np)
+        s.set_atom(0, prob.liz_pos, prob.liz_lmax, prob.liz_store_idx, prob.ubr, prob.ubrd)
+        s.solve_jobs(jobs, T.PREC_MIXED)
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / e2e_steps)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(prob)
+
+    value = world * N_ENERGIES / (ms_mixed * 1e-3)
+    fp64_value = world * N_ENERGIES / (ms_fp64 * 1e-3)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c64 trailing updates + c128 refinement",
+            "data": "synthetic (seeded phase-shift t-matrices, fcc LIZ)",
+            "config": {"workload": "fcc LIZ 135 sites a=6.82, lmax 3, N=2160, kkrsz_ns 16, "
+                                   "31-point semicircle contour -0.3..0.7 Ry, one atom per GPU",
+                       "solves_per_step": N_ENERGIES, "l2": "inputs larger than L2 "
+                       f"({N_ENERGIES} x {N * N * 16 / 1e6:.0f} MB KKR matrices per step)",
+                       "refinement_steps_mixed": 3, "refinement_steps_fp64": 1},
+            "fp64": {"value": fp64_value, "unit": "solves/s", "ms_per_step": ms_fp64,
+                     "mixed_over_fp64": value / fp64_value},
+            "err_mixed_vs_fp64": err,
+            "flops_per_solve": flops_per_solve,
+            "effective_tflops_mixed": value * flops_per_solve / 1e12,
+            "roofline": {"kernel": "tc_update_kernel + tc_pack_kernel (trailing update A22 -= A21 W, "
+                                   "tcgen05 kind::tf32, 3 hi/lo passes)",
+                         "bound": "tensor",
+                         "achieved": achieved, "unit": "TFLOP/s",
+                         "peak": tf32_peak, "frac": (achieved / tf32_peak) if achieved else None,
+                         "traffic": TRAFFIC_PER_LAUNCH,
+                         "launches_timed": k_launches, "device_ms": k_ms, "algorithmic_flops": k_flops,
+                         "flops_note": "algorithmic complex FLOPs 8 m n kb; the tensor pipe executes 3x "
+                                       "that (hi*hi + hi*lo + lo*hi)",
+                         "peak_source": f"TF32 dense = bf16_tflops / 2 of {peak_src} (measured bf16 "
+                                        f"{peaks.get('bf16_tflops')} TF/s)"},
+            "e2e": {"value": world * N_ENERGIES / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": int(launches),
+            "clocks": sampler.summary(),
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    s.close()
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+
+
+class _Null:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        return False
+
+
+if __name__ == "__main__":
+    main()

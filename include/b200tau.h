@@ -46,6 +46,9 @@ extern "C" {
 #define B200TAU_PREC_FP64 0  /* all arithmetic in FP64 */
 #define B200TAU_PREC_MIXED 1 /* FP32/TF32 trailing updates + FP64 refinement */
 
+#define B200TAU_ENGINE_TENSOR 0 /* mixed path: tcgen05 TF32 hi/lo trailing update (default) */
+#define B200TAU_ENGINE_SIMT 1   /* mixed path: FP32 CUDA-core trailing update (cross-check) */
+
 typedef struct b200tau_ctx b200tau_ctx;
 
 /* One solve: what calculateTauMatrix receives besides the shared state
@@ -89,6 +92,17 @@ int b200tau_set_atom(b200tau_ctx *ctx, int atom, int num_liz,
                      const int *liz_store_idx, const double *ubr,
                      const double *ubrd);
 
+/* Iterative-refinement steps for a precision (0..16).  Each step computes the FP64 residual
+ * R = [0; t0] - M X against the unmodified KKR matrix and applies the correction from the
+ * stored block factors (the refinement of the reference's zcgesv / cusolverDnIRSXgesv
+ * solvers, linearSolvers_CPU.cpp:148-174, linearSolvers_CUDA.cu:424-469, on the N x b
+ * system).  Defaults: FP64 1 step, MIXED 3 steps.  FP64 with 0 steps takes tau00 directly
+ * from the Schur complement like zblock_lu. */
+int b200tau_set_refinement(b200tau_ctx *ctx, int prec, int steps);
+
+/* Engine of the mixed path's trailing update (B200TAU_ENGINE_*). */
+int b200tau_set_mixed_engine(b200tau_ctx *ctx, int engine);
+
 /* Solve `njobs` (atom, energy, spin) problems in one batched device pass and
  * write each job's tau00_l (kkrsz_ns^2 complex, the layout calculateTauMatrix
  * writes through its tau00_l argument) to host memory at
@@ -124,6 +138,14 @@ int b200tau_build_kkr(b200tau_ctx *ctx, const b200tau_job *job, double *m_out,
  * GauntCoeficients::cgnt (Coeficients.hpp:37-92, cgaunt_c.f90:31).  cgnt must hold
  * (lmax+1) * kk * kk doubles; entries outside the l3 range are 0. */
 int b200tau_gaunt_numbers(int lmax, double *cgnt);
+
+/* Kernel-time accounting of the dominant kernel (the trailing-update launches of the block
+ * elimination).  While enabled, each such launch is bracketed by CUDA events on the context
+ * stream; b200tau_profile_read returns the summed device time (ms), the number of timed
+ * launches and their algorithmic FLOPs (8 (N-k-kb)^2 kb per job and step) since enabling.
+ * Enabling resets the totals. */
+int b200tau_set_profiling(b200tau_ctx *ctx, int enable);
+int b200tau_profile_read(b200tau_ctx *ctx, double *ms, long *launches, double *flops);
 
 /* Number of kernel launches the last solve issued (for launch accounting). */
 long b200tau_last_launch_count(const b200tau_ctx *ctx);

@@ -1,4 +1,4 @@
-// Plain-FP64 block elimination for tau00 (batched over jobs).
+// Block elimination and iterative refinement for tau00 (batched over jobs).
 //
 // Restates the reference's block LU contract (zblock_lu_cpp.cpp:19-86, zblock_lu_CPU.f:2-82,
 // block_inverse.cpp:24-47, tau_inv_postproc.f:1-77 / linearSolvers_CPU.cpp:299-330):
@@ -6,13 +6,20 @@
 // The reference eliminates bottom-up with pivoting restricted to each diagonal block (zgetrf on
 // the block, zgetrs on its block row, zgemm on the rest; its CUDA variant
 // zblock_lu_cuda_c.cu:56-353 re-blocks to 55 columns and inverts each diagonal block).
-// Here M is stored with the central site last and eliminated top-down in nb-column steps:
-//   1. diag_inverse_kernel  D = A11^-1 by Gauss-Jordan with partial pivoting inside the block
-//                           (one CTA per job, block in shared memory),
-//   2. zgemm_tile<kOverwrite>  W = D * A12 in place over the block row,
-//   3. zgemm_tile<kSubtract>   A22 -= A21 * W over the trailing matrix (the O(N^3) part).
-// After n = N - b columns the trailing b x b block holds 1 - Delta; finalize_kernel solves
-// (1 - Delta) tau00 = t0 by Gauss-Jordan and writes tau00_l.
+// Here M is stored with the central site last and eliminated top-down in 64-column steps on the
+// factor storage F (FP64 or FP32):
+//   diag_inverse_kernel   D = A11^-1, Gauss-Jordan with partial pivoting inside the block (FP64)
+//   zgemm_tile<kOverwrite> W = D A12 in place over the block row
+//   zgemm_tile<kSubtract>  A22 -= A21 W over the trailing matrix (the O(N^3) part; the mixed path
+//                          replaces this launch by the tensor-core kernel in tc_update.cu)
+// After n = N - b columns the trailing b x b block holds S = 1 - Delta and F holds, in place, the
+// block factors {D_k in the diagonal blocks, A21_k below them, W_k to their right}.
+// Without refinement, finalize solves S tau00 = t0.  With refinement (the reference's zcgesv /
+// cusolverDnIRSXgesv idea, linearSolvers_CPU.cpp:148-174, linearSolvers_CUDA.cu:424-469, applied
+// to the N x b system M X = [0; t0]):
+//   X = F^-1 B;  repeat: R = B - M X (FP64, M unmodified), Y = F^-1 R, X += Y;
+// where F^-1 is a forward sweep (Y_k = D_k R_k, R_below -= A21_k Y_k), the S solve, and a backward
+// sweep (Y_above -= W Y_k), each a kernel per block step over all jobs.  tau00 = X[n:N].
 
 #include <cuda_runtime.h>
 
@@ -25,6 +32,13 @@ __device__ __forceinline__ double2 cmul(double2 a, double2 b) {
   return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
 __device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ double2 cfma(double2 a, double2 b, double2 c) {  // c + a b
+  c.x = fma(a.x, b.x, c.x);
+  c.x = fma(-a.y, b.y, c.x);
+  c.y = fma(a.x, b.y, c.y);
+  c.y = fma(a.y, b.x, c.y);
+  return c;
+}
 __device__ __forceinline__ double cabs1(double2 a) { return fabs(a.x) + fabs(a.y); }
 __device__ __forceinline__ double2 crecip(double2 a) {
   // 1/a with scaling against overflow of |a|^2
@@ -33,13 +47,25 @@ __device__ __forceinline__ double2 crecip(double2 a) {
   const double d = ar * ar + ai * ai;
   return make_double2(ar / (d * s), -ai / (d * s));
 }
+__device__ __forceinline__ double2 ldc(const double2 *p) { return *p; }
+__device__ __forceinline__ double2 ldc(const float2 *p) {
+  const float2 v = *p;
+  return make_double2(v.x, v.y);
+}
+__device__ __forceinline__ void stc(double2 *p, double2 v) { *p = v; }
+__device__ __forceinline__ void stc(float2 *p, double2 v) { *p = make_float2((float)v.x, (float)v.y); }
+
+template <typename S> struct Vec2;
+template <> struct Vec2<double> { using t = double2; };
+template <> struct Vec2<float> { using t = float2; };
 
 // ---------------------------------------------------------------------------------------------
-// 1. In-place Gauss-Jordan inverse of the kb x kb diagonal block at (k, k), kb <= NB.
+// In-place Gauss-Jordan inverse of the kb x kb diagonal block at (k, k) of F, kb <= 64, in FP64.
 // ---------------------------------------------------------------------------------------------
-template <int NB>
+template <typename T>
 __global__ void __launch_bounds__(256) diag_inverse_kernel(const JobDev *__restrict__ jobs, int k,
                                                            int *info) {
+  constexpr int NB = kNb;
   const JobDev &J = jobs[blockIdx.x];
   if (k >= J.n) return;
   const int kb = min(NB, J.n - k);
@@ -48,11 +74,11 @@ __global__ void __launch_bounds__(256) diag_inverse_kernel(const JobDev *__restr
   __shared__ int perm[NB];
   __shared__ int s_piv;
   __shared__ double2 s_dinv;
-  double2 *__restrict__ Mk = J.M + (size_t)k + (size_t)k * J.ld;
+  T *__restrict__ Fk = static_cast<T *>(J.F) + (size_t)k + (size_t)k * J.ld;
   const int tid = threadIdx.x;
   for (int e = tid; e < kb * kb; e += blockDim.x) {
     const int c = e / kb, r = e - c * kb;
-    A[r][c] = Mk[r + (size_t)c * J.ld];
+    A[r][c] = ldc(Fk + r + (size_t)c * J.ld);
   }
   __syncthreads();
   bool singular = false;
@@ -91,16 +117,12 @@ __global__ void __launch_bounds__(256) diag_inverse_kernel(const JobDev *__restr
     __syncthreads();
     if (tid == 0) {
       const double2 d = A[p][p];
-      if (d.x == 0.0 && d.y == 0.0) {
-        s_dinv = make_double2(0.0, 0.0);
-      } else {
-        s_dinv = crecip(d);
-      }
+      s_dinv = (d.x == 0.0 && d.y == 0.0) ? make_double2(0.0, 0.0) : crecip(d);
     }
     __syncthreads();
     const double2 dinv = s_dinv;
     if (dinv.x == 0.0 && dinv.y == 0.0) singular = true;
-    // column-owner mapping: thread handles column c = tid % kb, rows r = tid / kb + q * (256/kb)
+    // column-owner mapping: thread handles column c = tid % NB and rows r0 + q * RS
     const int c = tid % NB;
     const int r0 = tid / NB;
     constexpr int RS = 256 / NB;
@@ -143,81 +165,77 @@ __global__ void __launch_bounds__(256) diag_inverse_kernel(const JobDev *__restr
   }
   for (int e = tid; e < kb * kb; e += blockDim.x) {
     const int c = e / kb, r = e - c * kb;
-    Mk[r + (size_t)c * J.ld] = A[r][c];
+    stc(Fk + r + (size_t)c * J.ld, A[r][c]);
   }
   if (singular && tid == 0) atomicCAS(&info[blockIdx.x], 0, k + 1);
 }
 
 // ---------------------------------------------------------------------------------------------
-// 2./3. Complex FP64 GEMM tile, C (m x n) = A (m x K) * B (K x n)  [kOverwrite, in place over B]
-//                               C (m x n) -= A (m x K) * B (K x n) [kSubtract]
-// 64 x 64 complex tile per CTA, 256 threads, 4 x 4 complex accumulators per thread; operands
-// double-buffered through shared memory in K-chunks of 16.  Thread (tx, ty) owns rows tx + 16 i
-// and columns ty + 16 j so that C / A accesses of consecutive lanes hit consecutive rows of the
-// column-major matrix (256-byte segments).
+// Complex GEMM tile on F (SIMT), C (m x n) = A (m x K) B (K x n)  [kOverwrite, in place over B]
+//                                C (m x n) -= A (m x K) B (K x n) [kSubtract]
+// 64 x 64 complex tile per CTA, 256 threads, 4 x 4 complex accumulators per thread in the storage
+// precision S; operands double-buffered through shared memory in K-chunks of 16.  Thread (tx, ty)
+// owns rows tx + 16 i and columns ty + 16 j so consecutive lanes touch consecutive rows of the
+// column-major matrix.
 // ---------------------------------------------------------------------------------------------
 constexpr int kTile = 64;
 constexpr int kKc = 16;
 enum { kOverwrite = 0, kSubtract = 1 };
 
-template <int MODE>
-__global__ void __launch_bounds__(256) zgemm_tile_kernel(const JobDev *__restrict__ jobs, int k, int nb) {
+template <typename S, int MODE>
+__global__ void __launch_bounds__(256) zgemm_tile_kernel(const JobDev *__restrict__ jobs, int k) {
+  using T = typename Vec2<S>::t;
   const JobDev &J = jobs[blockIdx.z];
   const int N = J.N, ld = J.ld;
   if (k >= J.n) return;
-  const int kb = min(nb, J.n - k);
+  const int kb = min(kNb, J.n - k);
   const int K = kb;
-  int row0, m, col0, n;
-  const double2 *Ab;
-  const double2 *Bb;
-  double2 *Cb;
-  // block row W = D A12 covers columns k+kb .. N-1 and rows k .. k+kb-1
-  col0 = k + kb + blockIdx.x * kTile;
-  n = N - col0;
+  T *__restrict__ F = static_cast<T *>(J.F);
+  int row0, m;
+  const T *Ab;
+  const int col0 = k + kb + blockIdx.x * kTile;
+  int n = N - col0;
   if (n <= 0) return;
   if (MODE == kOverwrite) {
     if (blockIdx.y != 0) return;
     row0 = k;
     m = kb;
-    Ab = J.M + (size_t)k + (size_t)k * ld;  // D (kb x kb)
+    Ab = F + (size_t)k + (size_t)k * ld;  // D (kb x kb)
   } else {
     row0 = k + kb + blockIdx.y * kTile;
     m = N - row0;
     if (m <= 0) return;
-    Ab = J.M + (size_t)row0 + (size_t)k * ld;  // A21
+    Ab = F + (size_t)row0 + (size_t)k * ld;  // A21
   }
-  Bb = J.M + (size_t)k + (size_t)col0 * ld;  // A12 / W
-  Cb = J.M + (size_t)row0 + (size_t)col0 * ld;
+  const T *Bb = F + (size_t)k + (size_t)col0 * ld;  // A12 / W
+  T *Cb = F + (size_t)row0 + (size_t)col0 * ld;
   m = min(m, kTile);
   n = min(n, kTile);
 
-  extern __shared__ __align__(16) double2 dyn_smem[];
-  double2(*As)[kKc][kTile] = reinterpret_cast<double2(*)[kKc][kTile]>(dyn_smem);  // As[buf][kk][row]
-  double2(*Bs)[kKc][kTile] =
-      reinterpret_cast<double2(*)[kKc][kTile]>(dyn_smem + 2 * kKc * kTile);  // Bs[buf][kk][col]
+  extern __shared__ __align__(16) unsigned char zsm[];
+  T(*As)[kKc][kTile] = reinterpret_cast<T(*)[kKc][kTile]>(zsm);  // As[buf][kk][row]
+  T(*Bs)[kKc][kTile] = reinterpret_cast<T(*)[kKc][kTile]>(zsm + 2 * kKc * kTile * sizeof(T));
   const int tid = threadIdx.x;
   const int tx = tid & 15, ty = tid >> 4;
+  const T zero = {S(0), S(0)};
 
-  double2 acc[4][4];
+  T acc[4][4];
 #pragma unroll
   for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = make_double2(0.0, 0.0);
+    for (int j = 0; j < 4; ++j) acc[i][j] = zero;
 
-  // global -> register staging: A chunk kKc x 64 rows (4 per thread), B chunk kKc x 64 cols.
-  double2 ra[4], rb[4];
+  T ra[4], rb[4];
   auto load_chunk = [&](int kc) {
 #pragma unroll
     for (int q = 0; q < 4; ++q) {
-      const int e = tid + q * 256;  // 0..1023
-      // A: row = e % 64, kk = e / 64
+      const int e = tid + q * 256;
       const int ar = e & 63, ak = e >> 6;
       const int kg = kc + ak;
-      ra[q] = (ar < m && kg < K) ? Ab[(size_t)ar + (size_t)kg * ld] : make_double2(0.0, 0.0);
-      // B: kk = e % 16, col = e / 16
+      ra[q] = (ar < m && kg < K) ? Ab[(size_t)ar + (size_t)kg * ld] : zero;
       const int bk = e & 15, bc = e >> 4;
       const int kg2 = kc + bk;
-      rb[q] = (bc < n && kg2 < K) ? Bb[(size_t)kg2 + (size_t)bc * ld] : make_double2(0.0, 0.0);
+      rb[q] = (bc < n && kg2 < K) ? Bb[(size_t)kg2 + (size_t)bc * ld] : zero;
     }
   };
   auto store_chunk = [&](int buf) {
@@ -238,7 +256,7 @@ __global__ void __launch_bounds__(256) zgemm_tile_kernel(const JobDev *__restric
     if (ch + 1 < nchunks) load_chunk((ch + 1) * kKc);
 #pragma unroll
     for (int kk = 0; kk < kKc; ++kk) {
-      double2 a[4], b[4];
+      T a[4], b[4];
 #pragma unroll
       for (int i = 0; i < 4; ++i) a[i] = As[buf][kk][tx + 16 * i];
 #pragma unroll
@@ -256,7 +274,7 @@ __global__ void __launch_bounds__(256) zgemm_tile_kernel(const JobDev *__restric
     if (ch + 1 < nchunks) store_chunk(buf ^ 1);
     __syncthreads();
   }
-  // epilogue (for kOverwrite, every read of B = C happened before the last __syncthreads)
+  // for kOverwrite every read of B = C happened before the last __syncthreads
 #pragma unroll
   for (int j = 0; j < 4; ++j) {
     const int c = ty + 16 * j;
@@ -265,38 +283,23 @@ __global__ void __launch_bounds__(256) zgemm_tile_kernel(const JobDev *__restric
     for (int i = 0; i < 4; ++i) {
       const int r = tx + 16 * i;
       if (r >= m) continue;
-      double2 *dst = Cb + (size_t)r + (size_t)c * ld;
+      T *dst = Cb + (size_t)r + (size_t)c * ld;
       if (MODE == kOverwrite) {
         *dst = acc[i][j];
       } else {
-        const double2 cv = *dst;
-        *dst = make_double2(cv.x - acc[i][j].x, cv.y - acc[i][j].y);
+        const T cv = *dst;
+        *dst = T{cv.x - acc[i][j].x, cv.y - acc[i][j].y};
       }
     }
   }
 }
 
 // ---------------------------------------------------------------------------------------------
-// Finalize: S = trailing b x b block (= 1 - Delta); tau00 = S^-1 t0 by Gauss-Jordan on [S | t0]
-// (tau_inv_postproc.f:36-49); out = tau00 - t0, rotated by trgtol for n_spin_cant = 2
-// (tau00Postprocess.cpp:52-101, trgtol.f:3-110), or raw tau00 (out_mode 1).
+// Small b x b solves by Gauss-Jordan on [A | rhs] in shared memory (FP64, partial pivoting).
+// A is kMaxB x (2 kMaxB + 1); on return columns [b, 2b) hold A^-1 rhs.  Returns singular.
 // ---------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) finalize_kernel(const JobDev *__restrict__ jobs, int ns,
-                                                       int kkrsz, int *info) {
-  const JobDev &J = jobs[blockIdx.x];
-  const int b = J.b;
-  __shared__ double2 A[kMaxB][2 * kMaxB + 1];
-  __shared__ int s_piv;
-  __shared__ double2 s_dinv;
+__device__ bool gj_solve_smem(double2 (*A)[2 * kMaxB + 1], int b, int *s_piv, double2 *s_dinv) {
   const int tid = threadIdx.x;
-  const double2 *S = J.M + (size_t)J.n + (size_t)J.n * J.ld;
-  for (int e = tid; e < b * b; e += blockDim.x) {
-    const int c = e / b, r = e - c * b;
-    A[r][c] = S[r + (size_t)c * J.ld];
-    const double2 t = J.t0[r + (size_t)c * J.t0_ld];
-    A[r][b + c] = t;
-  }
-  __syncthreads();
   bool singular = false;
   for (int p = 0; p < b; ++p) {
     if (tid < 32) {
@@ -317,10 +320,10 @@ __global__ void __launch_bounds__(256) finalize_kernel(const JobDev *__restrict_
           bi = oi;
         }
       }
-      if (tid == 0) s_piv = bi;
+      if (tid == 0) *s_piv = bi;
     }
     __syncthreads();
-    const int pv = s_piv;
+    const int pv = *s_piv;
     if (pv != p)
       for (int c = tid; c < 2 * b; c += blockDim.x) {
         const double2 t = A[p][c];
@@ -330,12 +333,11 @@ __global__ void __launch_bounds__(256) finalize_kernel(const JobDev *__restrict_
     __syncthreads();
     if (tid == 0) {
       const double2 d = A[p][p];
-      s_dinv = (d.x == 0.0 && d.y == 0.0) ? make_double2(0.0, 0.0) : crecip(d);
+      *s_dinv = (d.x == 0.0 && d.y == 0.0) ? make_double2(0.0, 0.0) : crecip(d);
     }
     __syncthreads();
-    const double2 dinv = s_dinv;
+    const double2 dinv = *s_dinv;
     if (dinv.x == 0.0 && dinv.y == 0.0) singular = true;
-    // scale row p, then eliminate column p from every other row
     for (int c = tid; c < 2 * b; c += blockDim.x) A[p][c] = cmul(A[p][c], dinv);
     __syncthreads();
     for (int e = tid; e < b * 2 * b; e += blockDim.x) {
@@ -348,9 +350,13 @@ __global__ void __launch_bounds__(256) finalize_kernel(const JobDev *__restrict_
       if (r != p) A[r][p] = make_double2(0.0, 0.0);
     __syncthreads();
   }
-  if (singular) {
-    if (tid == 0) atomicCAS(&info[blockIdx.x], 0, -1);
-  }
+  return singular;
+}
+
+// out = tau00 (out_mode 1) or rotate(tau00 - t0) (out_mode 0), tau00 in A[r][b + c].
+__device__ void write_out(const JobDev &J, double2 (*A)[2 * kMaxB + 1], int ns, int kkrsz) {
+  const int tid = threadIdx.x;
+  const int b = J.b;
   double2 *out = J.out;
   if (J.out_mode == 1) {
     for (int e = tid; e < b * b; e += blockDim.x) {
@@ -359,7 +365,6 @@ __global__ void __launch_bounds__(256) finalize_kernel(const JobDev *__restrict_
     }
     return;
   }
-  // d = tau00 - t0
   for (int e = tid; e < b * b; e += blockDim.x) {
     const int c = e / b, r = e - c * b;
     A[r][c] = csub(A[r][b + c], J.t0[r + (size_t)c * J.t0_ld]);
@@ -371,7 +376,7 @@ __global__ void __launch_bounds__(256) finalize_kernel(const JobDev *__restrict_
       out[e] = A[r][c];
     }
   } else {
-    // ml(:,:,k) = (u d ud) spin block k, k column-major over the 2x2 spin matrix
+    // trgtol.f:3-110: ml(:,:,k) = (u d ud) spin block k, k column-major over the 2x2 spin matrix
     const int nr = kkrsz;
     for (int e = tid; e < 4 * nr * nr; e += blockDim.x) {
       const int kblk = e / (nr * nr);
@@ -382,8 +387,7 @@ __global__ void __launch_bounds__(256) finalize_kernel(const JobDev *__restrict_
       for (int pp = 0; pp < 2; ++pp)
         for (int qq = 0; qq < 2; ++qq) {
           const double2 f = cmul(J.ubr[ia + 2 * pp], J.ubrd[qq + 2 * jb]);
-          const double2 g = A[pp * nr + r][qq * nr + c];
-          const double2 fg = cmul(f, g);
+          const double2 fg = cmul(f, A[pp * nr + r][qq * nr + c]);
           s.x += fg.x;
           s.y += fg.y;
         }
@@ -392,39 +396,406 @@ __global__ void __launch_bounds__(256) finalize_kernel(const JobDev *__restrict_
   }
 }
 
-}  // namespace
+// tau00 = S^-1 t0 from the Schur block in F (no refinement).
+template <typename T>
+__global__ void __launch_bounds__(256) finalize_direct_kernel(const JobDev *__restrict__ jobs, int ns,
+                                                              int kkrsz, int *info) {
+  const JobDev &J = jobs[blockIdx.x];
+  const int b = J.b;
+  __shared__ double2 A[kMaxB][2 * kMaxB + 1];
+  __shared__ int s_piv;
+  __shared__ double2 s_dinv;
+  const T *Sb = static_cast<const T *>(J.F) + (size_t)J.n + (size_t)J.n * J.ld;
+  for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
+    const int c = e / b, r = e - c * b;
+    A[r][c] = ldc(Sb + r + (size_t)c * J.ld);
+    A[r][b + c] = J.t0[r + (size_t)c * J.t0_ld];
+  }
+  __syncthreads();
+  if (gj_solve_smem(A, b, &s_piv, &s_dinv) && threadIdx.x == 0) atomicCAS(&info[blockIdx.x], 0, -1);
+  write_out(J, A, ns, kkrsz);
+}
 
-cudaError_t launch_lu_fp64(const JobDev *jobs, int njobs, int max_n, int max_N, int nb,
-                           int *info, cudaStream_t s, long *launches) {
-  if (nb != 64) return cudaErrorInvalidValue;
-  const int smem_diag = 64 * 65 * (int)sizeof(double2);
-  const int smem_gemm = 4 * kKc * kTile * (int)sizeof(double2);
+// out from X[n:N] (refined tau00).
+__global__ void __launch_bounds__(256) finalize_from_x_kernel(const JobDev *__restrict__ jobs, int ns,
+                                                              int kkrsz) {
+  const JobDev &J = jobs[blockIdx.x];
+  const int b = J.b;
+  __shared__ double2 A[kMaxB][2 * kMaxB + 1];
+  for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
+    const int c = e / b, r = e - c * b;
+    A[r][b + c] = J.X[(size_t)(J.n + r) + (size_t)c * J.ld];
+  }
+  __syncthreads();
+  write_out(J, A, ns, kkrsz);
+}
+
+// ---------------------------------------------------------------------------------------------
+// Refinement pieces.  X, R, Y are N x b FP64 column-major with leading dimension ld.
+// ---------------------------------------------------------------------------------------------
+
+// R = B - M X with B = [0; t0] (rows n..N-1 hold t0).  64 rows x b columns per CTA, K in chunks.
+__device__ __forceinline__ bool converged(const JobDev &J) {
+  return J.conv != nullptr && *reinterpret_cast<volatile const int *>(J.conv) != 0;
+}
+
+__global__ void __launch_bounds__(256) residual_kernel(const JobDev *__restrict__ jobs) {
+  const JobDev &J = jobs[blockIdx.y];
+  if (converged(J)) return;
+  const int N = J.N, ld = J.ld, b = J.b;
+  const int row0 = blockIdx.x * 64;
+  if (row0 >= N) return;
+  constexpr int KC = 16;
+  __shared__ double2 Ms[KC][65];     // Ms[kk][row]
+  __shared__ double2 Xs[KC][kMaxB];  // Xs[kk][col]
+  const int tid = threadIdx.x;
+  const int tr = tid & 63, tc = tid >> 6;  // row, column group (4 groups)
+  double2 acc[kMaxB / 4];
+#pragma unroll
+  for (int j = 0; j < kMaxB / 4; ++j) acc[j] = make_double2(0.0, 0.0);
+  const double2 *__restrict__ M = J.M;
+  const double2 *__restrict__ X = J.X;
+  for (int kc = 0; kc < N; kc += KC) {
+    for (int e = tid; e < 64 * KC; e += 256) {
+      const int r = e & 63, kk = e >> 6;
+      const int gr = row0 + r, gk = kc + kk;
+      Ms[kk][r] = (gr < N && gk < N) ? M[(size_t)gr + (size_t)gk * ld] : make_double2(0.0, 0.0);
+    }
+    for (int e = tid; e < KC * b; e += 256) {
+      const int kk = e % KC, c = e / KC;
+      const int gk = kc + kk;
+      Xs[kk][c] = (gk < N) ? X[(size_t)gk + (size_t)c * ld] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+#pragma unroll 4
+    for (int kk = 0; kk < KC; ++kk) {
+      const double2 a = Ms[kk][tr];
+#pragma unroll
+      for (int j = 0; j < kMaxB / 4; ++j) {
+        const int c = tc + 4 * j;
+        if (c < b) acc[j] = cfma(a, Xs[kk][c], acc[j]);
+      }
+    }
+    __syncthreads();
+  }
+  const int gr = row0 + tr;
+  if (gr >= N) return;
+#pragma unroll
+  for (int j = 0; j < kMaxB / 4; ++j) {
+    const int c = tc + 4 * j;
+    if (c >= b) continue;
+    const double2 bv = (gr >= J.n) ? J.t0[(gr - J.n) + (size_t)c * J.t0_ld] : make_double2(0.0, 0.0);
+    J.R[(size_t)gr + (size_t)c * ld] = csub(bv, acc[j]);
+  }
+}
+
+// Forward sweep, step k: Y_k = D_k R_k (every CTA computes it; CTA 0 stores it), then
+// R[rows] -= A21_k Y_k for this CTA's 64 rows of [k + kb, N).
+template <typename T>
+__global__ void __launch_bounds__(256) forward_step_kernel(const JobDev *__restrict__ jobs, int k) {
+  const JobDev &J = jobs[blockIdx.y];
+  if (k >= J.n || converged(J)) return;
+  const int kb = min(kNb, J.n - k);
+  const int N = J.N, ld = J.ld, b = J.b;
+  const int row0 = k + kb + blockIdx.x * 64;
+  if (row0 >= N && blockIdx.x != 0) return;
+  const T *__restrict__ F = static_cast<const T *>(J.F);
+  // dynamic smem: Ds[j][r] (D_k, kb x kb, column-major), Rs[j][c] (R_k), Ys[r][c] (Y_k)
+  extern __shared__ __align__(16) unsigned char fsm[];
+  T *Ds = reinterpret_cast<T *>(fsm);
+  double2 *Rs = reinterpret_cast<double2 *>(fsm + sizeof(T) * kNb * kNb);
+  double2(*Ys)[kMaxB] = reinterpret_cast<double2(*)[kMaxB]>(fsm + sizeof(T) * kNb * kNb +
+                                                              sizeof(double2) * kNb * kMaxB);
+  const int tid = threadIdx.x;
+  for (int e = tid; e < kb * kb; e += 256) {
+    const int r = e % kb, j = e / kb;
+    Ds[j * kNb + r] = F[(size_t)(k + r) + (size_t)(k + j) * ld];
+  }
+  for (int e = tid; e < kb * b; e += 256) {
+    const int r = e % kb, c = e / kb;
+    Rs[c * kNb + r] = J.R[(size_t)(k + r) + (size_t)c * ld];
+  }
+  __syncthreads();
+  for (int e = tid; e < kb * b; e += 256) {
+    const int r = e % kb, c = e / kb;
+    double2 s = make_double2(0.0, 0.0);
+#pragma unroll 8
+    for (int j = 0; j < kb; ++j) s = cfma(ldc(&Ds[j * kNb + r]), Rs[c * kNb + j], s);
+    Ys[r][c] = s;
+    if (blockIdx.x == 0) J.Y[(size_t)(k + r) + (size_t)c * ld] = s;
+  }
+  __syncthreads();
+  if (row0 >= N) return;
+  const int tr = tid & 63, tc = tid >> 6;
+  const int gr = row0 + tr;
+  if (gr >= N) return;
+  double2 acc[kMaxB / 4];
+#pragma unroll
+  for (int j = 0; j < kMaxB / 4; ++j) acc[j] = make_double2(0.0, 0.0);
+  const T *lrow = F + (size_t)gr + (size_t)k * ld;
+#pragma unroll 8
+  for (int jj = 0; jj < kb; ++jj) {
+    const double2 a = ldc(lrow + (size_t)jj * ld);
+#pragma unroll
+    for (int j = 0; j < kMaxB / 4; ++j) {
+      const int c = tc + 4 * j;
+      if (c < b) acc[j] = cfma(a, Ys[jj][c], acc[j]);
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < kMaxB / 4; ++j) {
+    const int c = tc + 4 * j;
+    if (c >= b) continue;
+    double2 *dst = J.R + (size_t)gr + (size_t)c * ld;
+    *dst = csub(*dst, acc[j]);
+  }
+}
+
+template <typename T>
+constexpr int forward_smem_bytes() {
+  return (int)(sizeof(T) * kNb * kNb + 2 * sizeof(double2) * kNb * kMaxB);
+}
+
+// Y[n:N] = S^-1 rhs with rhs = R[n:N] (mode 1) or t0 (mode 0, which also zeroes Y[0:n]).
+template <typename T>
+__global__ void __launch_bounds__(256) schur_solve_kernel(const JobDev *__restrict__ jobs, int mode,
+                                                          int *info) {
+  const JobDev &J = jobs[blockIdx.x];
+  if (mode == 1 && converged(J)) return;
+  const int b = J.b, n = J.n, ld = J.ld;
+  __shared__ double2 A[kMaxB][2 * kMaxB + 1];
+  __shared__ int s_piv;
+  __shared__ double2 s_dinv;
+  const T *Sb = static_cast<const T *>(J.F) + (size_t)n + (size_t)n * ld;
+  for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
+    const int c = e / b, r = e - c * b;
+    A[r][c] = ldc(Sb + r + (size_t)c * ld);
+    A[r][b + c] = mode == 0 ? J.t0[r + (size_t)c * J.t0_ld] : J.R[(size_t)(n + r) + (size_t)c * ld];
+  }
+  if (mode == 0)
+    for (int e = threadIdx.x; e < n * b; e += blockDim.x) {
+      const int r = e % n, c = e / n;
+      J.Y[(size_t)r + (size_t)c * ld] = make_double2(0.0, 0.0);
+    }
+  __syncthreads();
+  if (gj_solve_smem(A, b, &s_piv, &s_dinv) && threadIdx.x == 0) atomicCAS(&info[blockIdx.x], 0, -1);
+  for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
+    const int c = e / b, r = e - c * b;
+    J.Y[(size_t)(n + r) + (size_t)c * ld] = A[r][b + c];
+  }
+}
+
+// Backward sweep for the block of rows [k, k + kb): CTA 0 sets X_k = Y_k (mode 0) or X_k += Y_k
+// (mode 1); every CTA applies Y[rows] -= W[rows, k:k+kb] Y_k for its 64 rows of [0, k).
+// `central` selects the trailing b-row block (k = n, kb = b).
+template <typename T>
+__global__ void __launch_bounds__(256) backward_step_kernel(const JobDev *__restrict__ jobs, int k,
+                                                            int central, int mode) {
+  const JobDev &J = jobs[blockIdx.y];
+  if (mode == 1 && converged(J)) return;
+  int kb;
+  if (central) {
+    k = J.n;
+    kb = J.b;
+  } else {
+    if (k >= J.n) return;
+    kb = min(kNb, J.n - k);
+  }
+  const int ld = J.ld, b = J.b;
+  const int row0 = blockIdx.x * 64;
+  if (row0 >= k && blockIdx.x != 0) return;
+  __shared__ double2 Ys[kNb][kMaxB];
+  const int tid = threadIdx.x;
+  for (int e = tid; e < kb * b; e += 256) {
+    const int r = e % kb, c = e / kb;
+    const size_t idx = (size_t)(k + r) + (size_t)c * ld;
+    const double2 y = J.Y[idx];
+    Ys[r][c] = y;
+    if (blockIdx.x == 0) {
+      if (mode == 0) {
+        J.X[idx] = y;
+      } else {
+        const double2 x = J.X[idx];
+        J.X[idx] = make_double2(x.x + y.x, x.y + y.y);
+      }
+    }
+  }
+  __syncthreads();
+  if (row0 >= k) return;
+  const T *__restrict__ F = static_cast<const T *>(J.F);
+  const int tr = tid & 63, tc = tid >> 6;
+  const int gr = row0 + tr;
+  if (gr >= k) return;
+  double2 acc[kMaxB / 4];
+#pragma unroll
+  for (int j = 0; j < kMaxB / 4; ++j) acc[j] = make_double2(0.0, 0.0);
+  const T *urow = F + (size_t)gr + (size_t)k * ld;
+  for (int jj = 0; jj < kb; ++jj) {
+    const double2 a = ldc(urow + (size_t)jj * ld);
+#pragma unroll
+    for (int j = 0; j < kMaxB / 4; ++j) {
+      const int c = tc + 4 * j;
+      if (c < b) acc[j] = cfma(a, Ys[jj][c], acc[j]);
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < kMaxB / 4; ++j) {
+    const int c = tc + 4 * j;
+    if (c >= b) continue;
+    double2 *dst = J.Y + (size_t)gr + (size_t)c * ld;
+    *dst = csub(*dst, acc[j]);
+  }
+}
+
+template <typename T, typename S>
+cudaError_t eliminate_impl(const JobDev *jobs, int njobs, int max_n, int max_N, int *info, cudaStream_t s,
+                           long *launches, KernelTimer *timer, const TcMaps *tc, int *err) {
+  const int smem_diag = kNb * (kNb + 1) * (int)sizeof(double2);
+  const int smem_gemm = 4 * kKc * kTile * (int)sizeof(T);
   cudaError_t e;
-  if ((e = cudaFuncSetAttribute(diag_inverse_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  if ((e = cudaFuncSetAttribute(diag_inverse_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 smem_diag)) != cudaSuccess)
     return e;
-  if ((e = cudaFuncSetAttribute(zgemm_tile_kernel<kOverwrite>,
+  if ((e = cudaFuncSetAttribute(zgemm_tile_kernel<S, kOverwrite>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem_gemm)) != cudaSuccess)
     return e;
-  if ((e = cudaFuncSetAttribute(zgemm_tile_kernel<kSubtract>,
+  if ((e = cudaFuncSetAttribute(zgemm_tile_kernel<S, kSubtract>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem_gemm)) != cudaSuccess)
     return e;
-  for (int k = 0; k < max_n; k += nb) {
-    diag_inverse_kernel<64><<<njobs, 256, smem_diag, s>>>(jobs, k, info);
+  for (int k = 0; k < max_n; k += kNb) {
+    diag_inverse_kernel<T><<<njobs, 256, smem_diag, s>>>(jobs, k, info);
     const int rest = max_N - k - 1;
     const int tiles = (rest + kTile - 1) / kTile;
+    if (launches) *launches += 1;
     if (tiles > 0) {
-      zgemm_tile_kernel<kOverwrite><<<dim3(tiles, 1, njobs), 256, smem_gemm, s>>>(jobs, k, nb);
-      zgemm_tile_kernel<kSubtract><<<dim3(tiles, tiles, njobs), 256, smem_gemm, s>>>(jobs, k, nb);
+      zgemm_tile_kernel<S, kOverwrite><<<dim3(tiles, 1, njobs), 256, smem_gemm, s>>>(jobs, k);
+      const bool timed = timer && timer->used + 2 <= timer->cap;
+      if (timed) cudaEventRecord(timer->ev[timer->used++], s);
+      if (tc != nullptr) {
+        if ((e = launch_tc_step(*tc, jobs, njobs, k, max_N, err, s)) != cudaSuccess) return e;
+        if (launches) *launches += 1;  // pack + update
+      } else {
+        zgemm_tile_kernel<S, kSubtract><<<dim3(tiles, tiles, njobs), 256, smem_gemm, s>>>(jobs, k);
+      }
+      if (timed) cudaEventRecord(timer->ev[timer->used++], s);
+      if (launches) *launches += 2;
     }
-    if (launches) *launches += 3;
   }
   return cudaGetLastError();
 }
 
-cudaError_t launch_finalize(const JobDev *jobs, int njobs, int ns, int kkrsz, int *info,
-                            cudaStream_t s) {
-  finalize_kernel<<<njobs, 256, 0, s>>>(jobs, ns, kkrsz, info);
+template <typename T>
+void sweep_solve(const JobDev *jobs, int njobs, int max_n, int max_N, int mode, int *info, cudaStream_t s,
+                 long *launches) {
+  // forward (skipped for the initial solve: B is zero above the central block)
+  if (mode == 1) {
+    constexpr int fsmem = forward_smem_bytes<T>();
+    cudaFuncSetAttribute(forward_step_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsmem);
+    for (int k = 0; k < max_n; k += kNb) {
+      const int tiles = (max_N - k - 1) / 64 + 1;
+      forward_step_kernel<T><<<dim3(tiles, njobs), 256, fsmem, s>>>(jobs, k);
+      if (launches) *launches += 1;
+    }
+  }
+  schur_solve_kernel<T><<<njobs, 256, 0, s>>>(jobs, mode, info);
+  backward_step_kernel<T><<<dim3((max_n + 63) / 64 + 1, njobs), 256, 0, s>>>(jobs, 0, 1, mode);
+  if (launches) *launches += 2;
+  const int last = ((max_n - 1) / kNb) * kNb;
+  for (int k = last; k >= 0; k -= kNb) {
+    backward_step_kernel<T><<<dim3(k / 64 + 1, njobs), 256, 0, s>>>(jobs, k, 0, mode);
+    if (launches) *launches += 1;
+  }
+}
+
+// After a refinement round: the job is converged when the correction just applied to the tau00
+// block is below tol x max|tau00| (the error left after applying it is smaller still, by the
+// contraction factor of the refinement), and later rounds skip it.
+__global__ void __launch_bounds__(256) converge_check_kernel(const JobDev *__restrict__ jobs, double tol) {
+  const JobDev &J = jobs[blockIdx.x];
+  if (J.conv == nullptr || converged(J)) return;
+  const int b = J.b, n = J.n, ld = J.ld;
+  double my = 0.0, mx = 0.0;
+  for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
+    const int r = e % b, c = e / b;
+    const size_t idx = (size_t)(n + r) + (size_t)c * ld;
+    my = fmax(my, cabs1(J.Y[idx]));
+    mx = fmax(mx, cabs1(J.X[idx]));
+  }
+  __shared__ double sy[256], sx[256];
+  sy[threadIdx.x] = my;
+  sx[threadIdx.x] = mx;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if ((int)threadIdx.x < o) {
+      sy[threadIdx.x] = fmax(sy[threadIdx.x], sy[threadIdx.x + o]);
+      sx[threadIdx.x] = fmax(sx[threadIdx.x], sx[threadIdx.x + o]);
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0 && sy[0] <= tol * sx[0]) *J.conv = 1;
+}
+
+template <typename T>
+__global__ void copy_to_factor_kernel(const double2 *__restrict__ M, T *__restrict__ F, int n, int ld) {
+  const size_t total = (size_t)n * n;
+  for (size_t e = blockIdx.x * (size_t)blockDim.x + threadIdx.x; e < total; e += (size_t)gridDim.x * blockDim.x) {
+    const size_t c = e / n, r = e - c * n;
+    stc(F + r + c * ld, M[r + c * ld]);
+  }
+}
+
+}  // namespace
+
+cudaError_t launch_copy_to_factor(FactorKind fk, const double2 *M, void *F, int n, int ld, cudaStream_t s) {
+  const int blocks = 148 * 8;
+  if (fk == kFactorFP64)
+    copy_to_factor_kernel<double2><<<blocks, 256, 0, s>>>(M, static_cast<double2 *>(F), n, ld);
+  else
+    copy_to_factor_kernel<float2><<<blocks, 256, 0, s>>>(M, static_cast<float2 *>(F), n, ld);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_eliminate(FactorKind fk, const JobDev *jobs, int njobs, int max_n, int max_N, int *info,
+                             cudaStream_t s, long *launches, KernelTimer *timer, const TcMaps *tc,
+                             int *err) {
+  if (fk == kFactorFP64)
+    return eliminate_impl<double2, double>(jobs, njobs, max_n, max_N, info, s, launches, timer, nullptr, err);
+  if (tc) {
+    cudaError_t e = tc_prepare();
+    if (e != cudaSuccess) return e;
+  }
+  return eliminate_impl<float2, float>(jobs, njobs, max_n, max_N, info, s, launches, timer, tc, err);
+}
+
+cudaError_t launch_finalize_direct(FactorKind fk, const JobDev *jobs, int njobs, int ns, int kkrsz, int *info,
+                                   cudaStream_t s, long *launches) {
+  if (fk == kFactorFP64)
+    finalize_direct_kernel<double2><<<njobs, 256, 0, s>>>(jobs, ns, kkrsz, info);
+  else
+    finalize_direct_kernel<float2><<<njobs, 256, 0, s>>>(jobs, ns, kkrsz, info);
+  if (launches) *launches += 1;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_solve_refine(FactorKind fk, const JobDev *jobs, int njobs, int max_n, int max_N, int b,
+                                int steps, int ns, int kkrsz, int *info, cudaStream_t s, long *launches) {
+  (void)b;
+  auto solve = [&](int mode) {
+    if (fk == kFactorFP64) sweep_solve<double2>(jobs, njobs, max_n, max_N, mode, info, s, launches);
+    else sweep_solve<float2>(jobs, njobs, max_n, max_N, mode, info, s, launches);
+  };
+  solve(0);
+  for (int it = 0; it < steps; ++it) {
+    residual_kernel<<<dim3((max_N + 63) / 64, njobs), 256, 0, s>>>(jobs);
+    if (launches) *launches += 1;
+    solve(1);
+    if (it + 1 < steps) {
+      converge_check_kernel<<<njobs, 256, 0, s>>>(jobs, 1e-13);
+      if (launches) *launches += 1;
+    }
+  }
+  finalize_from_x_kernel<<<njobs, 256, 0, s>>>(jobs, ns, kkrsz);
+  if (launches) *launches += 1;
   return cudaGetLastError();
 }
 

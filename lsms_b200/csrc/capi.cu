@@ -3,10 +3,11 @@
 // The context replaces the reference's per-thread DeviceStorage (src/Accelerator/
 // DeviceStorage.hpp:55-144, DeviceStorage.cu:87-225) and DeviceAtom/DeviceConstants
 // (DeviceStorage.cu:341-404): it owns the device tmatStore copy, one device record per atom,
-// the angular tables, a stream, and a workspace of `slots` KKR matrices.  A solve call packs
-// the jobs into waves of at most `slots` jobs (largest N first), and per wave runs
-//   kkr_build -> FP64 block elimination (or the mixed-precision path) -> finalize
-// on the context stream, then copies the tau00_l blocks out.
+// the angular tables, a stream, and a workspace of `slots` jobs (KKR matrix M in FP64, factor
+// storage F in FP64 or FP32, and the N x b solution / residual / correction blocks).  A solve call
+// packs the jobs into waves of at most `slots` jobs (largest N first), and per wave runs
+//   kkr_build -> block elimination of F -> (refinement against M) -> tau00_l
+// on the context stream.
 
 #include <cuda_runtime.h>
 
@@ -39,6 +40,13 @@ struct AtomDev {
   bool valid = false;
 };
 
+// How a precision runs: factor type, refinement steps (0: direct from the Schur block).
+struct Plan {
+  FactorKind fk;
+  int steps;
+  bool f_separate;  // F is a second buffer (M kept for residuals)
+};
+
 }  // namespace
 
 struct b200tau_ctx {
@@ -52,19 +60,34 @@ struct b200tau_ctx {
   int nstore = 0;
   int group_size = 0;
   std::vector<AtomDev> atoms;
-  // workspace
-  double2 *d_work = nullptr;
-  size_t work_elems = 0;   // per slot
+  // workspace (per slot: M ld*ld double2, F ld*ld of the factor type, vec 3*ld*b double2)
+  double2 *d_M = nullptr;
+  unsigned char *d_F = nullptr;
+  double2 *d_vec = nullptr;
+  size_t m_elems = 0, f_bytes = 0, vec_elems = 0;
   int slots = 0;
   JobDev *d_jobs = nullptr;
   int jobs_cap = 0;
   int *d_info = nullptr;   // per slot
+  int *d_conv = nullptr;   // per slot: refinement converged
   int *d_err = nullptr;    // device error flags
   double2 *d_out = nullptr;
   size_t out_cap = 0;
   double2 *d_t0 = nullptr;  // dense-solve t0
   long launches = 0;
   int max_slots = 64;
+  int refine_steps[2] = {1, 3};  // FP64, MIXED
+  // profiling of the trailing-update launches (b200tau_set_profiling)
+  bool profiling = false;
+  std::vector<cudaEvent_t> events;
+  KernelTimer timer;
+  double prof_ms = 0.0, prof_flops = 0.0;
+  long prof_launches = 0;
+  // tensor-core trailing update of the mixed path: operand packs + TMA descriptors
+  int mixed_engine = B200TAU_ENGINE_TENSOR;
+  TcMaps tc;
+  float *d_pack = nullptr;
+  int tc_ld = 0, tc_slots = 0;
 };
 
 namespace {
@@ -100,18 +123,47 @@ void free_atom(AtomDev &a) {
 
 inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
 
-// Workspace: `slots` matrices of ld x ld complex, ld a multiple of 64.
-int ensure_workspace(b200tau_ctx *ctx, int ld, int slots) {
-  const size_t need = (size_t)ld * ld;
-  if (ctx->d_work && need <= ctx->work_elems && slots <= ctx->slots) return B200TAU_OK;
-  cudaFree(ctx->d_work);
-  ctx->d_work = nullptr;
+Plan plan_for(const b200tau_ctx *ctx, int prec) {
+  Plan p;
+  p.steps = ctx->refine_steps[prec == B200TAU_PREC_MIXED ? 1 : 0];
+  p.fk = prec == B200TAU_PREC_MIXED ? kFactorFP32 : kFactorFP64;
+  p.f_separate = (p.fk == kFactorFP32) || p.steps > 0;
+  return p;
+}
+
+size_t f_elem_bytes(const Plan &p) { return p.fk == kFactorFP32 ? sizeof(float2) : sizeof(double2); }
+
+int ensure_workspace(b200tau_ctx *ctx, int ld, int slots, const Plan &p) {
+  const size_t m_need = (size_t)ld * ld;
+  const size_t f_need = p.f_separate ? m_need * f_elem_bytes(p) : 0;
+  const size_t v_need = (size_t)3 * ld * kMaxB;
+  const bool ok = ctx->d_M && m_need <= ctx->m_elems && f_need <= ctx->f_bytes &&
+                  v_need <= ctx->vec_elems && slots <= ctx->slots;
+  if (ok) return B200TAU_OK;
+  CK(cudaStreamSynchronize(ctx->stream));
+  cudaFree(ctx->d_M);
+  cudaFree(ctx->d_F);
+  cudaFree(ctx->d_vec);
   cudaFree(ctx->d_info);
+  cudaFree(ctx->d_conv);
+  ctx->d_M = nullptr;
+  ctx->d_F = nullptr;
+  ctx->d_vec = nullptr;
   ctx->d_info = nullptr;
-  CK(cudaMalloc(&ctx->d_work, need * slots * sizeof(double2)));
-  CK(cudaMalloc(&ctx->d_info, sizeof(int) * slots));
-  ctx->work_elems = need;
-  ctx->slots = slots;
+  ctx->d_conv = nullptr;
+  const size_t m_el = std::max(m_need, ctx->m_elems);
+  const size_t f_b = std::max(f_need, ctx->f_bytes);
+  const size_t v_el = std::max(v_need, ctx->vec_elems);
+  const int sl = std::max(slots, ctx->slots);
+  CK(cudaMalloc(&ctx->d_M, m_el * sl * sizeof(double2)));
+  if (f_b) CK(cudaMalloc(&ctx->d_F, f_b * sl));
+  CK(cudaMalloc(&ctx->d_vec, v_el * sl * sizeof(double2)));
+  CK(cudaMalloc(&ctx->d_info, sizeof(int) * sl));
+  CK(cudaMalloc(&ctx->d_conv, sizeof(int) * sl));
+  ctx->m_elems = m_el;
+  ctx->f_bytes = f_b;
+  ctx->vec_elems = v_el;
+  ctx->slots = sl;
   return B200TAU_OK;
 }
 
@@ -133,20 +185,167 @@ int ensure_out(b200tau_ctx *ctx, size_t n) {
   return B200TAU_OK;
 }
 
-int choose_slots(b200tau_ctx *ctx, int ld, int njobs) {
+int choose_slots(b200tau_ctx *ctx, int ld, int njobs, const Plan &p) {
   size_t freeb = 0, totalb = 0;
   if (cudaMemGetInfo(&freeb, &totalb) != cudaSuccess) freeb = (size_t)8 << 30;
-  const size_t per = (size_t)ld * ld * sizeof(double2);
-  size_t budget = freeb / 2;
+  // memory already held by the context's workspace counts as available to it
+  freeb += ctx->m_elems * ctx->slots * sizeof(double2) + ctx->f_bytes * ctx->slots;
+  const size_t per = (size_t)ld * ld * (sizeof(double2) + (p.f_separate ? f_elem_bytes(p) : 0)) +
+                     (size_t)3 * ld * kMaxB * sizeof(double2);
+  const size_t budget = freeb / 2;
   int s = (int)std::max<size_t>(1, budget / std::max<size_t>(per, 1));
   s = std::min(s, ctx->max_slots);
   s = std::min(s, njobs);
   return std::max(s, 1);
 }
 
-// Validate jobs, build the JobDev records for one wave and run the device pipeline.
-int run_wave(b200tau_ctx *ctx, const b200tau_job *jobs, const int *idx, int nw, int ld,
-             int prec, double2 *out_base) {
+void fill_slot(b200tau_ctx *ctx, JobDev &J, int slot, int ld, const Plan &p) {
+  J.M = ctx->d_M + (size_t)slot * ctx->m_elems;
+  J.F = p.f_separate ? static_cast<void *>(ctx->d_F + (size_t)slot * ctx->f_bytes) : static_cast<void *>(J.M);
+  double2 *v = ctx->d_vec + (size_t)slot * ctx->vec_elems;
+  J.X = v;
+  J.R = v + (size_t)ld * kMaxB;
+  J.Y = v + (size_t)2 * ld * kMaxB;
+  J.ld = ld;
+  J.conv = ctx->d_conv + slot;
+}
+
+BuildParams build_params(const b200tau_ctx *ctx, const Plan &p) {
+  BuildParams bp;
+  bp.tables = ctx->d_tables;
+  bp.tmat = ctx->d_tmat;
+  bp.tmat_ld = ctx->tmat_ld;
+  bp.blk = ctx->blk;
+  bp.kkrsz = ctx->kkrsz;
+  bp.ns = ctx->ns;
+  bp.npola = ctx->npola;
+  bp.f_kind = !p.f_separate ? 0 : (p.fk == kFactorFP32 ? 2 : 1);
+  return bp;
+}
+
+// Device pipeline for one wave whose JobDev records are already in ctx->d_jobs.
+typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// 3-D float tensor (128 floats per row, `rows` rows per slot, `slots` slots) read in
+// 32 x box_rows boxes with 128-byte swizzle; out-of-range rows read as zero.
+int encode_pack_map(b200tau_ctx *ctx, EncodeTiledFn enc, CUtensorMap *map, float *base, int rows, int slots,
+                    int box_rows) {
+  const cuuint64_t dims[3] = {128, (cuuint64_t)rows, (cuuint64_t)slots};
+  const cuuint64_t strides[2] = {128 * sizeof(float), (cuuint64_t)rows * 128 * sizeof(float)};
+  const cuuint32_t box[3] = {32, (cuuint32_t)box_rows, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(ctx, B200TAU_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+  return B200TAU_OK;
+}
+
+int ensure_tc(b200tau_ctx *ctx, int ld, int slots) {
+  if (ctx->d_pack && ld <= ctx->tc_ld && slots <= ctx->tc_slots) return B200TAU_OK;
+  CK(cudaStreamSynchronize(ctx->stream));
+  cudaFree(ctx->d_pack);
+  ctx->d_pack = nullptr;
+  ld = std::max(ld, ctx->tc_ld);
+  slots = std::max(slots, ctx->tc_slots);
+  const size_t a_slot = (size_t)2 * ld * 128, b_slot = (size_t)ld * 128;
+  CK(cudaMalloc(&ctx->d_pack, sizeof(float) * 2 * (a_slot + b_slot) * slots));
+  TcMaps &t = ctx->tc;
+  t.a_slot = a_slot;
+  t.b_slot = b_slot;
+  t.a_hi = ctx->d_pack;
+  t.a_lo = t.a_hi + a_slot * slots;
+  t.b_hi = t.a_lo + a_slot * slots;
+  t.b_lo = t.b_hi + b_slot * slots;
+  void *fn = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+  if (!fn || q != cudaDriverEntryPointSuccess) return fail(ctx, B200TAU_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+  EncodeTiledFn enc = reinterpret_cast<EncodeTiledFn>(fn);
+  int rc;
+  if ((rc = encode_pack_map(ctx, enc, &t.tA_hi, t.a_hi, 2 * ld, slots, 128))) return rc;
+  if ((rc = encode_pack_map(ctx, enc, &t.tA_lo, t.a_lo, 2 * ld, slots, 128))) return rc;
+  if ((rc = encode_pack_map(ctx, enc, &t.tB_hi, t.b_hi, ld, slots, 256))) return rc;
+  if ((rc = encode_pack_map(ctx, enc, &t.tB_lo, t.b_lo, ld, slots, 256))) return rc;
+  ctx->tc_ld = ld;
+  ctx->tc_slots = slots;
+  return B200TAU_OK;
+}
+
+// Tensor map over the FP32 factor slots of the current wave (floats; column c of slot z starts at
+// z * f_bytes + c * 2 ld * 4 bytes), the destination of the tensor-core update's TMA reduce-add.
+int encode_factor_map(b200tau_ctx *ctx, int ld, int slots) {
+  void *fn = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
+  if (!fn || q != cudaDriverEntryPointSuccess) return fail(ctx, B200TAU_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+  EncodeTiledFn enc = reinterpret_cast<EncodeTiledFn>(fn);
+  const cuuint64_t dims[3] = {(cuuint64_t)2 * ld, (cuuint64_t)ld, (cuuint64_t)slots};
+  const cuuint64_t strides[2] = {(cuuint64_t)2 * ld * sizeof(float), (cuuint64_t)ctx->f_bytes};
+  const cuuint32_t box[3] = {128, 64, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  const CUresult r = enc(&ctx->tc.tF, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, ctx->d_F, dims, strides, box, estr,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(ctx, B200TAU_ERR_CUDA, "cuTensorMapEncodeTiled (F) failed (%d)", (int)r);
+  return B200TAU_OK;
+}
+
+// Fold the recorded (start, stop) event pairs into the profile totals.
+int drain_timer(b200tau_ctx *ctx) {
+  if (!ctx->profiling || ctx->timer.used == 0) return B200TAU_OK;
+  CK(cudaStreamSynchronize(ctx->stream));
+  for (int i = 0; i + 1 < ctx->timer.used; i += 2) {
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ctx->timer.ev[i], ctx->timer.ev[i + 1]));
+    ctx->prof_ms += ms;
+    ctx->prof_launches += 1;
+  }
+  ctx->timer.used = 0;
+  return B200TAU_OK;
+}
+
+// Algorithmic FLOPs of the trailing updates of one wave: sum over steps and jobs of
+// 8 (N - k - kb)^2 kb (complex multiply-add = 8 real FLOPs).
+double trailing_flops(const std::vector<JobDev> &h) {
+  double f = 0.0;
+  for (const JobDev &J : h)
+    for (int k = 0; k < J.n; k += kNb) {
+      const double kb = std::min(kNb, J.n - k);
+      const double rest = J.N - k - kb;
+      f += 8.0 * rest * rest * kb;
+    }
+  return f;
+}
+
+int run_pipeline(b200tau_ctx *ctx, int nw, int maxn, int maxN, int ld, int ns, int kkrsz, const Plan &p) {
+  if (ctx->profiling && ctx->timer.used + 4 * (maxn / kNb + 2) > ctx->timer.cap) {
+    int rc = drain_timer(ctx);
+    if (rc) return rc;
+  }
+  const TcMaps *tc = nullptr;
+  if (p.fk == kFactorFP32 && ctx->mixed_engine == B200TAU_ENGINE_TENSOR) {
+    // the jobs' leading dimension `ld` (fill_slot) fixes the column stride of the factor map
+    int rc = ensure_tc(ctx, ld, std::max(nw, ctx->slots));
+    if (rc) return rc;
+    if ((rc = encode_factor_map(ctx, ld, ctx->slots))) return rc;
+    tc = &ctx->tc;
+  }
+  CK(launch_eliminate(p.fk, ctx->d_jobs, nw, maxn, maxN, ctx->d_info, ctx->stream, &ctx->launches,
+                      ctx->profiling ? &ctx->timer : nullptr, tc, ctx->d_err));
+  if (p.steps > 0) {
+    CK(launch_solve_refine(p.fk, ctx->d_jobs, nw, maxn, maxN, ctx->b, p.steps, ns, kkrsz, ctx->d_info,
+                           ctx->stream, &ctx->launches));
+  } else {
+    CK(launch_finalize_direct(p.fk, ctx->d_jobs, nw, ns, kkrsz, ctx->d_info, ctx->stream, &ctx->launches));
+  }
+  return B200TAU_OK;
+}
+
+int run_wave(b200tau_ctx *ctx, const b200tau_job *jobs, const int *idx, int nw, int ld, const Plan &p,
+             double2 *out_base) {
   std::vector<JobDev> h(nw);
   int maxL = 0, maxN = 0, maxn = 0;
   for (int w = 0; w < nw; ++w) {
@@ -161,12 +360,11 @@ int run_wave(b200tau_ctx *ctx, const b200tau_job *jobs, const int *idx, int nw, 
     J.store = a.store;
     J.perm = a.perm;
     J.off = a.off;
-    J.M = ctx->d_work + (size_t)w * ctx->work_elems;
+    fill_slot(ctx, J, w, ld, p);
     J.L = a.L;
     J.N = a.N;
     J.b = a.b;
     J.n = a.N - a.b;
-    J.ld = ld;
     J.iie = jb.iie;
     J.ispin = jb.ispin;
     const long jsm = (ctx->npola != ctx->ns) ? (long)ctx->kkrsz * ctx->kkrsz * jb.ispin : 0;
@@ -184,21 +382,10 @@ int run_wave(b200tau_ctx *ctx, const b200tau_job *jobs, const int *idx, int nw, 
   }
   CK(cudaMemcpyAsync(ctx->d_jobs, h.data(), sizeof(JobDev) * nw, cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemsetAsync(ctx->d_info, 0, sizeof(int) * nw, ctx->stream));
-  BuildParams bp;
-  bp.tables = ctx->d_tables;
-  bp.tmat = ctx->d_tmat;
-  bp.tmat_ld = ctx->tmat_ld;
-  bp.blk = ctx->blk;
-  bp.kkrsz = ctx->kkrsz;
-  bp.ns = ctx->ns;
-  bp.npola = ctx->npola;
-  CK(launch_kkr_build(ctx->d_jobs, nw, maxL, bp, ctx->d_err, ctx->stream));
-  ctx->launches += 1;
-  (void)prec;
-  CK(launch_lu_fp64(ctx->d_jobs, nw, maxn, maxN, 64, ctx->d_info, ctx->stream, &ctx->launches));
-  CK(launch_finalize(ctx->d_jobs, nw, ctx->ns, ctx->kkrsz, ctx->d_info, ctx->stream));
-  ctx->launches += 1;
-  return B200TAU_OK;
+  CK(cudaMemsetAsync(ctx->d_conv, 0, sizeof(int) * nw, ctx->stream));
+  CK(launch_kkr_build(ctx->d_jobs, nw, maxL, build_params(ctx, p), ctx->d_err, ctx->stream, &ctx->launches));
+  if (ctx->profiling) ctx->prof_flops += trailing_flops(h);
+  return run_pipeline(ctx, nw, maxn, maxN, ld, ctx->ns, ctx->kkrsz, p);
 }
 
 int check_info(b200tau_ctx *ctx, const std::vector<int> &info, const int *idx, int nw) {
@@ -223,6 +410,7 @@ int validate_jobs(b200tau_ctx *ctx, const b200tau_job *jobs, int njobs) {
     const int nspin = (ctx->npola != ctx->ns) ? 2 : 1;
     if (jb.ispin < 0 || jb.ispin >= nspin)
       return fail(ctx, B200TAU_ERR_ARG, "job %d: ispin %d invalid", j, jb.ispin);
+    if (jb.reserved != 0) return fail(ctx, B200TAU_ERR_ARG, "job %d: reserved field must be 0", j);
     const AtomDev &a = ctx->atoms[jb.atom];
     for (int s : a.h_store)
       if (s < 0 || s >= ctx->nstore)
@@ -237,6 +425,7 @@ int solve_impl(b200tau_ctx *ctx, const b200tau_job *jobs, int njobs, int prec, d
   if (njobs == 0) return B200TAU_OK;
   int rc = validate_jobs(ctx, jobs, njobs);
   if (rc) return rc;
+  const Plan p = plan_for(ctx, prec);
   std::vector<int> order(njobs);
   for (int j = 0; j < njobs; ++j) order[j] = j;
   std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
@@ -244,14 +433,14 @@ int solve_impl(b200tau_ctx *ctx, const b200tau_job *jobs, int njobs, int prec, d
   });
   const int maxN = ctx->atoms[jobs[order[0]].atom].N;
   const int ld = round_up(maxN, 64);
-  const int slots = choose_slots(ctx, ld, njobs);
-  if ((rc = ensure_workspace(ctx, ld, slots))) return rc;
+  const int slots = choose_slots(ctx, ld, njobs, p);
+  if ((rc = ensure_workspace(ctx, ld, slots, p))) return rc;
   if ((rc = ensure_jobs(ctx, slots))) return rc;
   ctx->launches = 0;
   std::vector<int> info(slots);
   for (int w0 = 0; w0 < njobs; w0 += slots) {
     const int nw = std::min(slots, njobs - w0);
-    if ((rc = run_wave(ctx, jobs, &order[w0], nw, ld, prec, dev_out))) return rc;
+    if ((rc = run_wave(ctx, jobs, &order[w0], nw, ld, p, dev_out))) return rc;
     if (sync_and_check || w0 + nw < njobs) {
       CK(cudaMemcpyAsync(info.data(), ctx->d_info, sizeof(int) * nw, cudaMemcpyDeviceToHost,
                          ctx->stream));
@@ -269,6 +458,12 @@ int check_err_flags(b200tau_ctx *ctx) {
     cudaMemset(ctx->d_err, 0, sizeof(int));
     return fail(ctx, B200TAU_ERR_TIMEOUT, "a device-side wait exceeded its bound (flags %d)", flags);
   }
+  return B200TAU_OK;
+}
+
+int check_prec(b200tau_ctx *ctx, int prec) {
+  if (prec != B200TAU_PREC_FP64 && prec != B200TAU_PREC_MIXED)
+    return fail(ctx, B200TAU_ERR_ARG, "unknown precision %d", prec);
   return B200TAU_OK;
 }
 
@@ -314,12 +509,17 @@ void b200tau_destroy(b200tau_ctx *ctx) {
   for (auto &a : ctx->atoms) free_atom(a);
   cudaFree(ctx->d_tables);
   cudaFree(ctx->d_tmat);
-  cudaFree(ctx->d_work);
+  cudaFree(ctx->d_M);
+  cudaFree(ctx->d_F);
+  cudaFree(ctx->d_vec);
   cudaFree(ctx->d_jobs);
   cudaFree(ctx->d_info);
+  cudaFree(ctx->d_conv);
   cudaFree(ctx->d_err);
   cudaFree(ctx->d_out);
   cudaFree(ctx->d_t0);
+  cudaFree(ctx->d_pack);
+  for (auto &e : ctx->events) cudaEventDestroy(e);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -333,6 +533,50 @@ long b200tau_last_launch_count(const b200tau_ctx *ctx) { return ctx ? ctx->launc
 int b200tau_gaunt_numbers(int lmax, double *cgnt) {
   if (lmax < 0 || lmax > kMaxLmax || !cgnt) return B200TAU_ERR_ARG;
   gaunt_numbers(lmax, cgnt);
+  return B200TAU_OK;
+}
+
+int b200tau_set_profiling(b200tau_ctx *ctx, int enable) {
+  if (!ctx) return B200TAU_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if (enable && ctx->events.empty()) {
+    ctx->events.resize(4096);
+    for (auto &e : ctx->events) CK(cudaEventCreate(&e));
+    ctx->timer.ev = ctx->events.data();
+    ctx->timer.cap = (int)ctx->events.size();
+  }
+  ctx->timer.used = 0;
+  ctx->profiling = enable != 0;
+  ctx->prof_ms = ctx->prof_flops = 0.0;
+  ctx->prof_launches = 0;
+  return B200TAU_OK;
+}
+
+int b200tau_profile_read(b200tau_ctx *ctx, double *ms, long *launches, double *flops) {
+  if (!ctx) return B200TAU_ERR_ARG;
+  int rc = drain_timer(ctx);
+  if (rc) return rc;
+  if (ms) *ms = ctx->prof_ms;
+  if (launches) *launches = ctx->prof_launches;
+  if (flops) *flops = ctx->prof_flops;
+  return B200TAU_OK;
+}
+
+int b200tau_set_mixed_engine(b200tau_ctx *ctx, int engine) {
+  if (!ctx) return B200TAU_ERR_ARG;
+  if (engine != B200TAU_ENGINE_TENSOR && engine != B200TAU_ENGINE_SIMT)
+    return fail(ctx, B200TAU_ERR_ARG, "unknown engine %d", engine);
+  ctx->mixed_engine = engine;
+  return B200TAU_OK;
+}
+
+int b200tau_set_refinement(b200tau_ctx *ctx, int prec, int steps) {
+  if (!ctx) return B200TAU_ERR_ARG;
+  int rc = check_prec(ctx, prec);
+  if (rc) return rc;
+  if (steps < 0 || steps > 16) return fail(ctx, B200TAU_ERR_ARG, "refinement steps %d outside 0..16", steps);
+  ctx->refine_steps[prec == B200TAU_PREC_MIXED ? 1 : 0] = steps;
   return B200TAU_OK;
 }
 
@@ -413,15 +657,13 @@ int b200tau_solve(b200tau_ctx *ctx, const b200tau_job *jobs, int njobs, int prec
   if (!ctx) return B200TAU_ERR_ARG;
   if (njobs < 0 || (njobs > 0 && (!jobs || !tau00_l)))
     return fail(ctx, B200TAU_ERR_ARG, "solve: bad arguments");
-  if (prec != B200TAU_PREC_FP64 && prec != B200TAU_PREC_MIXED)
-    return fail(ctx, B200TAU_ERR_ARG, "solve: unknown precision %d", prec);
+  int rc = check_prec(ctx, prec);
+  if (rc) return rc;
   if (njobs == 0) return B200TAU_OK;
   CK(cudaSetDevice(ctx->device));
   const size_t outn = (size_t)njobs * ctx->b * ctx->b;
-  int rc = ensure_out(ctx, outn);
-  if (rc) return rc;
-  rc = solve_impl(ctx, jobs, njobs, prec, ctx->d_out, true);
-  if (rc) return rc;
+  if ((rc = ensure_out(ctx, outn))) return rc;
+  if ((rc = solve_impl(ctx, jobs, njobs, prec, ctx->d_out, true))) return rc;
   CK(cudaMemcpyAsync(tau00_l, ctx->d_out, sizeof(double2) * outn, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   return check_err_flags(ctx);
@@ -432,8 +674,8 @@ int b200tau_solve_device(b200tau_ctx *ctx, const b200tau_job *jobs, int njobs, i
   if (!ctx) return B200TAU_ERR_ARG;
   if (njobs < 0 || (njobs > 0 && (!jobs || !tau00_l_dev)))
     return fail(ctx, B200TAU_ERR_ARG, "solve_device: bad arguments");
-  if (prec != B200TAU_PREC_FP64 && prec != B200TAU_PREC_MIXED)
-    return fail(ctx, B200TAU_ERR_ARG, "solve_device: unknown precision %d", prec);
+  int rc = check_prec(ctx, prec);
+  if (rc) return rc;
   CK(cudaSetDevice(ctx->device));
   return solve_impl(ctx, jobs, njobs, prec, reinterpret_cast<double2 *>(tau00_l_dev), false);
 }
@@ -441,8 +683,8 @@ int b200tau_solve_device(b200tau_ctx *ctx, const b200tau_job *jobs, int njobs, i
 int b200tau_sync(b200tau_ctx *ctx) {
   if (!ctx) return B200TAU_ERR_ARG;
   CK(cudaStreamSynchronize(ctx->stream));
-  std::vector<int> info(std::max(ctx->slots, 1));
   if (ctx->d_info && ctx->slots > 0) {
+    std::vector<int> info(ctx->slots);
     CK(cudaMemcpy(info.data(), ctx->d_info, sizeof(int) * ctx->slots, cudaMemcpyDeviceToHost));
     for (int w = 0; w < ctx->slots; ++w)
       if (info[w] != 0) {
@@ -458,17 +700,20 @@ int b200tau_solve_dense(b200tau_ctx *ctx, const double *m, int n, int ldm, const
   if (!ctx) return B200TAU_ERR_ARG;
   if (!m || !t0 || !tau00 || n < 1 || b < 1 || b > n || b > kMaxB || ldm < n)
     return fail(ctx, B200TAU_ERR_ARG, "solve_dense: bad arguments (n %d, b %d, ldm %d)", n, b, ldm);
-  if (prec != B200TAU_PREC_FP64 && prec != B200TAU_PREC_MIXED)
-    return fail(ctx, B200TAU_ERR_ARG, "solve_dense: unknown precision %d", prec);
-  CK(cudaSetDevice(ctx->device));
-  const int ld = round_up(n, 64);
-  int rc = ensure_workspace(ctx, ld, std::max(1, ctx->slots));
+  int rc = check_prec(ctx, prec);
   if (rc) return rc;
+  CK(cudaSetDevice(ctx->device));
+  const Plan p = plan_for(ctx, prec);
+  const int ld = round_up(n, 64);
+  if ((rc = ensure_workspace(ctx, ld, std::max(1, ctx->slots), p))) return rc;
   if ((rc = ensure_jobs(ctx, 1))) return rc;
   if ((rc = ensure_out(ctx, (size_t)b * b))) return rc;
   if (!ctx->d_t0) CK(cudaMalloc(&ctx->d_t0, sizeof(double2) * kMaxB * kMaxB));
+  JobDev J;
+  std::memset(&J, 0, sizeof(J));
+  fill_slot(ctx, J, 0, ld, p);
   const int r = n - b;  // reorder: central block (first b) goes last
-  double2 *W = ctx->d_work;
+  double2 *W = J.M;
   const size_t es = sizeof(double2);
   const double2 *hm = reinterpret_cast<const double2 *>(m);
   // [Mrr Mr0; M0r M00] <- [M00 M0r; Mr0 Mrr]
@@ -482,25 +727,20 @@ int b200tau_solve_dense(b200tau_ctx *ctx, const double *m, int n, int ldm, const
   }
   CK(cudaMemcpy2DAsync(W + r + (size_t)r * ld, ld * es, hm, ldm * es, b * es, b, cudaMemcpyHostToDevice,
                        ctx->stream));
+  if (p.f_separate) CK(launch_copy_to_factor(p.fk, W, J.F, n, ld, ctx->stream));
   CK(cudaMemcpyAsync(ctx->d_t0, t0, es * b * b, cudaMemcpyHostToDevice, ctx->stream));
-  JobDev J;
-  std::memset(&J, 0, sizeof(J));
-  J.M = W;
   J.N = n;
   J.n = r;
   J.b = b;
-  J.ld = ld;
   J.t0 = ctx->d_t0;
   J.t0_ld = b;
   J.out = ctx->d_out;
   J.out_mode = 1;
   CK(cudaMemcpyAsync(ctx->d_jobs, &J, sizeof(J), cudaMemcpyHostToDevice, ctx->stream));
   CK(cudaMemsetAsync(ctx->d_info, 0, sizeof(int), ctx->stream));
+  CK(cudaMemsetAsync(ctx->d_conv, 0, sizeof(int), ctx->stream));
   ctx->launches = 0;
-  (void)prec;
-  CK(launch_lu_fp64(ctx->d_jobs, 1, r, n, 64, ctx->d_info, ctx->stream, &ctx->launches));
-  CK(launch_finalize(ctx->d_jobs, 1, 1, b, ctx->d_info, ctx->stream));
-  ctx->launches += 1;
+  if ((rc = run_pipeline(ctx, 1, r, n, ld, 1, b, p))) return rc;
   int info = 0;
   CK(cudaMemcpyAsync(&info, ctx->d_info, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaMemcpyAsync(tau00, ctx->d_out, es * b * b, cudaMemcpyDeviceToHost, ctx->stream));
@@ -518,7 +758,11 @@ int b200tau_build_kkr(b200tau_ctx *ctx, const b200tau_job *job, double *m_out, i
   if (n != a.N) return fail(ctx, B200TAU_ERR_ARG, "build_kkr: n %d != N %d", n, a.N);
   CK(cudaSetDevice(ctx->device));
   const int ld = round_up(a.N, 64);
-  if ((rc = ensure_workspace(ctx, ld, std::max(1, ctx->slots)))) return rc;
+  Plan p;
+  p.fk = kFactorFP64;
+  p.steps = 0;
+  p.f_separate = false;
+  if ((rc = ensure_workspace(ctx, ld, std::max(1, ctx->slots), p))) return rc;
   if ((rc = ensure_jobs(ctx, 1))) return rc;
   JobDev J;
   std::memset(&J, 0, sizeof(J));
@@ -529,29 +773,21 @@ int b200tau_build_kkr(b200tau_ctx *ctx, const b200tau_job *job, double *m_out, i
   J.store = a.store;
   J.perm = a.perm;
   J.off = a.off;
-  J.M = ctx->d_work;
+  fill_slot(ctx, J, 0, ld, p);
   J.L = a.L;
   J.N = a.N;
   J.b = a.b;
   J.n = a.N - a.b;
-  J.ld = ld;
   J.iie = job->iie;
   J.ispin = job->ispin;
   CK(cudaMemcpyAsync(ctx->d_jobs, &J, sizeof(J), cudaMemcpyHostToDevice, ctx->stream));
-  BuildParams bp;
-  bp.tables = ctx->d_tables;
-  bp.tmat = ctx->d_tmat;
-  bp.tmat_ld = ctx->tmat_ld;
-  bp.blk = ctx->blk;
-  bp.kkrsz = ctx->kkrsz;
-  bp.ns = ctx->ns;
-  bp.npola = ctx->npola;
-  CK(launch_kkr_build(ctx->d_jobs, 1, a.L, bp, ctx->d_err, ctx->stream));
+  ctx->launches = 0;
+  CK(launch_kkr_build(ctx->d_jobs, 1, a.L, build_params(ctx, p), ctx->d_err, ctx->stream, &ctx->launches));
   // undo the central-site-last order: rows/cols [0, r) <-> [b, N), [r, N) <-> [0, b)
   const int r = a.N - a.b, b = a.b;
   const size_t es = sizeof(double2);
   double2 *hm = reinterpret_cast<double2 *>(m_out);
-  const double2 *W = ctx->d_work;
+  const double2 *W = J.M;
   if (r > 0) {
     CK(cudaMemcpy2DAsync(hm + b + (size_t)b * n, n * es, W, ld * es, r * es, r, cudaMemcpyDeviceToHost,
                          ctx->stream));

@@ -1,8 +1,10 @@
 // Internal declarations shared by the b200tau CUDA sources.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
+#include <cstddef>
 #include <cstdint>
 
 namespace b200 {
@@ -14,6 +16,7 @@ constexpr int kMaxLend = 2 * kMaxLmax;                          // 6
 constexpr int kNdlm = (kMaxLend + 1) * (kMaxLend + 2) / 2;       // 28 P_lm values
 constexpr int kNdlj = (kMaxLend + 1) * (kMaxLend + 1);           // 49 D_lm values
 constexpr int kMaxTerms = kMaxLmax + 1;                          // Gaunt terms per G element
+constexpr int kNb = 64;                                         // elimination block width
 
 // Angular-momentum tables for G_ij (makegij_c.f:79-128, buildKKRMatrix_CPU.cpp:144-176),
 // laid out as a gather list: G(lm2, lm1) = pi4 * i^rot * sum_q coef[q] * D[didx[q]]
@@ -38,13 +41,18 @@ static_assert(sizeof(AngularTables) % 16 == 0, "bulk-copy size must be a multipl
 
 // Host-side table construction (angular.cpp).  Returns 0 on success.
 int build_angular_tables(int lmax, AngularTables *out);
-// Gaunt numbers cgnt[l3/2 + (lmax+1)*(j1 + kk*j2)] and the i-factors, exposed for tests.
+// Gaunt numbers cgnt[l3/2 + (lmax+1)*(j1 + kk*j2)], exposed for tests.
 void gaunt_numbers(int lmax, double *cgnt);
 
-// One solve as the device sees it.  Matrices are column-major complex (double2).
+// One solve as the device sees it.  Matrices are column-major complex.
 // Site order inside M: LIZ sites 1..L-1 first, the central site 0 last, so that
 // eliminating the first n = N - b columns leaves the Schur complement
 // S = M00 - M0r Mrr^-1 Mr0 = 1 - Delta in the trailing b x b block.
+//
+// M  : the KKR matrix in FP64, kept unmodified when refinement is on (residuals).
+// F  : the factor storage (FP64 `double2` or FP32 `float2`, see the launcher's type); the block
+//      elimination runs in place on F.  F may alias M (FP64, no refinement).
+// X  : N x b solution (FP64), R : N x b residual, Y : N x b correction (FP64), ld = ld.
 struct JobDev {
   double2 energy;
   double2 prel;
@@ -53,12 +61,14 @@ struct JobDev {
   const int *store;      // L (tmatStore column per site)
   const int *perm;       // L: perm[p] = LIZ site at position p (site 0 last)
   const int *off;        // L+1: row/column offset of position p
-  double2 *M;            // workspace, ld = ld
-  const double2 *t0;     // central t-matrix (b x b, ld t0_ld) for the finalize step
+  double2 *M;
+  void *F;
+  double2 *X;
+  double2 *R;
+  double2 *Y;
+  const double2 *t0;     // central t-matrix (b x b, ld t0_ld)
   double2 *out;          // b*b complex result
-  float2 *Mf;            // FP32 working copy (mixed precision), ld = ld
-  double2 *X;            // N x b solution (mixed precision refinement), ld = ld
-  double2 *R;            // N x b residual / correction (mixed precision), ld = ld
+  int *conv;             // refinement converged flag (set on the device, skips later rounds)
   double2 ubr[4];
   double2 ubrd[4];
   int L, N, n, b;
@@ -77,14 +87,51 @@ struct BuildParams {
   int kkrsz;                    // (maxlmax+1)^2
   int ns;                       // n_spin_cant
   int npola;                    // n_spin_pola
+  int f_kind;                   // 0: no F copy (F aliases M), 1: FP64 copy, 2: FP32 copy
 };
 
-// Launchers (return cudaGetLastError of the launch).
+enum FactorKind { kFactorFP64 = 0, kFactorFP32 = 1 };
+
+// Optional CUDA-event bracketing of the trailing-update launches (the dominant kernel), on the
+// launching stream.  `ev` holds `cap` events; pairs (start, stop) are recorded from `used`.
+struct KernelTimer {
+  cudaEvent_t *ev = nullptr;
+  int cap = 0;
+  int used = 0;
+};
+
+// Operand packs and TMA descriptors of the tensor-core trailing update (tc_update.cu).
+// Per wave slot: A pack 2 ld rows x 128 floats (hi and lo), B pack ld rows x 128 floats.
+struct TcMaps {
+  CUtensorMap tA_hi, tA_lo, tB_hi, tB_lo;
+  CUtensorMap tF;  // the wave's FP32 factor slots as floats {2 ld, ld, slots}, box {128, 64, 1}
+  float *a_hi = nullptr, *a_lo = nullptr, *b_hi = nullptr, *b_lo = nullptr;
+  size_t a_slot = 0, b_slot = 0;  // floats per slot
+};
+size_t tc_smem_bytes();
+cudaError_t tc_prepare();
+// Pack + tensor-core update A22 -= A21 W for step k of every job in the wave (FP32 factors).
+cudaError_t launch_tc_step(const TcMaps &maps, const JobDev *jobs, int njobs, int k, int max_N, int *err,
+                           cudaStream_t s);
+
+// Launchers (return cudaGetLastError of the launches).  `launches` accumulates the number of
+// kernels enqueued.
 cudaError_t launch_kkr_build(const JobDev *jobs, int njobs, int max_L, const BuildParams &p,
-                             int *err_flags, cudaStream_t s);
-cudaError_t launch_lu_fp64(const JobDev *jobs, int njobs, int max_n, int max_N, int nb,
-                           int *info, cudaStream_t s, long *launches);
-cudaError_t launch_finalize(const JobDev *jobs, int njobs, int ns, int kkrsz, int *info,
-                            cudaStream_t s);
+                             int *err_flags, cudaStream_t s, long *launches);
+// Block elimination of F over the first n columns (all jobs of the wave).
+// With FP32 factors and `tc` non-null the trailing update runs on the tensor cores (tc_update.cu).
+cudaError_t launch_eliminate(FactorKind fk, const JobDev *jobs, int njobs, int max_n, int max_N,
+                             int *info, cudaStream_t s, long *launches, KernelTimer *timer,
+                             const TcMaps *tc, int *err);
+// F = M (n x n, leading dimension ld) converted to the factor type.
+cudaError_t launch_copy_to_factor(FactorKind fk, const double2 *M, void *F, int n, int ld, cudaStream_t s);
+// tau00 from the Schur block directly (no refinement): out = S^-1 t0 (- t0, rotated).
+cudaError_t launch_finalize_direct(FactorKind fk, const JobDev *jobs, int njobs, int ns, int kkrsz,
+                                   int *info, cudaStream_t s, long *launches);
+// Iterative refinement of X for M X = [0; t0]: initial solve from the factors, then `steps`
+// rounds of R = B - M X (FP64), Y = F^-1 R, X += Y; then out from X[n:N].
+cudaError_t launch_solve_refine(FactorKind fk, const JobDev *jobs, int njobs, int max_n, int max_N,
+                                int b, int steps, int ns, int kkrsz, int *info, cudaStream_t s,
+                                long *launches);
 
 }  // namespace b200

@@ -123,6 +123,15 @@ __global__ void __launch_bounds__(kThreads)
   const int col0 = J.off[pc];
   const int ld = J.ld;
   double2 *__restrict__ M = J.M;
+  // second copy for the factorisation when refinement keeps M: FP64 (f_kind 1) or FP32 (2)
+  const int f_kind = p.f_kind;
+  double2 *__restrict__ F64 = f_kind == 1 ? static_cast<double2 *>(J.F) : nullptr;
+  float2 *__restrict__ F32 = f_kind == 2 ? static_cast<float2 *>(J.F) : nullptr;
+  auto put = [&](size_t idx, double2 v) {
+    M[idx] = v;
+    if (f_kind == 1) F64[idx] = v;
+    else if (f_kind == 2) F32[idx] = make_float2((float)v.x, (float)v.y);
+  };
   const double2 prel = J.prel;
   // collinear spin-polarised: spin block offset kkrsz^2 * ispin (buildKKRMatrix_CPU.cpp:402)
   const long jsm = (p.npola != p.ns) ? (long)kkrsz * kkrsz * J.ispin : 0;
@@ -136,8 +145,7 @@ __global__ void __launch_bounds__(kThreads)
     if (pr == pc) {  // diagonal block: identity (buildKKRMatrix_CPU.cpp:266-268)
       for (int c = 0; c < nc; ++c)
         for (int r = lane; r < nr; r += 32)
-          M[(size_t)(row0 + r) + (size_t)(col0 + c) * ld] =
-              make_double2(r == c ? 1.0 : 0.0, 0.0);
+          put((size_t)(row0 + r) + (size_t)(col0 + c) * ld, make_double2(r == c ? 1.0 : 0.0, 0.0));
       continue;
     }
     // rij = pos(ir1) - pos(ir2), ir1 = row site (calculateTauMatrix.cpp:206-208)
@@ -263,7 +271,7 @@ __global__ void __launch_bounds__(kThreads)
 #pragma unroll
           for (int k = 0; k < kMaxKK; ++k)
             if (k < kki) acc = cfma(trow_v[k], sm.G[warp][k * kMaxKK + cp], acc);
-          M[(size_t)(row0 + rr) + (size_t)(col0 + sc * kkj + cp) * ld] = make_double2(-acc.x, -acc.y);
+          put((size_t)(row0 + rr) + (size_t)(col0 + sc * kkj + cp) * ld, make_double2(-acc.x, -acc.y));
         }
       }
     }
@@ -274,12 +282,13 @@ __global__ void __launch_bounds__(kThreads)
 }  // namespace
 
 cudaError_t launch_kkr_build(const JobDev *jobs, int njobs, int max_L, const BuildParams &p,
-                             int *err_flags, cudaStream_t s) {
+                             int *err_flags, cudaStream_t s, long *launches) {
   const int smem = (int)sizeof(BuildSmem);
   cudaError_t e = cudaFuncSetAttribute(kkr_build_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
   dim3 grid(max_L, njobs);
   kkr_build_kernel<<<grid, kThreads, smem, s>>>(jobs, p, err_flags);
+  if (launches) *launches += 1;
   return cudaGetLastError();
 }
 

@@ -36,13 +36,16 @@ ERR_TIMEOUT = 5
 ERR_STATE = 6
 PREC_FP64 = 0
 PREC_MIXED = 1
+ENGINE_TENSOR = 0
+ENGINE_SIMT = 1
 
 # Symbols declared in include/b200tau.h.
 EXPORTS = (
     "b200tau_create", "b200tau_destroy", "b200tau_last_error", "b200tau_stream",
     "b200tau_upload_tmat", "b200tau_set_atom", "b200tau_solve", "b200tau_solve_device",
     "b200tau_sync", "b200tau_solve_dense", "b200tau_build_kkr", "b200tau_last_launch_count",
-    "b200tau_gaunt_numbers",
+    "b200tau_gaunt_numbers", "b200tau_set_refinement", "b200tau_set_profiling",
+    "b200tau_profile_read", "b200tau_set_mixed_engine",
 )
 
 
@@ -88,6 +91,10 @@ def load_library():
     lib.b200tau_last_launch_count.argtypes = [P]
     lib.b200tau_last_launch_count.restype = L
     lib.b200tau_gaunt_numbers.argtypes = [I, P]
+    lib.b200tau_set_refinement.argtypes = [P, I, I]
+    lib.b200tau_set_profiling.argtypes = [P, I]
+    lib.b200tau_set_mixed_engine.argtypes = [P, I]
+    lib.b200tau_profile_read.argtypes = [P, P, P, P]
     _lib = lib
     return lib
 
@@ -156,6 +163,23 @@ class TauSolver:
     @property
     def last_launch_count(self) -> int:
         return int(self.lib.b200tau_last_launch_count(self.ctx))
+
+    def set_refinement(self, prec: int, steps: int):
+        """FP64 refinement steps of a precision (see b200tau_set_refinement)."""
+        self._check(self.lib.b200tau_set_refinement(self.ctx, prec, steps))
+
+    def set_mixed_engine(self, engine: int):
+        """Trailing-update engine of the mixed path: ENGINE_TENSOR (tcgen05) or ENGINE_SIMT."""
+        self._check(self.lib.b200tau_set_mixed_engine(self.ctx, engine))
+
+    def set_profiling(self, enable: bool):
+        self._check(self.lib.b200tau_set_profiling(self.ctx, int(bool(enable))))
+
+    def profile_read(self):
+        """(device ms, launches, algorithmic FLOPs) of the timed trailing-update launches."""
+        ms, n, fl = ctypes.c_double(), ctypes.c_long(), ctypes.c_double()
+        self._check(self.lib.b200tau_profile_read(self.ctx, ctypes.byref(ms), ctypes.byref(n), ctypes.byref(fl)))
+        return ms.value, n.value, fl.value
 
     # -- uploads (DeviceStorage / DeviceAtom) ----------------------------------------------
     def upload_tmat(self, tmat_store: np.ndarray):
