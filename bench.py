@@ -171,6 +171,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--energies", type=int, default=N_ENERGIES,
+                    help="contour points solved per step (31 = the benchmark; fewer for small profiling cases)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup()
@@ -193,12 +195,13 @@ def main():
 
     # each rank its own atom (seed) -> independent solves
     prob = W.config_n2160(seed=2 + rank, npts=N_ENERGIES)
+    ne = max(1, min(args.energies, N_ENERGIES))
     N, b, L = prob.nrmat_ns, prob.kkrsz_ns, prob.num_liz
     flops_per_solve = algorithmic_flops(N, b, L)
     s = T.TauSolver(prob.lmax, prob.n_spin_cant, prob.n_spin_pola, device=local)
     s.load_problem(prob)
-    jobs = T.make_jobs([(0, i, 0, prob.energies[i]) for i in range(N_ENERGIES)])
-    out = torch.empty(N_ENERGIES * b * b * 2, dtype=torch.float64, device=f"cuda:{local}")
+    jobs = T.make_jobs([(0, i, 0, prob.energies[i]) for i in range(ne)])
+    out = torch.empty(ne * b * b * 2, dtype=torch.float64, device=f"cuda:{local}")
     stream = torch.cuda.ExternalStream(s.stream, device=f"cuda:{local}")
 
     def barrier():
@@ -241,10 +244,10 @@ def main():
     # --- plain FP64 on the same workload ---------------------------------------------------------
     ms_fp64, _ = timed(T.PREC_FP64, max(2, args.steps // 2), 1)
     fp64_out = out.clone()
-    a = mixed_out.cpu().numpy().view(np.complex128).reshape(N_ENERGIES, -1)
-    f = fp64_out.cpu().numpy().view(np.complex128).reshape(N_ENERGIES, -1)
-    t0l = np.stack([prob.t_block(int(prob.liz_store_idx[0]), i).T.reshape(-1) for i in range(N_ENERGIES)])
-    err = float(max(np.abs(a[i] - f[i]).max() / np.abs(f[i] + t0l[i]).max() for i in range(N_ENERGIES)))
+    a = mixed_out.cpu().numpy().view(np.complex128).reshape(ne, -1)
+    f = fp64_out.cpu().numpy().view(np.complex128).reshape(ne, -1)
+    t0l = np.stack([prob.t_block(int(prob.liz_store_idx[0]), i).T.reshape(-1) for i in range(ne)])
+    err = float(max(np.abs(a[i] - f[i]).max() / np.abs(f[i] + t0l[i]).max() for i in range(ne)))
 
     # --- roofline of the dominant kernel (trailing update), CUDA events on the library stream ---
     s.set_profiling(True)
@@ -261,7 +264,7 @@ def main():
     tm_host = torch.from_numpy(np.ascontiguousarray(prob.tmat_store).view(np.float64)).pin_memory()
     tm_np = tm_host.numpy().view(np.complex128).reshape(prob.tmat_store.shape)
     h2d = tm_np.nbytes + prob.liz_pos.nbytes + prob.liz_lmax.nbytes + prob.liz_store_idx.nbytes
-    d2h = N_ENERGIES * b * b * 16
+    d2h = ne * b * b * 16
     for _ in range(2):
         s.upload_tmat(tm_np)
         s.set_atom(0, prob.liz_pos, prob.liz_lmax, prob.liz_store_idx, prob.ubr, prob.ubrd)
@@ -279,8 +282,8 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(prob)
 
-    value = world * N_ENERGIES / (ms_mixed * 1e-3)
-    fp64_value = world * N_ENERGIES / (ms_fp64 * 1e-3)
+    value = world * ne / (ms_mixed * 1e-3)
+    fp64_value = world * ne / (ms_fp64 * 1e-3)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
@@ -289,8 +292,8 @@ def main():
             "data": "synthetic (seeded phase-shift t-matrices, fcc LIZ)",
             "config": {"workload": "fcc LIZ 135 sites a=6.82, lmax 3, N=2160, kkrsz_ns 16, "
                                    "31-point semicircle contour -0.3..0.7 Ry, one atom per GPU",
-                       "solves_per_step": N_ENERGIES, "l2": "inputs larger than L2 "
-                       f"({N_ENERGIES} x {N * N * 16 / 1e6:.0f} MB KKR matrices per step)",
+                       "solves_per_step": ne, "l2": "inputs larger than L2 "
+                       f"({ne} x {N * N * 16 / 1e6:.0f} MB KKR matrices per step)",
                        "refinement_steps_mixed": 3, "refinement_steps_fp64": 1},
             "fp64": {"value": fp64_value, "unit": "solves/s", "ms_per_step": ms_fp64,
                      "mixed_over_fp64": value / fp64_value},
@@ -308,7 +311,7 @@ def main():
                                        "that (hi*hi + hi*lo + lo*hi)",
                          "peak_source": f"TF32 dense = bf16_tflops / 2 of {peak_src} (measured bf16 "
                                         f"{peaks.get('bf16_tflops')} TF/s)"},
-            "e2e": {"value": world * N_ENERGIES / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
+            "e2e": {"value": world * ne / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": int(launches),
             "clocks": sampler.summary(),
