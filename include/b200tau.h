@@ -126,6 +126,24 @@ int b200tau_sync(b200tau_ctx *ctx);
 int b200tau_solve_dense(b200tau_ctx *ctx, const double *m, int n, int ldm,
                         const double *t0, int b, int prec, double *tau00);
 
+/* Allocation-free variant of b200tau_solve_dense, for callers that cannot call cudaMalloc:
+ * programs whose GPU memory is owned by another allocator (memory reserved up front for an
+ * application pool, where an allocation inside this library would fail or fragment it) and
+ * latency-critical paths that cannot accept cudaMalloc/cudaFree's implicit synchronisation.
+ * No counterpart in the reference.
+ *   m (n x n, leading dimension ldm, central site first), t0 (b x b) and tau00 (b x b output,
+ *   raw tau00 as b200tau_solve_dense) are DEVICE pointers owned by the caller; the FP64 path
+ *   with one refinement step runs on `stream` (a cudaStream_t, NULL = default stream) and the
+ *   call returns after synchronising that stream.
+ *   No context, no cudaMalloc/cudaFree: all scratch lives in one fixed file-scope device array
+ *   of about 8.9 MB that every GPU loading the library keeps until the process exits.
+ *   Limits: n <= 512, b <= 32; larger sizes return B200TAU_ERR_ARG.
+ *   The array's device address is looked up once per device by the first call on that device,
+ *   so make that first call before any stream capture.  All calls share the array (the call
+ *   clears what must start at zero); calls that overlap on the GPU race and must be serialised. */
+int b200tau_solve_dense_noalloc(const double *m, int n, int ldm, const double *t0, int b,
+                                double *tau00, void *stream);
+
 /* Build only: the KKR matrix M = 1 - t G for one job in the reference's site
  * order (central site first), written to host memory (n x n, ld = n) where
  * n = n_spin_cant * nrmat.  Parity hook for buildKKRMatrix*; not on the hot

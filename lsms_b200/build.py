@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "_lib")
 LIB_PATH = os.path.join(LIB_DIR, "libb200tau.so")
-SOURCES = ["capi.cu", "kkr_build.cu", "block_lu.cu", "tc_update.cu", "angular.cpp"]
+SOURCES = ["capi.cu", "kkr_build.cu", "block_lu.cu", "tc_update.cu", "noalloc.cu", "angular.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -45,7 +45,7 @@ EXPORTS = (
     "b200tau_upload_tmat", "b200tau_set_atom", "b200tau_solve", "b200tau_solve_device",
     "b200tau_sync", "b200tau_solve_dense", "b200tau_build_kkr", "b200tau_last_launch_count",
     "b200tau_gaunt_numbers", "b200tau_set_refinement", "b200tau_set_profiling",
-    "b200tau_profile_read", "b200tau_set_mixed_engine",
+    "b200tau_profile_read", "b200tau_set_mixed_engine", "b200tau_solve_dense_noalloc",
 )
 
 
