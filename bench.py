@@ -255,6 +255,7 @@ def main():
         s.solve_jobs_device(jobs, out.data_ptr(), T.PREC_MIXED)
     s.sync()
     k_ms, k_launches, k_flops = s.profile_read()
+    phases = {k: v / 2.0 for k, v in s.profile_phases().items()}
     s.set_profiling(False)
     peaks, peak_src = measured_peaks()
     achieved = k_flops / (k_ms * 1e-3) / 1e12 if k_ms > 0 else None
@@ -294,10 +295,12 @@ def main():
                                    "31-point semicircle contour -0.3..0.7 Ry, one atom per GPU",
                        "solves_per_step": ne, "l2": "inputs larger than L2 "
                        f"({ne} x {N * N * 16 / 1e6:.0f} MB KKR matrices per step)",
-                       "refinement_steps_mixed": 3, "refinement_steps_fp64": 1},
+                       "refinement_steps_mixed": "up to 6, per job until the correction estimate < 1e-13",
+                       "refinement_steps_fp64": 1},
             "fp64": {"value": fp64_value, "unit": "solves/s", "ms_per_step": ms_fp64,
                      "mixed_over_fp64": value / fp64_value},
             "err_mixed_vs_fp64": err,
+            "phase_ms_per_step_mixed": phases,
             "flops_per_solve": flops_per_solve,
             "effective_tflops_mixed": value * flops_per_solve / 1e12,
             "roofline": {"kernel": "tc_update_kernel + tc_pack_kernel (trailing update A22 -= A21 W, "

@@ -164,6 +164,9 @@ int b200tau_gaunt_numbers(int lmax, double *cgnt);
  * Enabling resets the totals. */
 int b200tau_set_profiling(b200tau_ctx *ctx, int enable);
 int b200tau_profile_read(b200tau_ctx *ctx, double *ms, long *launches, double *flops);
+/* Device time per phase of the solves since profiling was enabled, from CUDA events on the
+ * context stream: ms3[0] KKR build, ms3[1] block elimination, ms3[2] refinement and tau00_l. */
+int b200tau_profile_phases(b200tau_ctx *ctx, double *ms3);
 
 /* Number of kernel launches the last solve issued (for launch accounting). */
 long b200tau_last_launch_count(const b200tau_ctx *ctx);

@@ -19,41 +19,18 @@
 // to the N x b system M X = [0; t0]):
 //   X = F^-1 B;  repeat: R = B - M X (FP64, M unmodified), Y = F^-1 R, X += Y;
 // where F^-1 is a forward sweep (Y_k = D_k R_k, R_below -= A21_k Y_k), the S solve, and a backward
-// sweep (Y_above -= W Y_k), each a kernel per block step over all jobs.  tau00 = X[n:N].
+// sweep (Y_above -= W Y_k), each one launch with a thread-block cluster per job (sweep.cu).
+// tau00 = X[n:N].
 
 #include <cuda_runtime.h>
 
 #include "common.cuh"
+#include "cplx.cuh"
 
 namespace b200 {
 namespace {
 
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
-}
-__device__ __forceinline__ double2 csub(double2 a, double2 b) { return make_double2(a.x - b.x, a.y - b.y); }
-__device__ __forceinline__ double2 cfma(double2 a, double2 b, double2 c) {  // c + a b
-  c.x = fma(a.x, b.x, c.x);
-  c.x = fma(-a.y, b.y, c.x);
-  c.y = fma(a.x, b.y, c.y);
-  c.y = fma(a.y, b.x, c.y);
-  return c;
-}
-__device__ __forceinline__ double cabs1(double2 a) { return fabs(a.x) + fabs(a.y); }
-__device__ __forceinline__ double2 crecip(double2 a) {
-  // 1/a with scaling against overflow of |a|^2
-  const double s = fmax(fabs(a.x), fabs(a.y));
-  const double ar = a.x / s, ai = a.y / s;
-  const double d = ar * ar + ai * ai;
-  return make_double2(ar / (d * s), -ai / (d * s));
-}
-__device__ __forceinline__ double2 ldc(const double2 *p) { return *p; }
-__device__ __forceinline__ double2 ldc(const float2 *p) {
-  const float2 v = *p;
-  return make_double2(v.x, v.y);
-}
-__device__ __forceinline__ void stc(double2 *p, double2 v) { *p = v; }
-__device__ __forceinline__ void stc(float2 *p, double2 v) { *p = make_float2((float)v.x, (float)v.y); }
+using namespace cx;
 
 template <typename S> struct Vec2;
 template <> struct Vec2<double> { using t = double2; };
@@ -82,58 +59,50 @@ __global__ void __launch_bounds__(256) diag_inverse_kernel(const JobDev *__restr
   }
   __syncthreads();
   bool singular = false;
+  (void)s_piv;
+  (void)s_dinv;
+  // column-owner mapping: thread handles column c = tid % NB and rows r0 + q * RS
+  const int c = tid % NB;
+  const int r0 = tid / NB;
+  constexpr int RS = 256 / NB;
+  const int lane = tid & 31;
   for (int p = 0; p < kb; ++p) {
-    if (tid < 32) {  // pivot search |re|+|im| over rows p..kb-1 (izamax convention)
-      double best = -1.0;
-      int bi = p;
-      for (int r = p + tid; r < kb; r += 32) {
-        const double v = cabs1(A[r][p]);
-        if (v > best) {
-          best = v;
-          bi = r;
-        }
-      }
-      for (int o = 16; o > 0; o >>= 1) {
-        const double ob = __shfl_down_sync(0xffffffffu, best, o);
-        const int oi = __shfl_down_sync(0xffffffffu, bi, o);
-        if (ob > best || (ob == best && oi < bi)) {
-          best = ob;
-          bi = oi;
-        }
-      }
-      if (tid == 0) {
-        s_piv = bi;
-        perm[p] = bi;
+    // pivot search |re|+|im| over rows p..kb-1 (izamax convention), done by every warp so that no
+    // barrier is needed to share the result (same data, same reduction order: same answer)
+    double best = -1.0;
+    int bi = p;
+    for (int r = p + lane; r < kb; r += 32) {
+      const double v = cabs1(A[r][p]);
+      if (v > best) {
+        best = v;
+        bi = r;
       }
     }
-    __syncthreads();
-    const int pv = s_piv;
-    if (pv != p)
-      for (int c = tid; c < kb; c += blockDim.x) {
-        const double2 t = A[p][c];
-        A[p][c] = A[pv][c];
-        A[pv][c] = t;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ob > best || (ob == best && oi < bi)) {
+        best = ob;
+        bi = oi;
       }
-    __syncthreads();
-    if (tid == 0) {
-      const double2 d = A[p][p];
-      s_dinv = (d.x == 0.0 && d.y == 0.0) ? make_double2(0.0, 0.0) : crecip(d);
     }
-    __syncthreads();
-    const double2 dinv = s_dinv;
+    const int pv = bi;
+    if (tid == 0) perm[p] = pv;
+    // read phase: the row swap p <-> pv is folded into the reads
+    const double2 d = A[pv][p];
+    const double2 dinv = (d.x == 0.0 && d.y == 0.0) ? make_double2(0.0, 0.0) : crecip(d);
     if (dinv.x == 0.0 && dinv.y == 0.0) singular = true;
-    // column-owner mapping: thread handles column c = tid % NB and rows r0 + q * RS
-    const int c = tid % NB;
-    const int r0 = tid / NB;
-    constexpr int RS = 256 / NB;
-    double2 rowp = make_double2(0.0, 0.0);
-    double2 f[NB / RS];
+    double2 rowp = make_double2(0.0, 0.0);  // new row p, column c
+    double2 f[NB / RS], cur[NB / RS];
     if (c < kb) {
-      rowp = (c == p) ? dinv : cmul(A[p][c], dinv);
+      rowp = (c == p) ? dinv : cmul(A[pv][c], dinv);
 #pragma unroll
       for (int q = 0; q < NB / RS; ++q) {
         const int r = r0 + q * RS;
-        f[q] = (r < kb) ? A[r][p] : make_double2(0.0, 0.0);
+        const int src = (r == pv) ? p : r;  // row r after the swap
+        f[q] = (r < kb) ? A[src][p] : make_double2(0.0, 0.0);
+        cur[q] = (r < kb) ? A[src][c] : make_double2(0.0, 0.0);
       }
     }
     __syncthreads();
@@ -145,7 +114,7 @@ __global__ void __launch_bounds__(256) diag_inverse_kernel(const JobDev *__restr
         if (r == p) {
           A[r][c] = rowp;
         } else {
-          const double2 base = (c == p) ? make_double2(0.0, 0.0) : A[r][c];
+          const double2 base = (c == p) ? make_double2(0.0, 0.0) : cur[q];
           A[r][c] = csub(base, cmul(f[q], rowp));
         }
       }
@@ -183,7 +152,9 @@ constexpr int kKc = 16;
 enum { kOverwrite = 0, kSubtract = 1 };
 
 template <typename S, int MODE>
-__global__ void __launch_bounds__(256) zgemm_tile_kernel(const JobDev *__restrict__ jobs, int k) {
+// Two resident CTAs per SM: with K = 64 per step each CTA runs only four K-chunks, so its operand
+// prologue and C read-modify-write latencies are hidden by the other CTA's FMAs.
+__global__ void __launch_bounds__(256, 2) zgemm_tile_kernel(const JobDev *__restrict__ jobs, int k) {
   using T = typename Vec2<S>::t;
   const JobDev &J = jobs[blockIdx.z];
   const int N = J.N, ld = J.ld;
@@ -435,9 +406,7 @@ __global__ void __launch_bounds__(256) finalize_from_x_kernel(const JobDev *__re
 // ---------------------------------------------------------------------------------------------
 
 // R = B - M X with B = [0; t0] (rows n..N-1 hold t0).  64 rows x b columns per CTA, K in chunks.
-__device__ __forceinline__ bool converged(const JobDev &J) {
-  return J.conv != nullptr && *reinterpret_cast<volatile const int *>(J.conv) != 0;
-}
+__device__ __forceinline__ bool converged(const JobDev &J) { return cx::converged(J.conv); }
 
 __global__ void __launch_bounds__(256) residual_kernel(const JobDev *__restrict__ jobs) {
   const JobDev &J = jobs[blockIdx.y];
@@ -455,18 +424,43 @@ __global__ void __launch_bounds__(256) residual_kernel(const JobDev *__restrict_
   for (int j = 0; j < kMaxB / 4; ++j) acc[j] = make_double2(0.0, 0.0);
   const double2 *__restrict__ M = J.M;
   const double2 *__restrict__ X = J.X;
-  for (int kc = 0; kc < N; kc += KC) {
-    for (int e = tid; e < 64 * KC; e += 256) {
+  // register double buffer: the loads of chunk kc + KC are in flight while chunk kc is consumed
+  constexpr int MQ = 64 * KC / 256;             // M elements per thread per chunk
+  constexpr int XQ = (KC * kMaxB + 255) / 256;  // X elements per thread per chunk
+  double2 rm[MQ], rx[XQ];
+  auto load = [&](int kc) {
+#pragma unroll
+    for (int q = 0; q < MQ; ++q) {
+      const int e = tid + q * 256;
       const int r = e & 63, kk = e >> 6;
       const int gr = row0 + r, gk = kc + kk;
-      Ms[kk][r] = (gr < N && gk < N) ? M[(size_t)gr + (size_t)gk * ld] : make_double2(0.0, 0.0);
+      rm[q] = (gr < N && gk < N) ? M[(size_t)gr + (size_t)gk * ld] : make_double2(0.0, 0.0);
     }
-    for (int e = tid; e < KC * b; e += 256) {
+#pragma unroll
+    for (int q = 0; q < XQ; ++q) {
+      const int e = tid + q * 256;
       const int kk = e % KC, c = e / KC;
       const int gk = kc + kk;
-      Xs[kk][c] = (gk < N) ? X[(size_t)gk + (size_t)c * ld] : make_double2(0.0, 0.0);
+      rx[q] = (c < b && gk < N) ? X[(size_t)gk + (size_t)c * ld] : make_double2(0.0, 0.0);
     }
-    __syncthreads();
+  };
+  auto store = [&]() {
+#pragma unroll
+    for (int q = 0; q < MQ; ++q) {
+      const int e = tid + q * 256;
+      Ms[e >> 6][e & 63] = rm[q];
+    }
+#pragma unroll
+    for (int q = 0; q < XQ; ++q) {
+      const int e = tid + q * 256;
+      if (e < KC * kMaxB) Xs[e % KC][e / KC] = rx[q];
+    }
+  };
+  load(0);
+  store();
+  __syncthreads();
+  for (int kc = 0; kc < N; kc += KC) {
+    if (kc + KC < N) load(kc + KC);
 #pragma unroll 4
     for (int kk = 0; kk < KC; ++kk) {
       const double2 a = Ms[kk][tr];
@@ -476,6 +470,8 @@ __global__ void __launch_bounds__(256) residual_kernel(const JobDev *__restrict_
         if (c < b) acc[j] = cfma(a, Xs[kk][c], acc[j]);
       }
     }
+    __syncthreads();
+    if (kc + KC < N) store();
     __syncthreads();
   }
   const int gr = row0 + tr;
@@ -487,73 +483,6 @@ __global__ void __launch_bounds__(256) residual_kernel(const JobDev *__restrict_
     const double2 bv = (gr >= J.n) ? J.t0[(gr - J.n) + (size_t)c * J.t0_ld] : make_double2(0.0, 0.0);
     J.R[(size_t)gr + (size_t)c * ld] = csub(bv, acc[j]);
   }
-}
-
-// Forward sweep, step k: Y_k = D_k R_k (every CTA computes it; CTA 0 stores it), then
-// R[rows] -= A21_k Y_k for this CTA's 64 rows of [k + kb, N).
-template <typename T>
-__global__ void __launch_bounds__(256) forward_step_kernel(const JobDev *__restrict__ jobs, int k) {
-  const JobDev &J = jobs[blockIdx.y];
-  if (k >= J.n || converged(J)) return;
-  const int kb = min(kNb, J.n - k);
-  const int N = J.N, ld = J.ld, b = J.b;
-  const int row0 = k + kb + blockIdx.x * 64;
-  if (row0 >= N && blockIdx.x != 0) return;
-  const T *__restrict__ F = static_cast<const T *>(J.F);
-  // dynamic smem: Ds[j][r] (D_k, kb x kb, column-major), Rs[j][c] (R_k), Ys[r][c] (Y_k)
-  extern __shared__ __align__(16) unsigned char fsm[];
-  T *Ds = reinterpret_cast<T *>(fsm);
-  double2 *Rs = reinterpret_cast<double2 *>(fsm + sizeof(T) * kNb * kNb);
-  double2(*Ys)[kMaxB] = reinterpret_cast<double2(*)[kMaxB]>(fsm + sizeof(T) * kNb * kNb +
-                                                              sizeof(double2) * kNb * kMaxB);
-  const int tid = threadIdx.x;
-  for (int e = tid; e < kb * kb; e += 256) {
-    const int r = e % kb, j = e / kb;
-    Ds[j * kNb + r] = F[(size_t)(k + r) + (size_t)(k + j) * ld];
-  }
-  for (int e = tid; e < kb * b; e += 256) {
-    const int r = e % kb, c = e / kb;
-    Rs[c * kNb + r] = J.R[(size_t)(k + r) + (size_t)c * ld];
-  }
-  __syncthreads();
-  for (int e = tid; e < kb * b; e += 256) {
-    const int r = e % kb, c = e / kb;
-    double2 s = make_double2(0.0, 0.0);
-#pragma unroll 8
-    for (int j = 0; j < kb; ++j) s = cfma(ldc(&Ds[j * kNb + r]), Rs[c * kNb + j], s);
-    Ys[r][c] = s;
-    if (blockIdx.x == 0) J.Y[(size_t)(k + r) + (size_t)c * ld] = s;
-  }
-  __syncthreads();
-  if (row0 >= N) return;
-  const int tr = tid & 63, tc = tid >> 6;
-  const int gr = row0 + tr;
-  if (gr >= N) return;
-  double2 acc[kMaxB / 4];
-#pragma unroll
-  for (int j = 0; j < kMaxB / 4; ++j) acc[j] = make_double2(0.0, 0.0);
-  const T *lrow = F + (size_t)gr + (size_t)k * ld;
-#pragma unroll 8
-  for (int jj = 0; jj < kb; ++jj) {
-    const double2 a = ldc(lrow + (size_t)jj * ld);
-#pragma unroll
-    for (int j = 0; j < kMaxB / 4; ++j) {
-      const int c = tc + 4 * j;
-      if (c < b) acc[j] = cfma(a, Ys[jj][c], acc[j]);
-    }
-  }
-#pragma unroll
-  for (int j = 0; j < kMaxB / 4; ++j) {
-    const int c = tc + 4 * j;
-    if (c >= b) continue;
-    double2 *dst = J.R + (size_t)gr + (size_t)c * ld;
-    *dst = csub(*dst, acc[j]);
-  }
-}
-
-template <typename T>
-constexpr int forward_smem_bytes() {
-  return (int)(sizeof(T) * kNb * kNb + 2 * sizeof(double2) * kNb * kMaxB);
 }
 
 // Y[n:N] = S^-1 rhs with rhs = R[n:N] (mode 1) or t0 (mode 0, which also zeroes Y[0:n]).
@@ -582,68 +511,6 @@ __global__ void __launch_bounds__(256) schur_solve_kernel(const JobDev *__restri
   for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
     const int c = e / b, r = e - c * b;
     J.Y[(size_t)(n + r) + (size_t)c * ld] = A[r][b + c];
-  }
-}
-
-// Backward sweep for the block of rows [k, k + kb): CTA 0 sets X_k = Y_k (mode 0) or X_k += Y_k
-// (mode 1); every CTA applies Y[rows] -= W[rows, k:k+kb] Y_k for its 64 rows of [0, k).
-// `central` selects the trailing b-row block (k = n, kb = b).
-template <typename T>
-__global__ void __launch_bounds__(256) backward_step_kernel(const JobDev *__restrict__ jobs, int k,
-                                                            int central, int mode) {
-  const JobDev &J = jobs[blockIdx.y];
-  if (mode == 1 && converged(J)) return;
-  int kb;
-  if (central) {
-    k = J.n;
-    kb = J.b;
-  } else {
-    if (k >= J.n) return;
-    kb = min(kNb, J.n - k);
-  }
-  const int ld = J.ld, b = J.b;
-  const int row0 = blockIdx.x * 64;
-  if (row0 >= k && blockIdx.x != 0) return;
-  __shared__ double2 Ys[kNb][kMaxB];
-  const int tid = threadIdx.x;
-  for (int e = tid; e < kb * b; e += 256) {
-    const int r = e % kb, c = e / kb;
-    const size_t idx = (size_t)(k + r) + (size_t)c * ld;
-    const double2 y = J.Y[idx];
-    Ys[r][c] = y;
-    if (blockIdx.x == 0) {
-      if (mode == 0) {
-        J.X[idx] = y;
-      } else {
-        const double2 x = J.X[idx];
-        J.X[idx] = make_double2(x.x + y.x, x.y + y.y);
-      }
-    }
-  }
-  __syncthreads();
-  if (row0 >= k) return;
-  const T *__restrict__ F = static_cast<const T *>(J.F);
-  const int tr = tid & 63, tc = tid >> 6;
-  const int gr = row0 + tr;
-  if (gr >= k) return;
-  double2 acc[kMaxB / 4];
-#pragma unroll
-  for (int j = 0; j < kMaxB / 4; ++j) acc[j] = make_double2(0.0, 0.0);
-  const T *urow = F + (size_t)gr + (size_t)k * ld;
-  for (int jj = 0; jj < kb; ++jj) {
-    const double2 a = ldc(urow + (size_t)jj * ld);
-#pragma unroll
-    for (int j = 0; j < kMaxB / 4; ++j) {
-      const int c = tc + 4 * j;
-      if (c < b) acc[j] = cfma(a, Ys[jj][c], acc[j]);
-    }
-  }
-#pragma unroll
-  for (int j = 0; j < kMaxB / 4; ++j) {
-    const int c = tc + 4 * j;
-    if (c >= b) continue;
-    double2 *dst = J.Y + (size_t)gr + (size_t)c * ld;
-    *dst = csub(*dst, acc[j]);
   }
 }
 
@@ -685,31 +552,25 @@ cudaError_t eliminate_impl(const JobDev *jobs, int njobs, int max_n, int max_N, 
 }
 
 template <typename T>
-void sweep_solve(const JobDev *jobs, int njobs, int max_n, int max_N, int mode, int *info, cudaStream_t s,
-                 long *launches) {
+cudaError_t sweep_solve(const JobDev *jobs, int njobs, int b, int mode, int *info, cudaStream_t s,
+                        long *launches) {
+  const FactorKind fk = sizeof(T) == sizeof(double2) ? kFactorFP64 : kFactorFP32;
+  cudaError_t e;
   // forward (skipped for the initial solve: B is zero above the central block)
   if (mode == 1) {
-    constexpr int fsmem = forward_smem_bytes<T>();
-    cudaFuncSetAttribute(forward_step_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsmem);
-    for (int k = 0; k < max_n; k += kNb) {
-      const int tiles = (max_N - k - 1) / 64 + 1;
-      forward_step_kernel<T><<<dim3(tiles, njobs), 256, fsmem, s>>>(jobs, k);
-      if (launches) *launches += 1;
-    }
-  }
-  schur_solve_kernel<T><<<njobs, 256, 0, s>>>(jobs, mode, info);
-  backward_step_kernel<T><<<dim3((max_n + 63) / 64 + 1, njobs), 256, 0, s>>>(jobs, 0, 1, mode);
-  if (launches) *launches += 2;
-  const int last = ((max_n - 1) / kNb) * kNb;
-  for (int k = last; k >= 0; k -= kNb) {
-    backward_step_kernel<T><<<dim3(k / 64 + 1, njobs), 256, 0, s>>>(jobs, k, 0, mode);
+    if ((e = launch_sweep(fk, jobs, njobs, b, true, mode, s)) != cudaSuccess) return e;
     if (launches) *launches += 1;
   }
+  schur_solve_kernel<T><<<njobs, 256, 0, s>>>(jobs, mode, info);
+  if ((e = launch_sweep(fk, jobs, njobs, b, false, mode, s)) != cudaSuccess) return e;
+  if (launches) *launches += 2;
+  return cudaSuccess;
 }
 
-// After a refinement round: the job is converged when the correction just applied to the tau00
-// block is below tol x max|tau00| (the error left after applying it is smaller still, by the
-// contraction factor of the refinement), and later rounds skip it.
+// After a refinement round: c = max|correction| / max|tau00| on the tau00 block.  The error left
+// after applying the correction is about c times the contraction factor of the refinement,
+// estimated as c / c_prev from the previous round; the job is converged when c * min(1, c / c_prev)
+// is below tol, and later rounds skip it.
 __global__ void __launch_bounds__(256) converge_check_kernel(const JobDev *__restrict__ jobs, double tol) {
   const JobDev &J = jobs[blockIdx.x];
   if (J.conv == nullptr || converged(J)) return;
@@ -732,7 +593,13 @@ __global__ void __launch_bounds__(256) converge_check_kernel(const JobDev *__res
     }
     __syncthreads();
   }
-  if (threadIdx.x == 0 && sy[0] <= tol * sx[0]) *J.conv = 1;
+  if (threadIdx.x == 0) {
+    const double c = sx[0] > 0.0 ? sy[0] / sx[0] : 0.0;
+    const double prev = J.cnorm ? *J.cnorm : 0.0;
+    const double est = prev > 0.0 ? c * fmin(1.0, c / prev) : c;
+    if (est <= tol) *J.conv = 1;
+    if (J.cnorm) *J.cnorm = c;
+  }
 }
 
 template <typename T>
@@ -777,26 +644,43 @@ cudaError_t launch_finalize_direct(FactorKind fk, const JobDev *jobs, int njobs,
   return cudaGetLastError();
 }
 
-cudaError_t launch_solve_refine(FactorKind fk, const JobDev *jobs, int njobs, int max_n, int max_N, int b,
-                                int steps, int ns, int kkrsz, int *info, cudaStream_t s, long *launches) {
-  (void)b;
-  auto solve = [&](int mode) {
-    if (fk == kFactorFP64) sweep_solve<double2>(jobs, njobs, max_n, max_N, mode, info, s, launches);
-    else sweep_solve<float2>(jobs, njobs, max_n, max_N, mode, info, s, launches);
-  };
-  solve(0);
-  for (int it = 0; it < steps; ++it) {
-    residual_kernel<<<dim3((max_N + 63) / 64, njobs), 256, 0, s>>>(jobs);
+cudaError_t launch_refine_begin(FactorKind fk, const JobDev *jobs, int njobs, int max_n, int max_N, int b,
+                                int *info, cudaStream_t s, long *launches) {
+  (void)max_n;
+  (void)max_N;
+  const cudaError_t e = fk == kFactorFP64 ? sweep_solve<double2>(jobs, njobs, b, 0, info, s, launches)
+                                           : sweep_solve<float2>(jobs, njobs, b, 0, info, s, launches);
+  return e != cudaSuccess ? e : cudaGetLastError();
+}
+
+cudaError_t launch_refine_round(FactorKind fk, const JobDev *jobs, int njobs, int max_n, int max_N, int b,
+                                bool check, int *info, cudaStream_t s, long *launches) {
+  (void)max_n;
+  residual_kernel<<<dim3((max_N + 63) / 64, njobs), 256, 0, s>>>(jobs);
+  if (launches) *launches += 1;
+  const cudaError_t e = fk == kFactorFP64 ? sweep_solve<double2>(jobs, njobs, b, 1, info, s, launches)
+                                           : sweep_solve<float2>(jobs, njobs, b, 1, info, s, launches);
+  if (e != cudaSuccess) return e;
+  if (check) {
+    converge_check_kernel<<<njobs, 256, 0, s>>>(jobs, 1e-13);
     if (launches) *launches += 1;
-    solve(1);
-    if (it + 1 < steps) {
-      converge_check_kernel<<<njobs, 256, 0, s>>>(jobs, 1e-13);
-      if (launches) *launches += 1;
-    }
   }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_refine_end(const JobDev *jobs, int njobs, int ns, int kkrsz, cudaStream_t s, long *launches) {
   finalize_from_x_kernel<<<njobs, 256, 0, s>>>(jobs, ns, kkrsz);
   if (launches) *launches += 1;
   return cudaGetLastError();
+}
+
+cudaError_t launch_solve_refine(FactorKind fk, const JobDev *jobs, int njobs, int max_n, int max_N, int b,
+                                int steps, int ns, int kkrsz, int *info, cudaStream_t s, long *launches) {
+  cudaError_t e = launch_refine_begin(fk, jobs, njobs, max_n, max_N, b, info, s, launches);
+  for (int it = 0; it < steps && e == cudaSuccess; ++it)
+    e = launch_refine_round(fk, jobs, njobs, max_n, max_N, b, it + 1 < steps, info, s, launches);
+  if (e != cudaSuccess) return e;
+  return launch_refine_end(jobs, njobs, ns, kkrsz, s, launches);
 }
 
 }  // namespace b200

@@ -68,21 +68,32 @@ struct b200tau_ctx {
   int slots = 0;
   JobDev *d_jobs = nullptr;
   int jobs_cap = 0;
-  int *d_info = nullptr;   // per slot
+  JobDev *d_jobs2 = nullptr;  // the jobs still refining after compaction (at most `slots`)
+  int jobs2_cap = 0;
+  int *d_info = nullptr;   // 2 x slots: the wave's jobs, then the compacted list
   int *d_conv = nullptr;   // per slot: refinement converged
+  double *d_cnorm = nullptr;  // per slot: relative size of the last refinement correction
   int *d_err = nullptr;    // device error flags
   double2 *d_out = nullptr;
   size_t out_cap = 0;
   double2 *d_t0 = nullptr;  // dense-solve t0
+  unsigned char *d_tdiag = nullptr;  // per (store, energy, spin) t block: exactly diagonal
   long launches = 0;
   int max_slots = 64;
-  int refine_steps[2] = {1, 3};  // FP64, MIXED
+  // refinement rounds, FP64 and MIXED; MIXED stops early per job once the correction estimate
+  // is below 1e-13 of tau00 (block_lu.cu, converge_check_kernel)
+  int refine_steps[2] = {1, 6};
   // profiling of the trailing-update launches (b200tau_set_profiling)
   bool profiling = false;
   std::vector<cudaEvent_t> events;
   KernelTimer timer;
   double prof_ms = 0.0, prof_flops = 0.0;
   long prof_launches = 0;
+  // phase timing (b200tau_profile_phases): event pairs around build, elimination, refinement
+  std::vector<cudaEvent_t> pev;
+  std::vector<int> pev_phase;
+  int pev_used = 0;
+  double phase_ms[3] = {0.0, 0.0, 0.0};
   // tensor-core trailing update of the mixed path: operand packs + TMA descriptors
   int mixed_engine = B200TAU_ENGINE_TENSOR;
   TcMaps tc;
@@ -146,11 +157,13 @@ int ensure_workspace(b200tau_ctx *ctx, int ld, int slots, const Plan &p) {
   cudaFree(ctx->d_vec);
   cudaFree(ctx->d_info);
   cudaFree(ctx->d_conv);
+  cudaFree(ctx->d_cnorm);
   ctx->d_M = nullptr;
   ctx->d_F = nullptr;
   ctx->d_vec = nullptr;
   ctx->d_info = nullptr;
   ctx->d_conv = nullptr;
+  ctx->d_cnorm = nullptr;
   const size_t m_el = std::max(m_need, ctx->m_elems);
   const size_t f_b = std::max(f_need, ctx->f_bytes);
   const size_t v_el = std::max(v_need, ctx->vec_elems);
@@ -158,8 +171,9 @@ int ensure_workspace(b200tau_ctx *ctx, int ld, int slots, const Plan &p) {
   CK(cudaMalloc(&ctx->d_M, m_el * sl * sizeof(double2)));
   if (f_b) CK(cudaMalloc(&ctx->d_F, f_b * sl));
   CK(cudaMalloc(&ctx->d_vec, v_el * sl * sizeof(double2)));
-  CK(cudaMalloc(&ctx->d_info, sizeof(int) * sl));
+  CK(cudaMalloc(&ctx->d_info, sizeof(int) * 2 * sl));
   CK(cudaMalloc(&ctx->d_conv, sizeof(int) * sl));
+  CK(cudaMalloc(&ctx->d_cnorm, sizeof(double) * sl));
   ctx->m_elems = m_el;
   ctx->f_bytes = f_b;
   ctx->vec_elems = v_el;
@@ -208,6 +222,17 @@ void fill_slot(b200tau_ctx *ctx, JobDev &J, int slot, int ld, const Plan &p) {
   J.Y = v + (size_t)2 * ld * kMaxB;
   J.ld = ld;
   J.conv = ctx->d_conv + slot;
+  J.cnorm = ctx->d_cnorm + slot;
+}
+
+// Clears the per-slot status of the first nw slots: singular-pivot info, converged flag, last
+// correction size.
+int reset_slot_status(b200tau_ctx *ctx, int nw) {
+  CK(cudaMemsetAsync(ctx->d_info, 0, sizeof(int) * nw, ctx->stream));
+  CK(cudaMemsetAsync(ctx->d_info + ctx->slots, 0, sizeof(int) * nw, ctx->stream));
+  CK(cudaMemsetAsync(ctx->d_conv, 0, sizeof(int) * nw, ctx->stream));
+  CK(cudaMemsetAsync(ctx->d_cnorm, 0, sizeof(double) * nw, ctx->stream));
+  return B200TAU_OK;
 }
 
 BuildParams build_params(const b200tau_ctx *ctx, const Plan &p) {
@@ -220,7 +245,43 @@ BuildParams build_params(const b200tau_ctx *ctx, const Plan &p) {
   bp.ns = ctx->ns;
   bp.npola = ctx->npola;
   bp.f_kind = !p.f_separate ? 0 : (p.fk == kFactorFP32 ? 2 : 1);
+  bp.tdiag = ctx->d_tdiag;
+  bp.group = ctx->group_size;
   return bp;
+}
+
+// Phase timing: an event before and after each phase on the context stream, read back by
+// b200tau_profile_phases.  Phases: 0 KKR build, 1 block elimination, 2 refinement and tau00_l.
+int drain_phases(b200tau_ctx *ctx);
+
+int phase_begin(b200tau_ctx *ctx) {
+  if (!ctx->profiling || ctx->pev.empty()) return B200TAU_OK;
+  if (ctx->pev_used + 2 > (int)ctx->pev.size()) {
+    int rc = drain_phases(ctx);
+    if (rc) return rc;
+  }
+  CK(cudaEventRecord(ctx->pev[ctx->pev_used], ctx->stream));
+  return B200TAU_OK;
+}
+
+int phase_end(b200tau_ctx *ctx, int phase) {
+  if (!ctx->profiling || ctx->pev.empty()) return B200TAU_OK;
+  CK(cudaEventRecord(ctx->pev[ctx->pev_used + 1], ctx->stream));
+  ctx->pev_phase[ctx->pev_used / 2] = phase;
+  ctx->pev_used += 2;
+  return B200TAU_OK;
+}
+
+int drain_phases(b200tau_ctx *ctx) {
+  if (ctx->pev_used == 0) return B200TAU_OK;
+  CK(cudaStreamSynchronize(ctx->stream));
+  for (int i = 0; i + 1 < ctx->pev_used; i += 2) {
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, ctx->pev[i], ctx->pev[i + 1]));
+    ctx->phase_ms[ctx->pev_phase[i / 2]] += ms;
+  }
+  ctx->pev_used = 0;
+  return B200TAU_OK;
 }
 
 // Device pipeline for one wave whose JobDev records are already in ctx->d_jobs.
@@ -320,7 +381,61 @@ double trailing_flops(const std::vector<JobDev> &h) {
   return f;
 }
 
-int run_pipeline(b200tau_ctx *ctx, int nw, int maxn, int maxN, int ld, int ns, int kkrsz, const Plan &p) {
+// Refinement rounds run on every job of the wave until this many are done; then the host reads the
+// converged flags once and the remaining rounds run on the unconverged jobs only.
+constexpr int kCompactAfterRounds = 2;
+
+int ensure_jobs2(b200tau_ctx *ctx, int n) {
+  if (n <= ctx->jobs2_cap) return B200TAU_OK;
+  cudaFree(ctx->d_jobs2);
+  ctx->d_jobs2 = nullptr;
+  CK(cudaMalloc(&ctx->d_jobs2, sizeof(JobDev) * n));
+  ctx->jobs2_cap = n;
+  return B200TAU_OK;
+}
+
+// Initial solve, `p.steps` refinement rounds (converged jobs skip the later ones, and are dropped
+// from the launches after kCompactAfterRounds), tau00_l.  `h` are the wave's records as uploaded
+// to ctx->d_jobs.
+int run_refinement(b200tau_ctx *ctx, const std::vector<JobDev> &h, int nw, int maxn, int maxN, int b, int ns,
+                   int kkrsz, const Plan &p) {
+  CK(launch_refine_begin(p.fk, ctx->d_jobs, nw, maxn, maxN, b, ctx->d_info, ctx->stream, &ctx->launches));
+  const JobDev *cur = ctx->d_jobs;
+  int ncur = nw, cmaxn = maxn, cmaxN = maxN;
+  int *cur_info = ctx->d_info;
+  for (int it = 0; it < p.steps; ++it) {
+    if (it == kCompactAfterRounds) {
+      std::vector<int> conv(nw);
+      CK(cudaMemcpyAsync(conv.data(), ctx->d_conv, sizeof(int) * nw, cudaMemcpyDeviceToHost, ctx->stream));
+      CK(cudaStreamSynchronize(ctx->stream));
+      std::vector<JobDev> keep;
+      cmaxn = cmaxN = 0;
+      for (int w = 0; w < nw; ++w)
+        if (!conv[w]) {
+          keep.push_back(h[w]);
+          cmaxn = std::max(cmaxn, h[w].n);
+          cmaxN = std::max(cmaxN, h[w].N);
+        }
+      if (keep.empty()) break;
+      if ((int)keep.size() < nw) {
+        int rc = ensure_jobs2(ctx, ctx->slots);
+        if (rc) return rc;
+        CK(cudaMemcpyAsync(ctx->d_jobs2, keep.data(), sizeof(JobDev) * keep.size(), cudaMemcpyHostToDevice,
+                           ctx->stream));
+        cur = ctx->d_jobs2;
+        ncur = (int)keep.size();
+        cur_info = ctx->d_info + ctx->slots;  // the compacted list's own pivot flags
+      }
+    }
+    CK(launch_refine_round(p.fk, cur, ncur, cmaxn, cmaxN, b, it + 1 < p.steps, cur_info, ctx->stream,
+                           &ctx->launches));
+  }
+  CK(launch_refine_end(ctx->d_jobs, nw, ns, kkrsz, ctx->stream, &ctx->launches));
+  return B200TAU_OK;
+}
+
+int run_pipeline(b200tau_ctx *ctx, const std::vector<JobDev> &h, int nw, int maxn, int maxN, int ld, int ns,
+                 int kkrsz, int b, const Plan &p) {
   if (ctx->profiling && ctx->timer.used + 4 * (maxn / kNb + 2) > ctx->timer.cap) {
     int rc = drain_timer(ctx);
     if (rc) return rc;
@@ -333,15 +448,17 @@ int run_pipeline(b200tau_ctx *ctx, int nw, int maxn, int maxN, int ld, int ns, i
     if ((rc = encode_factor_map(ctx, ld, ctx->slots))) return rc;
     tc = &ctx->tc;
   }
+  int rc = phase_begin(ctx);
+  if (rc) return rc;
   CK(launch_eliminate(p.fk, ctx->d_jobs, nw, maxn, maxN, ctx->d_info, ctx->stream, &ctx->launches,
                       ctx->profiling ? &ctx->timer : nullptr, tc, ctx->d_err));
+  if ((rc = phase_end(ctx, 1)) || (rc = phase_begin(ctx))) return rc;
   if (p.steps > 0) {
-    CK(launch_solve_refine(p.fk, ctx->d_jobs, nw, maxn, maxN, ctx->b, p.steps, ns, kkrsz, ctx->d_info,
-                           ctx->stream, &ctx->launches));
+    if ((rc = run_refinement(ctx, h, nw, maxn, maxN, b, ns, kkrsz, p))) return rc;
   } else {
     CK(launch_finalize_direct(p.fk, ctx->d_jobs, nw, ns, kkrsz, ctx->d_info, ctx->stream, &ctx->launches));
   }
-  return B200TAU_OK;
+  return phase_end(ctx, 2);
 }
 
 int run_wave(b200tau_ctx *ctx, const b200tau_job *jobs, const int *idx, int nw, int ld, const Plan &p,
@@ -381,11 +498,12 @@ int run_wave(b200tau_ctx *ctx, const b200tau_job *jobs, const int *idx, int nw, 
     maxn = std::max(maxn, a.N - a.b);
   }
   CK(cudaMemcpyAsync(ctx->d_jobs, h.data(), sizeof(JobDev) * nw, cudaMemcpyHostToDevice, ctx->stream));
-  CK(cudaMemsetAsync(ctx->d_info, 0, sizeof(int) * nw, ctx->stream));
-  CK(cudaMemsetAsync(ctx->d_conv, 0, sizeof(int) * nw, ctx->stream));
+  int rc = reset_slot_status(ctx, nw);
+  if (rc || (rc = phase_begin(ctx))) return rc;
   CK(launch_kkr_build(ctx->d_jobs, nw, maxL, build_params(ctx, p), ctx->d_err, ctx->stream, &ctx->launches));
+  if ((rc = phase_end(ctx, 0))) return rc;
   if (ctx->profiling) ctx->prof_flops += trailing_flops(h);
-  return run_pipeline(ctx, nw, maxn, maxN, ld, ctx->ns, ctx->kkrsz, p);
+  return run_pipeline(ctx, h, nw, maxn, maxN, ld, ctx->ns, ctx->kkrsz, ctx->b, p);
 }
 
 int check_info(b200tau_ctx *ctx, const std::vector<int> &info, const int *idx, int nw) {
@@ -513,13 +631,17 @@ void b200tau_destroy(b200tau_ctx *ctx) {
   cudaFree(ctx->d_F);
   cudaFree(ctx->d_vec);
   cudaFree(ctx->d_jobs);
+  cudaFree(ctx->d_jobs2);
   cudaFree(ctx->d_info);
   cudaFree(ctx->d_conv);
+  cudaFree(ctx->d_cnorm);
   cudaFree(ctx->d_err);
   cudaFree(ctx->d_out);
   cudaFree(ctx->d_t0);
+  cudaFree(ctx->d_tdiag);
   cudaFree(ctx->d_pack);
   for (auto &e : ctx->events) cudaEventDestroy(e);
+  for (auto &e : ctx->pev) cudaEventDestroy(e);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -546,10 +668,25 @@ int b200tau_set_profiling(b200tau_ctx *ctx, int enable) {
     ctx->timer.ev = ctx->events.data();
     ctx->timer.cap = (int)ctx->events.size();
   }
+  if (enable && ctx->pev.empty()) {
+    ctx->pev.resize(512);
+    for (auto &e : ctx->pev) CK(cudaEventCreate(&e));
+    ctx->pev_phase.assign(ctx->pev.size() / 2, 0);
+  }
   ctx->timer.used = 0;
+  ctx->pev_used = 0;
   ctx->profiling = enable != 0;
   ctx->prof_ms = ctx->prof_flops = 0.0;
   ctx->prof_launches = 0;
+  for (double &m : ctx->phase_ms) m = 0.0;
+  return B200TAU_OK;
+}
+
+int b200tau_profile_phases(b200tau_ctx *ctx, double *ms3) {
+  if (!ctx || !ms3) return B200TAU_ERR_ARG;
+  int rc = drain_phases(ctx);
+  if (rc) return rc;
+  for (int i = 0; i < 3; ++i) ms3[i] = ctx->phase_ms[i];
   return B200TAU_OK;
 }
 
@@ -594,10 +731,33 @@ int b200tau_upload_tmat(b200tau_ctx *ctx, const double *tmat_store, long ld, int
     CK(cudaMalloc(&ctx->d_tmat, bytes));
   }
   CK(cudaMemcpyAsync(ctx->d_tmat, tmat_store, bytes, cudaMemcpyHostToDevice, ctx->stream));
+  // Which t blocks are exactly diagonal (no spin-orbit or non-spherical coupling): the KKR build
+  // then forms the block row t_i G_ij from the diagonal alone.  One flag per (store, energy, spin).
+  const int group = (int)(ld / blk_size);
+  const bool colpol = ctx->npola != ctx->ns;
+  const int b = ctx->b, kk = ctx->kkrsz;
+  std::vector<unsigned char> flags((size_t)nstore * group * 2, 0);
+  for (int s = 0; s < nstore; ++s)
+    for (int ie = 0; ie < group; ++ie)
+      for (int sp = 0; sp < (colpol ? 2 : 1); ++sp) {
+        const double *t = tmat_store + 2 * ((size_t)s * ld + (size_t)ie * blk_size + (colpol ? kk * kk * sp : 0));
+        bool diag = true;
+        for (int c = 0; c < b && diag; ++c)
+          for (int r = 0; r < b; ++r)
+            if (r != c && (t[2 * (r + (size_t)c * b)] != 0.0 || t[2 * (r + (size_t)c * b) + 1] != 0.0)) {
+              diag = false;
+              break;
+            }
+        flags[((size_t)s * group + ie) * 2 + sp] = diag ? 1 : 0;
+      }
   CK(cudaStreamSynchronize(ctx->stream));
+  cudaFree(ctx->d_tdiag);
+  ctx->d_tdiag = nullptr;
+  CK(cudaMalloc(&ctx->d_tdiag, flags.size()));
+  CK(cudaMemcpy(ctx->d_tdiag, flags.data(), flags.size(), cudaMemcpyHostToDevice));
   ctx->tmat_ld = ld;
   ctx->nstore = nstore;
-  ctx->group_size = (int)(ld / blk_size);
+  ctx->group_size = group;
   return B200TAU_OK;
 }
 
@@ -737,10 +897,9 @@ int b200tau_solve_dense(b200tau_ctx *ctx, const double *m, int n, int ldm, const
   J.out = ctx->d_out;
   J.out_mode = 1;
   CK(cudaMemcpyAsync(ctx->d_jobs, &J, sizeof(J), cudaMemcpyHostToDevice, ctx->stream));
-  CK(cudaMemsetAsync(ctx->d_info, 0, sizeof(int), ctx->stream));
-  CK(cudaMemsetAsync(ctx->d_conv, 0, sizeof(int), ctx->stream));
+  if ((rc = reset_slot_status(ctx, 1))) return rc;
   ctx->launches = 0;
-  if ((rc = run_pipeline(ctx, 1, r, n, ld, 1, b, p))) return rc;
+  if ((rc = run_pipeline(ctx, std::vector<JobDev>{J}, 1, r, n, ld, 1, b, b, p))) return rc;
   int info = 0;
   CK(cudaMemcpyAsync(&info, ctx->d_info, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaMemcpyAsync(tau00, ctx->d_out, es * b * b, cudaMemcpyDeviceToHost, ctx->stream));

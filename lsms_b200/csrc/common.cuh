@@ -69,6 +69,7 @@ struct JobDev {
   const double2 *t0;     // central t-matrix (b x b, ld t0_ld)
   double2 *out;          // b*b complex result
   int *conv;             // refinement converged flag (set on the device, skips later rounds)
+  double *cnorm;         // relative size of the previous refinement correction (0 before round 1)
   double2 ubr[4];
   double2 ubrd[4];
   int L, N, n, b;
@@ -88,6 +89,8 @@ struct BuildParams {
   int ns;                       // n_spin_cant
   int npola;                    // n_spin_pola
   int f_kind;                   // 0: no F copy (F aliases M), 1: FP64 copy, 2: FP32 copy
+  const unsigned char *tdiag;   // [(store * group + iie) * 2 + ispin]: t block exactly diagonal
+  int group;                    // energies in the uploaded tmatStore group
 };
 
 enum FactorKind { kFactorFP64 = 0, kFactorFP32 = 1 };
@@ -133,5 +136,16 @@ cudaError_t launch_finalize_direct(FactorKind fk, const JobDev *jobs, int njobs,
 cudaError_t launch_solve_refine(FactorKind fk, const JobDev *jobs, int njobs, int max_n, int max_N,
                                 int b, int steps, int ns, int kkrsz, int *info, cudaStream_t s,
                                 long *launches);
+// The same in pieces, for a driver that drops converged jobs between rounds: the initial solve
+// X = F^-1 [0; t0], one refinement round (with the convergence check when `check`), and tau00_l.
+cudaError_t launch_refine_begin(FactorKind fk, const JobDev *jobs, int njobs, int max_n, int max_N, int b,
+                                int *info, cudaStream_t s, long *launches);
+cudaError_t launch_refine_round(FactorKind fk, const JobDev *jobs, int njobs, int max_n, int max_N, int b,
+                                bool check, int *info, cudaStream_t s, long *launches);
+cudaError_t launch_refine_end(const JobDev *jobs, int njobs, int ns, int kkrsz, cudaStream_t s, long *launches);
+// One block sweep of the correction solve for all jobs, one 8-CTA cluster per job (sweep.cu):
+// forward (R -> Y over the D_k, A21_k factors) or backward (Y over the W_k factors, X (+)= Y).
+cudaError_t launch_sweep(FactorKind fk, const JobDev *jobs, int njobs, int b, bool forward, int mode,
+                         cudaStream_t s);
 
 }  // namespace b200

@@ -258,6 +258,26 @@ __global__ void __launch_bounds__(kThreads)
         p.tmat + (long)J.store[i] * p.tmat_ld + (long)J.iie * p.blk + jsm;
     const int r_lo = lane & 15;
     const int c_par = lane >> 4;
+    const bool tdiag = p.tdiag != nullptr && p.tdiag[((long)J.store[i] * p.group + J.iie) * 2 + J.ispin] != 0;
+    if (tdiag) {
+      // t_i diagonal (spherical scatterer): M[(s, r'), (s', c')] = -delta_ss' t_rr G[r', c']
+      for (int rr = r_lo; rr < nr; rr += 16) {
+        const int sr = rr / kki, rp = rr - sr * kki;
+        const int trow = sr * kkrsz + rp;
+        const double2 tr = __ldg(tb + trow + (long)trow * bstore);
+        for (int sc = 0; sc < ns; ++sc)
+          for (int cp = c_par; cp < kkj; cp += 2) {
+            double2 v = make_double2(0.0, 0.0);
+            if (sc == sr) {  // the general path's one nonzero term, rounded the same way
+              const double2 pr = cfma(tr, sm.G[warp][rp * kMaxKK + cp], make_double2(0.0, 0.0));
+              v = make_double2(-pr.x, -pr.y);
+            }
+            put((size_t)(row0 + rr) + (size_t)(col0 + sc * kkj + cp) * ld, v);
+          }
+      }
+      __syncwarp();
+      continue;
+    }
     for (int rr = r_lo; rr < nr; rr += 16) {
       const int trow = (rr / kki) * kkrsz + (rr % kki);
       for (int sc = 0; sc < ns; ++sc) {

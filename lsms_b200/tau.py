@@ -46,6 +46,7 @@ EXPORTS = (
     "b200tau_sync", "b200tau_solve_dense", "b200tau_build_kkr", "b200tau_last_launch_count",
     "b200tau_gaunt_numbers", "b200tau_set_refinement", "b200tau_set_profiling",
     "b200tau_profile_read", "b200tau_set_mixed_engine", "b200tau_solve_dense_noalloc",
+    "b200tau_profile_phases",
 )
 
 
@@ -95,6 +96,7 @@ def load_library():
     lib.b200tau_set_profiling.argtypes = [P, I]
     lib.b200tau_set_mixed_engine.argtypes = [P, I]
     lib.b200tau_profile_read.argtypes = [P, P, P, P]
+    lib.b200tau_profile_phases.argtypes = [P, P]
     _lib = lib
     return lib
 
@@ -180,6 +182,12 @@ class TauSolver:
         ms, n, fl = ctypes.c_double(), ctypes.c_long(), ctypes.c_double()
         self._check(self.lib.b200tau_profile_read(self.ctx, ctypes.byref(ms), ctypes.byref(n), ctypes.byref(fl)))
         return ms.value, n.value, fl.value
+
+    def profile_phases(self) -> dict:
+        """Device ms per phase since profiling was enabled: KKR build, elimination, refinement."""
+        ms = (ctypes.c_double * 3)()
+        self._check(self.lib.b200tau_profile_phases(self.ctx, ms))
+        return {"build_ms": ms[0], "eliminate_ms": ms[1], "refine_ms": ms[2]}
 
     # -- uploads (DeviceStorage / DeviceAtom) ----------------------------------------------
     def upload_tmat(self, tmat_store: np.ndarray):
