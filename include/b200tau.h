@@ -49,6 +49,9 @@ extern "C" {
 #define B200TAU_ENGINE_TENSOR 0 /* mixed path: tcgen05 TF32 hi/lo trailing update (default) */
 #define B200TAU_ENGINE_SIMT 1   /* mixed path: FP32 CUDA-core trailing update (cross-check) */
 
+#define B200TAU_SWEEP_FP64 0 /* mixed path: correction solve in FP64 arithmetic on FP32 factors */
+#define B200TAU_SWEEP_FP32 1 /* mixed path: correction solve in FP32, as zcgesv (default) */
+
 typedef struct b200tau_ctx b200tau_ctx;
 
 /* One solve: what calculateTauMatrix receives besides the shared state
@@ -96,12 +99,19 @@ int b200tau_set_atom(b200tau_ctx *ctx, int atom, int num_liz,
  * R = [0; t0] - M X against the unmodified KKR matrix and applies the correction from the
  * stored block factors (the refinement of the reference's zcgesv / cusolverDnIRSXgesv
  * solvers, linearSolvers_CPU.cpp:148-174, linearSolvers_CUDA.cu:424-469, on the N x b
- * system).  Defaults: FP64 1 step, MIXED 3 steps.  FP64 with 0 steps takes tau00 directly
- * from the Schur complement like zblock_lu. */
+ * system).  Defaults: FP64 1 step, MIXED 6 steps, of which each job runs only as many as it
+ * needs: after every step but the last, a job whose estimated remaining error (the relative size
+ * c of the correction just applied times its contraction c / c_previous) is below 1e-13 of
+ * tau00 stops.  FP64 with 0 steps takes tau00 directly from the Schur complement like
+ * zblock_lu. */
 int b200tau_set_refinement(b200tau_ctx *ctx, int prec, int steps);
 
 /* Engine of the mixed path's trailing update (B200TAU_ENGINE_*). */
 int b200tau_set_mixed_engine(b200tau_ctx *ctx, int engine);
+
+/* Arithmetic of the mixed path's correction solve Y = F^-1 R between FP64 residuals
+ * (B200TAU_SWEEP_*).  The residual R = B - M X and the update X += Y are FP64 either way. */
+int b200tau_set_mixed_sweep(b200tau_ctx *ctx, int sweep);
 
 /* Solve `njobs` (atom, energy, spin) problems in one batched device pass and
  * write each job's tau00_l (kkrsz_ns^2 complex, the layout calculateTauMatrix

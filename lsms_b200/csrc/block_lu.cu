@@ -37,104 +37,131 @@ template <> struct Vec2<double> { using t = double2; };
 template <> struct Vec2<float> { using t = float2; };
 
 // ---------------------------------------------------------------------------------------------
-// In-place Gauss-Jordan inverse of the kb x kb diagonal block at (k, k) of F, kb <= 64, in FP64.
+// In-place inverse of the kb x kb diagonal block at (k, k) of F, kb <= 64: FP64 Gauss-Jordan with
+// partial pivoting inside the block on |re| + |im| (izamax's measure; ties go to the lowest row).
+// Rows are never interchanged: step p pivots on the not-yet-used row pv with the largest
+// |A[pv][p]|, and the permutation is applied when the block is written back (for the in-place
+// result P, A^-1[i][pv_k] = P[pv_i][k]).  The block lives in registers, thread (c, g) holding
+// column c and rows g + kRg q; per step the pivot column (the multipliers) and the scaled pivot
+// row pass through shared memory, with two barriers.  The column-p entries follow the same rank-1
+// update as the others because the published pivot row holds dinv + 1 in column p:
+// A[r][p] - f_r (dinv + 1) = -f_r dinv, since A[r][p] = f_r.
 // ---------------------------------------------------------------------------------------------
+constexpr int kDiagThreads = 256;
+constexpr int kRg = kDiagThreads / kNb;  // row groups
+constexpr int kRq = kNb / kRg;           // rows per thread
+
 template <typename T>
-__global__ void __launch_bounds__(256) diag_inverse_kernel(const JobDev *__restrict__ jobs, int k,
-                                                           int *info) {
+__global__ void __launch_bounds__(kDiagThreads) diag_inverse_kernel(const JobDev *__restrict__ jobs, int k,
+                                                                    int *info) {
   constexpr int NB = kNb;
   const JobDev &J = jobs[blockIdx.x];
   if (k >= J.n) return;
   const int kb = min(NB, J.n - k);
   extern __shared__ __align__(16) double2 dyn_smem[];
-  double2(*A)[NB + 1] = reinterpret_cast<double2(*)[NB + 1]>(dyn_smem);  // A[row][col]
-  __shared__ int perm[NB];
-  __shared__ int s_piv;
-  __shared__ double2 s_dinv;
+  double2(*As)[NB + 1] = reinterpret_cast<double2(*)[NB + 1]>(dyn_smem);  // staging As[row][col]
+  __shared__ double2 s_f[2][NB];   // column p before the step: the multipliers
+  __shared__ double2 s_rp[2][NB];  // pivot row scaled by dinv, dinv + 1 in column p
+  __shared__ double s_cval[2][kRg];
+  __shared__ int s_cidx[2][kRg];
+  __shared__ int s_pv[NB], s_inv[NB];
   T *__restrict__ Fk = static_cast<T *>(J.F) + (size_t)k + (size_t)k * J.ld;
   const int tid = threadIdx.x;
-  for (int e = tid; e < kb * kb; e += blockDim.x) {
-    const int c = e / kb, r = e - c * kb;
-    A[r][c] = ldc(Fk + r + (size_t)c * J.ld);
+  for (int e = tid; e < kb * kb; e += kDiagThreads) {
+    const int cc = e / kb, r = e - cc * kb;
+    As[r][cc] = ldc(Fk + r + (size_t)cc * J.ld);
   }
   __syncthreads();
+  const int c = tid % NB, g = tid / NB;
+  double2 a[kRq];
+#pragma unroll
+  for (int q = 0; q < kRq; ++q) {
+    const int r = g + kRg * q;
+    a[q] = (r < kb && c < kb) ? As[r][c] : make_double2(0.0, 0.0);
+  }
+  unsigned long long used = 0;  // rows already pivoted on (the same in every thread)
   bool singular = false;
-  (void)s_piv;
-  (void)s_dinv;
-  // column-owner mapping: thread handles column c = tid % NB and rows r0 + q * RS
-  const int c = tid % NB;
-  const int r0 = tid / NB;
-  constexpr int RS = 256 / NB;
-  const int lane = tid & 31;
   for (int p = 0; p < kb; ++p) {
-    // pivot search |re|+|im| over rows p..kb-1 (izamax convention), done by every warp so that no
-    // barrier is needed to share the result (same data, same reduction order: same answer)
-    double best = -1.0;
-    int bi = p;
-    for (int r = p + lane; r < kb; r += 32) {
-      const double v = cabs1(A[r][p]);
-      if (v > best) {
-        best = v;
-        bi = r;
-      }
-    }
+    const int par = p & 1;
+    if (c == p) {  // this row group's candidate, and the multipliers
+      double best = -1.0;
+      int bi = NB;
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-      if (ob > best || (ob == best && oi < bi)) {
-        best = ob;
-        bi = oi;
-      }
-    }
-    const int pv = bi;
-    if (tid == 0) perm[p] = pv;
-    // read phase: the row swap p <-> pv is folded into the reads
-    const double2 d = A[pv][p];
-    const double2 dinv = (d.x == 0.0 && d.y == 0.0) ? make_double2(0.0, 0.0) : crecip(d);
-    if (dinv.x == 0.0 && dinv.y == 0.0) singular = true;
-    double2 rowp = make_double2(0.0, 0.0);  // new row p, column c
-    double2 f[NB / RS], cur[NB / RS];
-    if (c < kb) {
-      rowp = (c == p) ? dinv : cmul(A[pv][c], dinv);
-#pragma unroll
-      for (int q = 0; q < NB / RS; ++q) {
-        const int r = r0 + q * RS;
-        const int src = (r == pv) ? p : r;  // row r after the swap
-        f[q] = (r < kb) ? A[src][p] : make_double2(0.0, 0.0);
-        cur[q] = (r < kb) ? A[src][c] : make_double2(0.0, 0.0);
-      }
-    }
-    __syncthreads();
-    if (c < kb) {
-#pragma unroll
-      for (int q = 0; q < NB / RS; ++q) {
-        const int r = r0 + q * RS;
-        if (r >= kb) continue;
-        if (r == p) {
-          A[r][c] = rowp;
-        } else {
-          const double2 base = (c == p) ? make_double2(0.0, 0.0) : cur[q];
-          A[r][c] = csub(base, cmul(f[q], rowp));
+      for (int q = 0; q < kRq; ++q) {
+        const int r = g + kRg * q;
+        const double v = cabs1(a[q]);
+        if (r < kb && !((used >> r) & 1ull) && v > best) {
+          best = v;
+          bi = r;
         }
+        s_f[par][r] = a[q];
       }
+      s_cval[par][g] = best;
+      s_cidx[par][g] = bi;
     }
     __syncthreads();
-  }
-  // undo the row interchanges as column interchanges, last first
-  for (int p = kb - 1; p >= 0; --p) {
-    const int pv = perm[p];
-    if (pv != p)
-      for (int r = tid; r < kb; r += blockDim.x) {
-        const double2 t = A[r][p];
-        A[r][p] = A[r][pv];
-        A[r][pv] = t;
+    double best = s_cval[par][0];
+    int pv = s_cidx[par][0];
+#pragma unroll
+    for (int i = 1; i < kRg; ++i) {
+      const double v = s_cval[par][i];
+      const int ix = s_cidx[par][i];
+      if (v > best || (v == best && ix < pv)) {
+        best = v;
+        pv = ix;
       }
+    }
+    used |= 1ull << pv;
+    const double2 d = s_f[par][pv];
+    double2 dinv = make_double2(0.0, 0.0);
+    if (d.x == 0.0 && d.y == 0.0) {
+      singular = true;
+    } else {  // conj(d) / |d|^2 (pivots of these blocks are far from the FP64 range limits)
+      const double rr = 1.0 / (d.x * d.x + d.y * d.y);
+      dinv = make_double2(d.x * rr, -d.y * rr);
+    }
+    if (g == pv % kRg) {  // the warps holding row pv publish it, scaled
+      double2 v = make_double2(0.0, 0.0);
+#pragma unroll
+      for (int q = 0; q < kRq; ++q) {
+        double2 t = a[q];
+        asm volatile("" : "+d"(t.x), "+d"(t.y));  // an opaque copy: the compiler otherwise turns the
+                                                  // selection into an indexed local-memory load
+        if (q == pv / kRg) v = t;
+      }
+      s_rp[par][c] = (c == p) ? make_double2(dinv.x + 1.0, dinv.y) : cmul(v, dinv);
+    }
+    if (tid == 0) s_pv[p] = pv;
     __syncthreads();
+    const double2 rp = s_rp[par][c];
+#pragma unroll
+    for (int q = 0; q < kRq; ++q) {
+      const int r = g + kRg * q;
+      if (r == pv) {
+        a[q] = (c == p) ? dinv : cmul(a[q], dinv);
+      } else {
+        const double2 f = s_f[par][r];
+        a[q].x = fma(-f.x, rp.x, a[q].x);
+        a[q].x = fma(f.y, rp.y, a[q].x);
+        a[q].y = fma(-f.x, rp.y, a[q].y);
+        a[q].y = fma(-f.y, rp.x, a[q].y);
+      }
+    }
   }
-  for (int e = tid; e < kb * kb; e += blockDim.x) {
-    const int c = e / kb, r = e - c * kb;
-    stc(Fk + r + (size_t)c * J.ld, A[r][c]);
+  if (tid < kb) s_inv[s_pv[tid]] = tid;
+  __syncthreads();
+  if (c < kb) {
+    const int col = s_pv[c];
+#pragma unroll
+    for (int q = 0; q < kRq; ++q) {
+      const int r = g + kRg * q;
+      if (r < kb) As[s_inv[r]][col] = a[q];
+    }
+  }
+  __syncthreads();
+  for (int e = tid; e < kb * kb; e += kDiagThreads) {
+    const int cc = e / kb, r = e - cc * kb;
+    stc(Fk + r + (size_t)cc * J.ld, As[r][cc]);
   }
   if (singular && tid == 0) atomicCAS(&info[blockIdx.x], 0, k + 1);
 }
@@ -405,80 +432,75 @@ __global__ void __launch_bounds__(256) finalize_from_x_kernel(const JobDev *__re
 // Refinement pieces.  X, R, Y are N x b FP64 column-major with leading dimension ld.
 // ---------------------------------------------------------------------------------------------
 
-// R = B - M X with B = [0; t0] (rows n..N-1 hold t0).  64 rows x b columns per CTA, K in chunks.
 __device__ __forceinline__ bool converged(const JobDev &J) { return cx::converged(J.conv); }
 
-__global__ void __launch_bounds__(256) residual_kernel(const JobDev *__restrict__ jobs) {
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+
+// R = B - M X with B = [0; t0] (rows n..N-1 hold t0), FP64.  The product is FP64-FMA bound
+// (b complex multiply-adds per 16-byte element of M), so each thread keeps one row x 16 columns of
+// accumulators and every M element it loads feeds 16 complex FMAs: M streams through registers
+// (a batch of RB columns in flight ahead of use), X through a two-stage cp.async ring in shared
+// memory, read as broadcasts.  BC = 16 or 32 is the padded column count (b <= BC).
+template <int BC>
+__global__ void __launch_bounds__(256, 2) residual_kernel(const JobDev *__restrict__ jobs) {
+  constexpr int NC = 16;            // columns per thread
+  constexpr int ROWS = 256 * NC / BC;  // rows per CTA
+  constexpr int KC = 32;            // X rows per stage
+  constexpr int RB = 4;             // M columns per register batch
   const JobDev &J = jobs[blockIdx.y];
   if (converged(J)) return;
   const int N = J.N, ld = J.ld, b = J.b;
-  const int row0 = blockIdx.x * 64;
+  const int row0 = blockIdx.x * ROWS;
   if (row0 >= N) return;
-  constexpr int KC = 16;
-  __shared__ double2 Ms[KC][65];     // Ms[kk][row]
-  __shared__ double2 Xs[KC][kMaxB];  // Xs[kk][col]
+  __shared__ __align__(16) double2 Xs[2][KC][BC];
   const int tid = threadIdx.x;
-  const int tr = tid & 63, tc = tid >> 6;  // row, column group (4 groups)
-  double2 acc[kMaxB / 4];
-#pragma unroll
-  for (int j = 0; j < kMaxB / 4; ++j) acc[j] = make_double2(0.0, 0.0);
-  const double2 *__restrict__ M = J.M;
+  const int r = tid % ROWS, cg = tid / ROWS;
+  const int gr = row0 + r;
+  const double2 *__restrict__ Mrow = J.M + min(gr, N - 1);
   const double2 *__restrict__ X = J.X;
-  // register double buffer: the loads of chunk kc + KC are in flight while chunk kc is consumed
-  constexpr int MQ = 64 * KC / 256;             // M elements per thread per chunk
-  constexpr int XQ = (KC * kMaxB + 255) / 256;  // X elements per thread per chunk
-  double2 rm[MQ], rx[XQ];
-  auto load = [&](int kc) {
-#pragma unroll
-    for (int q = 0; q < MQ; ++q) {
-      const int e = tid + q * 256;
-      const int r = e & 63, kk = e >> 6;
-      const int gr = row0 + r, gk = kc + kk;
-      rm[q] = (gr < N && gk < N) ? M[(size_t)gr + (size_t)gk * ld] : make_double2(0.0, 0.0);
-    }
-#pragma unroll
-    for (int q = 0; q < XQ; ++q) {
-      const int e = tid + q * 256;
+  // X rows [kc, kc + KC) into stage st; columns >= b and rows >= N read as zero
+  auto stage_x = [&](int kc, int st) {
+    for (int e = tid; e < KC * BC; e += 256) {
       const int kk = e % KC, c = e / KC;
-      const int gk = kc + kk;
-      rx[q] = (c < b && gk < N) ? X[(size_t)gk + (size_t)c * ld] : make_double2(0.0, 0.0);
+      if (c < b && kc + kk < N) cp_async16(&Xs[st][kk][c], X + (size_t)(kc + kk) + (size_t)c * ld);
+      else Xs[st][kk][c] = make_double2(0.0, 0.0);
     }
+    asm volatile("cp.async.commit_group;" ::: "memory");
   };
-  auto store = [&]() {
+  auto load_m = [&](double2 (&m)[RB], int k0) {
 #pragma unroll
-    for (int q = 0; q < MQ; ++q) {
-      const int e = tid + q * 256;
-      Ms[e >> 6][e & 63] = rm[q];
-    }
-#pragma unroll
-    for (int q = 0; q < XQ; ++q) {
-      const int e = tid + q * 256;
-      if (e < KC * kMaxB) Xs[e % KC][e / KC] = rx[q];
-    }
+    for (int i = 0; i < RB; ++i) m[i] = (k0 + i < N) ? Mrow[(size_t)(k0 + i) * ld] : make_double2(0.0, 0.0);
   };
-  load(0);
-  store();
-  __syncthreads();
-  for (int kc = 0; kc < N; kc += KC) {
-    if (kc + KC < N) load(kc + KC);
-#pragma unroll 4
-    for (int kk = 0; kk < KC; ++kk) {
-      const double2 a = Ms[kk][tr];
+  double2 acc[NC];
 #pragma unroll
-      for (int j = 0; j < kMaxB / 4; ++j) {
-        const int c = tc + 4 * j;
-        if (c < b) acc[j] = cfma(a, Xs[kk][c], acc[j]);
-      }
+  for (int j = 0; j < NC; ++j) acc[j] = make_double2(0.0, 0.0);
+  double2 mc[RB], mn[RB];
+  stage_x(0, 0);
+  load_m(mc, 0);
+  for (int k0 = 0; k0 < N; k0 += RB) {
+    const int st = (k0 / KC) & 1;
+    if (k0 % KC == 0) {
+      asm volatile("cp.async.wait_group 0;" ::: "memory");
+      __syncthreads();  // stage st complete for all threads; the other stage is no longer read
+      if (k0 + KC < N) stage_x(k0 + KC, st ^ 1);
     }
-    __syncthreads();
-    if (kc + KC < N) store();
-    __syncthreads();
+    if (k0 + RB < N) load_m(mn, k0 + RB);
+    const int kr = k0 % KC;
+#pragma unroll
+    for (int i = 0; i < RB; ++i) {
+#pragma unroll
+      for (int j = 0; j < NC; ++j) acc[j] = cfma(mc[i], Xs[st][kr + i][cg * NC + j], acc[j]);
+    }
+#pragma unroll
+    for (int i = 0; i < RB; ++i) mc[i] = mn[i];
   }
-  const int gr = row0 + tr;
   if (gr >= N) return;
 #pragma unroll
-  for (int j = 0; j < kMaxB / 4; ++j) {
-    const int c = tc + 4 * j;
+  for (int j = 0; j < NC; ++j) {
+    const int c = cg * NC + j;
     if (c >= b) continue;
     const double2 bv = (gr >= J.n) ? J.t0[(gr - J.n) + (size_t)c * J.t0_ld] : make_double2(0.0, 0.0);
     J.R[(size_t)gr + (size_t)c * ld] = csub(bv, acc[j]);
@@ -530,7 +552,7 @@ cudaError_t eliminate_impl(const JobDev *jobs, int njobs, int max_n, int max_N, 
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem_gemm)) != cudaSuccess)
     return e;
   for (int k = 0; k < max_n; k += kNb) {
-    diag_inverse_kernel<T><<<njobs, 256, smem_diag, s>>>(jobs, k, info);
+    diag_inverse_kernel<T><<<njobs, kDiagThreads, smem_diag, s>>>(jobs, k, info);
     const int rest = max_N - k - 1;
     const int tiles = (rest + kTile - 1) / kTile;
     if (launches) *launches += 1;
@@ -553,16 +575,16 @@ cudaError_t eliminate_impl(const JobDev *jobs, int njobs, int max_n, int max_N, 
 
 template <typename T>
 cudaError_t sweep_solve(const JobDev *jobs, int njobs, int b, int mode, int *info, cudaStream_t s,
-                        long *launches) {
+                        long *launches, bool fp32) {
   const FactorKind fk = sizeof(T) == sizeof(double2) ? kFactorFP64 : kFactorFP32;
   cudaError_t e;
   // forward (skipped for the initial solve: B is zero above the central block)
   if (mode == 1) {
-    if ((e = launch_sweep(fk, jobs, njobs, b, true, mode, s)) != cudaSuccess) return e;
+    if ((e = launch_sweep(fk, jobs, njobs, b, true, mode, fp32, s)) != cudaSuccess) return e;
     if (launches) *launches += 1;
   }
   schur_solve_kernel<T><<<njobs, 256, 0, s>>>(jobs, mode, info);
-  if ((e = launch_sweep(fk, jobs, njobs, b, false, mode, s)) != cudaSuccess) return e;
+  if ((e = launch_sweep(fk, jobs, njobs, b, false, mode, fp32, s)) != cudaSuccess) return e;
   if (launches) *launches += 2;
   return cudaSuccess;
 }
@@ -645,21 +667,22 @@ cudaError_t launch_finalize_direct(FactorKind fk, const JobDev *jobs, int njobs,
 }
 
 cudaError_t launch_refine_begin(FactorKind fk, const JobDev *jobs, int njobs, int max_n, int max_N, int b,
-                                int *info, cudaStream_t s, long *launches) {
+                                int *info, cudaStream_t s, long *launches, bool fp32_sweep) {
   (void)max_n;
   (void)max_N;
-  const cudaError_t e = fk == kFactorFP64 ? sweep_solve<double2>(jobs, njobs, b, 0, info, s, launches)
-                                           : sweep_solve<float2>(jobs, njobs, b, 0, info, s, launches);
+  const cudaError_t e = fk == kFactorFP64 ? sweep_solve<double2>(jobs, njobs, b, 0, info, s, launches, false)
+                                           : sweep_solve<float2>(jobs, njobs, b, 0, info, s, launches, fp32_sweep);
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 cudaError_t launch_refine_round(FactorKind fk, const JobDev *jobs, int njobs, int max_n, int max_N, int b,
-                                bool check, int *info, cudaStream_t s, long *launches) {
+                                bool check, int *info, cudaStream_t s, long *launches, bool fp32_sweep) {
   (void)max_n;
-  residual_kernel<<<dim3((max_N + 63) / 64, njobs), 256, 0, s>>>(jobs);
+  if (b <= 16) residual_kernel<16><<<dim3((max_N + 255) / 256, njobs), 256, 0, s>>>(jobs);
+  else residual_kernel<32><<<dim3((max_N + 127) / 128, njobs), 256, 0, s>>>(jobs);
   if (launches) *launches += 1;
-  const cudaError_t e = fk == kFactorFP64 ? sweep_solve<double2>(jobs, njobs, b, 1, info, s, launches)
-                                           : sweep_solve<float2>(jobs, njobs, b, 1, info, s, launches);
+  const cudaError_t e = fk == kFactorFP64 ? sweep_solve<double2>(jobs, njobs, b, 1, info, s, launches, false)
+                                           : sweep_solve<float2>(jobs, njobs, b, 1, info, s, launches, fp32_sweep);
   if (e != cudaSuccess) return e;
   if (check) {
     converge_check_kernel<<<njobs, 256, 0, s>>>(jobs, 1e-13);
@@ -675,10 +698,11 @@ cudaError_t launch_refine_end(const JobDev *jobs, int njobs, int ns, int kkrsz, 
 }
 
 cudaError_t launch_solve_refine(FactorKind fk, const JobDev *jobs, int njobs, int max_n, int max_N, int b,
-                                int steps, int ns, int kkrsz, int *info, cudaStream_t s, long *launches) {
-  cudaError_t e = launch_refine_begin(fk, jobs, njobs, max_n, max_N, b, info, s, launches);
+                                int steps, int ns, int kkrsz, int *info, cudaStream_t s, long *launches,
+                                bool fp32_sweep) {
+  cudaError_t e = launch_refine_begin(fk, jobs, njobs, max_n, max_N, b, info, s, launches, fp32_sweep);
   for (int it = 0; it < steps && e == cudaSuccess; ++it)
-    e = launch_refine_round(fk, jobs, njobs, max_n, max_N, b, it + 1 < steps, info, s, launches);
+    e = launch_refine_round(fk, jobs, njobs, max_n, max_N, b, it + 1 < steps, info, s, launches, fp32_sweep);
   if (e != cudaSuccess) return e;
   return launch_refine_end(jobs, njobs, ns, kkrsz, s, launches);
 }

@@ -96,6 +96,7 @@ struct b200tau_ctx {
   double phase_ms[3] = {0.0, 0.0, 0.0};
   // tensor-core trailing update of the mixed path: operand packs + TMA descriptors
   int mixed_engine = B200TAU_ENGINE_TENSOR;
+  int mixed_sweep = B200TAU_SWEEP_FP32;  // arithmetic of the mixed path's correction solve
   TcMaps tc;
   float *d_pack = nullptr;
   int tc_ld = 0, tc_slots = 0;
@@ -399,7 +400,9 @@ int ensure_jobs2(b200tau_ctx *ctx, int n) {
 // to ctx->d_jobs.
 int run_refinement(b200tau_ctx *ctx, const std::vector<JobDev> &h, int nw, int maxn, int maxN, int b, int ns,
                    int kkrsz, const Plan &p) {
-  CK(launch_refine_begin(p.fk, ctx->d_jobs, nw, maxn, maxN, b, ctx->d_info, ctx->stream, &ctx->launches));
+  const bool fp32_sweep = p.fk == kFactorFP32 && ctx->mixed_sweep == B200TAU_SWEEP_FP32;
+  CK(launch_refine_begin(p.fk, ctx->d_jobs, nw, maxn, maxN, b, ctx->d_info, ctx->stream, &ctx->launches,
+                         fp32_sweep));
   const JobDev *cur = ctx->d_jobs;
   int ncur = nw, cmaxn = maxn, cmaxN = maxN;
   int *cur_info = ctx->d_info;
@@ -428,7 +431,7 @@ int run_refinement(b200tau_ctx *ctx, const std::vector<JobDev> &h, int nw, int m
       }
     }
     CK(launch_refine_round(p.fk, cur, ncur, cmaxn, cmaxN, b, it + 1 < p.steps, cur_info, ctx->stream,
-                           &ctx->launches));
+                           &ctx->launches, fp32_sweep));
   }
   CK(launch_refine_end(ctx->d_jobs, nw, ns, kkrsz, ctx->stream, &ctx->launches));
   return B200TAU_OK;
@@ -705,6 +708,14 @@ int b200tau_set_mixed_engine(b200tau_ctx *ctx, int engine) {
   if (engine != B200TAU_ENGINE_TENSOR && engine != B200TAU_ENGINE_SIMT)
     return fail(ctx, B200TAU_ERR_ARG, "unknown engine %d", engine);
   ctx->mixed_engine = engine;
+  return B200TAU_OK;
+}
+
+int b200tau_set_mixed_sweep(b200tau_ctx *ctx, int sweep) {
+  if (!ctx) return B200TAU_ERR_ARG;
+  if (sweep != B200TAU_SWEEP_FP64 && sweep != B200TAU_SWEEP_FP32)
+    return fail(ctx, B200TAU_ERR_ARG, "unknown sweep arithmetic %d", sweep);
+  ctx->mixed_sweep = sweep;
   return B200TAU_OK;
 }
 

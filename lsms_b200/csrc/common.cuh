@@ -133,19 +133,22 @@ cudaError_t launch_finalize_direct(FactorKind fk, const JobDev *jobs, int njobs,
                                    int *info, cudaStream_t s, long *launches);
 // Iterative refinement of X for M X = [0; t0]: initial solve from the factors, then `steps`
 // rounds of R = B - M X (FP64), Y = F^-1 R, X += Y; then out from X[n:N].
+// `fp32_sweep` (FP32 factors only) runs the correction solve in FP32 arithmetic, as LAPACK's
+// zcgesv does; the residual and X += Y stay FP64.
 cudaError_t launch_solve_refine(FactorKind fk, const JobDev *jobs, int njobs, int max_n, int max_N,
                                 int b, int steps, int ns, int kkrsz, int *info, cudaStream_t s,
-                                long *launches);
+                                long *launches, bool fp32_sweep = false);
 // The same in pieces, for a driver that drops converged jobs between rounds: the initial solve
 // X = F^-1 [0; t0], one refinement round (with the convergence check when `check`), and tau00_l.
 cudaError_t launch_refine_begin(FactorKind fk, const JobDev *jobs, int njobs, int max_n, int max_N, int b,
-                                int *info, cudaStream_t s, long *launches);
+                                int *info, cudaStream_t s, long *launches, bool fp32_sweep = false);
 cudaError_t launch_refine_round(FactorKind fk, const JobDev *jobs, int njobs, int max_n, int max_N, int b,
-                                bool check, int *info, cudaStream_t s, long *launches);
+                                bool check, int *info, cudaStream_t s, long *launches, bool fp32_sweep = false);
 cudaError_t launch_refine_end(const JobDev *jobs, int njobs, int ns, int kkrsz, cudaStream_t s, long *launches);
-// One block sweep of the correction solve for all jobs, one 8-CTA cluster per job (sweep.cu):
-// forward (R -> Y over the D_k, A21_k factors) or backward (Y over the W_k factors, X (+)= Y).
+// One block sweep of the correction solve for all jobs, one thread-block cluster per job
+// (sweep.cu): forward (R -> Y over the D_k, A21_k factors) or backward (Y over the W_k factors,
+// X (+)= Y).  `fp32_arith` selects FP32 arithmetic on FP32 factors.
 cudaError_t launch_sweep(FactorKind fk, const JobDev *jobs, int njobs, int b, bool forward, int mode,
-                         cudaStream_t s);
+                         bool fp32_arith, cudaStream_t s);
 
 }  // namespace b200

@@ -34,6 +34,29 @@ __device__ __forceinline__ double2 ldc(const float2 *p) {
 __device__ __forceinline__ void stc(double2 *p, double2 v) { *p = v; }
 __device__ __forceinline__ void stc(float2 *p, double2 v) { *p = make_float2((float)v.x, (float)v.y); }
 
+// FP32 complex multiply-add (c + a b).
+__device__ __forceinline__ float2 cfma(float2 a, float2 b, float2 c) {
+  c.x = fmaf(a.x, b.x, c.x);
+  c.x = fmaf(-a.y, b.y, c.x);
+  c.y = fmaf(a.x, b.y, c.y);
+  c.y = fmaf(a.y, b.x, c.y);
+  return c;
+}
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+
+// Conversions between the storage type and the arithmetic type V (double2 or float2).
+template <typename V> __device__ __forceinline__ V to_v(double2 a);
+template <> __device__ __forceinline__ double2 to_v<double2>(double2 a) { return a; }
+template <> __device__ __forceinline__ float2 to_v<float2>(double2 a) { return make_float2((float)a.x, (float)a.y); }
+template <typename V> __device__ __forceinline__ V to_v(float2 a);
+template <> __device__ __forceinline__ double2 to_v<double2>(float2 a) { return make_double2(a.x, a.y); }
+template <> __device__ __forceinline__ float2 to_v<float2>(float2 a) { return a; }
+__device__ __forceinline__ double2 to_d(double2 a) { return a; }
+__device__ __forceinline__ double2 to_d(float2 a) { return make_double2(a.x, a.y); }
+template <typename V> __device__ __forceinline__ V vzero();
+template <> __device__ __forceinline__ double2 vzero<double2>() { return make_double2(0.0, 0.0); }
+template <> __device__ __forceinline__ float2 vzero<float2>() { return make_float2(0.f, 0.f); }
+
 // Refinement round skip flag (set on the device by the convergence check, read by later launches).
 __device__ __forceinline__ bool converged(const int *conv) {
   return conv != nullptr && *reinterpret_cast<volatile const int *>(conv) != 0;

@@ -1,4 +1,4 @@
-// Block sweeps of the correction solve Y = F^-1 R, one thread-block cluster of 8 CTAs per job.
+// Block sweeps of the correction solve Y = F^-1 R, one thread-block cluster per job.
 //
 // F holds the block factors of the elimination (block_lu.cu): D_k = A11_k^-1 in the diagonal
 // blocks, A21_k below them, W_k = D_k A12_k to their right, S in the trailing b x b block.
@@ -7,10 +7,16 @@
 // (the S solve between them is schur_solve_kernel).  This is the same contract as the reference's
 // zgetrs on the block LU factors (zblock_lu_cpp.cpp:60-86) applied to the N x b right-hand side.
 //
-// One launch covers the whole sweep: the 8 CTAs of a cluster split the trailing 64-row tiles
-// (tile t on rank t % 8, so each tile of R or Y always has the same writer) and meet at a cluster
-// barrier (release / acquire) after each block step; cross-CTA reads go through L2 (__ldcg).
-// Each CTA recomputes the small Y_k = D_k R_k itself rather than waiting for another CTA's copy.
+// Layout of the work.  The CTAs of a cluster (cluster size cs, chosen per launch so that one
+// wave of jobs fills the GPU once) split the 64-row tiles of R or Y: tile t always belongs to
+// rank t % cs, so every tile has one writer.  The operand panels (A21_k or W_k rows of a tile,
+// 64 rows x 32 columns per unit) are constant during a sweep, so each CTA streams its units
+// through a two-stage cp.async ring in shared memory, fetching the next unit while it multiplies
+// the current one; the arithmetic is FP64 FMA.  One cluster barrier (release / acquire) per block
+// step orders the tile updates; cross-CTA reads of R and Y go through L2 (__ldcg).
+// In the forward sweep the owner of the next diagonal block updates that tile first and computes
+// Y_(k+1) = D_(k+1) R_(k+1) while the other CTAs finish step k, so the small D multiply is off the
+// critical path of all but one CTA.
 
 #include <cuda_runtime.h>
 
@@ -22,12 +28,18 @@ namespace {
 
 using namespace cx;
 
-constexpr int kClus = 8;
+constexpr int kUnitCols = 32;  // operand columns per pipeline unit
+constexpr int kMaxCluster = 8;
 
-__device__ __forceinline__ unsigned cluster_rank() {
+__device__ __forceinline__ int cluster_rank() {
   unsigned r;
   asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
-  return r;
+  return (int)r;
+}
+__device__ __forceinline__ int cluster_size() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+  return (int)r;
 }
 // Every thread of every CTA of the cluster; orders the global writes made before it.
 __device__ __forceinline__ void cluster_sync() {
@@ -36,100 +48,286 @@ __device__ __forceinline__ void cluster_sync() {
       "barrier.cluster.wait.acquire.aligned;" ::
           : "memory");
 }
-
-template <typename T>
-constexpr int forward_smem_bytes() {
-  return (int)(sizeof(T) * kNb * kNb + 2 * sizeof(double2) * kNb * kMaxB);
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// Grid (8, njobs), cluster (8, 1, 1).  mode is 1 (refinement rounds only: the initial solve has
-// B = 0 above the central block, so its forward sweep is the identity).
+// Copies the 64 x ncol block of F at (row0, col0) into shared memory, column-major with 64 rows
+// per column (dst[c * 64 + r]).  The rows past N up to the leading dimension are inside the
+// allocation (ld >= N rounded up to 64) and are never used by the arithmetic.
 template <typename T>
-__global__ void __cluster_dims__(kClus, 1, 1) __launch_bounds__(256)
-    forward_sweep_kernel(const JobDev *__restrict__ jobs) {
-  const JobDev &J = jobs[blockIdx.y];
-  if (converged(J.conv)) return;  // the flag changes only between launches: uniform per cluster
-  const int rank = (int)cluster_rank();
-  const int n = J.n, N = J.N, ld = J.ld, b = J.b;
-  const T *__restrict__ F = static_cast<const T *>(J.F);
-  extern __shared__ __align__(16) unsigned char fsm[];
-  T *Ds = reinterpret_cast<T *>(fsm);                                            // Ds[j * 64 + r]
-  double2 *Rs = reinterpret_cast<double2 *>(fsm + sizeof(T) * kNb * kNb);        // Rs[c * 64 + r]
-  double2(*Ys)[kMaxB] = reinterpret_cast<double2(*)[kMaxB]>(fsm + sizeof(T) * kNb * kNb +
-                                                              sizeof(double2) * kNb * kMaxB);
-  const int tid = threadIdx.x;
-  const int tr = tid & 63, tc = tid >> 6;
-  for (int k = 0; k < n; k += kNb) {
-    const int kb = min(kNb, n - k);
-    for (int e = tid; e < kb * kb; e += 256) {
-      const int r = e % kb, j = e / kb;
-      Ds[j * kNb + r] = F[(size_t)(k + r) + (size_t)(k + j) * ld];
-    }
-    for (int e = tid; e < kb * b; e += 256) {
-      const int r = e % kb, c = e / kb;
-      Rs[c * kNb + r] = __ldcg(J.R + (size_t)(k + r) + (size_t)c * ld);
-    }
-    __syncthreads();
-    for (int e = tid; e < kb * b; e += 256) {
-      const int r = e % kb, c = e / kb;
-      double2 s = make_double2(0.0, 0.0);
-#pragma unroll 8
-      for (int j = 0; j < kb; ++j) s = cfma(ldc(&Ds[j * kNb + r]), Rs[c * kNb + j], s);
-      Ys[r][c] = s;
-      if (rank == 0) J.Y[(size_t)(k + r) + (size_t)c * ld] = s;
-    }
-    __syncthreads();
-    // R[k+kb:N] -= A21_k Y_k over absolute 64-row tiles
-    for (int t = (k + kb) / 64; t * 64 < N; ++t) {
-      if (t % kClus != rank) continue;
-      const int gr = t * 64 + tr;
-      if (gr < k + kb || gr >= N) continue;
-      double2 acc[kMaxB / 4];
-#pragma unroll
-      for (int j = 0; j < kMaxB / 4; ++j) acc[j] = make_double2(0.0, 0.0);
-      const T *lrow = F + (size_t)gr + (size_t)k * ld;
-#pragma unroll 8
-      for (int jj = 0; jj < kb; ++jj) {
-        const double2 a = ldc(lrow + (size_t)jj * ld);
-#pragma unroll
-        for (int j = 0; j < kMaxB / 4; ++j) {
-          const int c = tc + 4 * j;
-          if (c < b) acc[j] = cfma(a, Ys[jj][c], acc[j]);
-        }
-      }
-#pragma unroll
-      for (int j = 0; j < kMaxB / 4; ++j) {
-        const int c = tc + 4 * j;
-        if (c >= b) continue;
-        double2 *dst = J.R + (size_t)gr + (size_t)c * ld;
-        *dst = csub(__ldcg(dst), acc[j]);
-      }
-    }
-    cluster_sync();  // R_(k+64) complete before any CTA stages it; Ds, Rs, Ys free again
+__device__ __forceinline__ void stage_block(T *dst, const T *F, int ld, int row0, int col0, int ncol) {
+  constexpr int kPer = 16 / (int)sizeof(T);  // elements per 16-byte copy
+  constexpr int kCpc = 64 / kPer;            // copies per column
+  for (int e = threadIdx.x; e < ncol * kCpc; e += blockDim.x) {
+    const int c = e / kCpc, part = e - c * kCpc;
+    cp_async16(dst + c * 64 + part * kPer, F + (size_t)row0 + part * kPer + (size_t)(col0 + c) * ld);
   }
 }
 
-// Grid (8, njobs), cluster (8, 1, 1).  mode 0 sets X = Y, mode 1 adds X += Y (and skips
-// converged jobs).
-template <typename T>
-__global__ void __cluster_dims__(kClus, 1, 1) __launch_bounds__(256)
-    backward_sweep_kernel(const JobDev *__restrict__ jobs, int mode) {
+// Shared-memory layout of the sweep kernels.
+// T: factor storage type; V: arithmetic type of the sweep (double2, or float2 for a correction
+// solve in single precision on FP32 factors, as in LAPACK's zcgesv).
+template <typename T, typename V>
+struct SweepSmem {
+  static constexpr int kUnitBytes = kUnitCols * 64 * (int)sizeof(T);
+  static constexpr int kLs = 0;                                     // 2 units
+  static constexpr int kDs = kLs + 2 * kUnitBytes;                  // D_(k+1), 64 x 64 (forward)
+  static constexpr int kYs = kDs + 64 * 64 * (int)sizeof(T);        // Y_k, 64 x kMaxB
+  static constexpr int kRs = kYs + 64 * kMaxB * (int)sizeof(V);     // R_(k+1) (forward)
+  static constexpr int kForward = kRs + 64 * kMaxB * (int)sizeof(V);
+  static constexpr int kBackward = kDs + 64 * kMaxB * (int)sizeof(V);  // Ls + Ys only
+};
+
+// The units (64-row tile t, 32-column slice h of block step k) of one CTA in the order it
+// consumes them; a second copy runs ahead to issue the prefetches.
+struct ForwardUnits {
+  int n, N, cs, rank;
+  int k, kb, t, h;
+  __device__ void begin() {
+    k = 0;
+    seek();
+  }
+  __device__ bool done() const { return k >= n; }
+  __device__ int ncol() const { return min(kUnitCols, kb - h * kUnitCols); }
+  // first own tile of step k (rows from k + kb), or of a later step
+  __device__ void seek() {
+    for (; k < n; k += 64) {
+      kb = min(64, n - k);
+      const int tlo = (k + kb) / 64;
+      t = tlo + (rank - tlo % cs + cs) % cs;
+      if (t * 64 < N) {
+        h = 0;
+        return;
+      }
+    }
+  }
+  __device__ void next() {
+    if (++h * kUnitCols < kb) return;
+    h = 0;
+    t += cs;
+    if (t * 64 < N) return;
+    k += 64;
+    seek();
+  }
+};
+
+struct BackwardUnits {
+  int n, b, cs, rank;
+  int k, kb, t, h;
+  bool fin;
+  __device__ void begin() {
+    k = n;
+    kb = b;
+    fin = false;
+    seek();
+  }
+  __device__ bool done() const { return fin; }
+  __device__ int ncol() const { return min(kUnitCols, kb - h * kUnitCols); }
+  // own tiles of block k cover rows [0, k); blocks run central, last, last - 64, ..., 0
+  __device__ void seek() {
+    for (;;) {
+      t = rank;
+      if (t * 64 < k) {
+        h = 0;
+        return;
+      }
+      if (k == 0) {
+        fin = true;
+        return;
+      }
+      k = (k == n) ? ((n - 1) / 64) * 64 : k - 64;
+      kb = min(64, n - k);
+    }
+  }
+  __device__ void next() {
+    if (++h * kUnitCols < kb) return;
+    h = 0;
+    t += cs;
+    if (t * 64 < k) return;
+    if (k == 0) {
+      fin = true;
+      return;
+    }
+    k = (k == n) ? ((n - 1) / 64) * 64 : k - 64;
+    kb = min(64, n - k);
+    seek();
+  }
+};
+
+// acc[j] += sum_kk Lu[kk][r] * Ys[y0 + kk][cg + 4 j] over one unit of ncol columns.
+template <typename T, typename V, int NJ>
+__device__ __forceinline__ void unit_product(V (&acc)[NJ], const T *__restrict__ Lu,
+                                             const V (*__restrict__ Ys)[kMaxB], int y0, int ncol, int r, int cg) {
+#pragma unroll 8
+  for (int kk = 0; kk < ncol; ++kk) {
+    const V a = to_v<V>(Lu[kk * 64 + r]);
+#pragma unroll
+    for (int j = 0; j < NJ; ++j) acc[j] = cfma(a, Ys[y0 + kk][cg + 4 * j], acc[j]);
+  }
+}
+
+// Columns [b, bc) of a 64 x kMaxB staging block read as zero.
+template <typename V>
+__device__ __forceinline__ void zero_pad_columns(V (*Ys)[kMaxB], int b, int bc) {
+  for (int e = threadIdx.x; e < 64 * (bc - b); e += blockDim.x) Ys[e % 64][b + e / 64] = vzero<V>();
+}
+
+// Grid (cs, njobs), cluster (cs, 1, 1), 256 threads.  Refinement rounds only: the initial solve
+// has B = 0 above the central block, so its forward sweep is the identity.  BC is 16 or 32,
+// the padded column count of the right-hand side (b <= BC).
+template <typename T, typename V, int BC>
+__global__ void __launch_bounds__(256) forward_sweep_kernel(const JobDev *__restrict__ jobs) {
+  constexpr int NJ = BC / 4;
+  using L = SweepSmem<T, V>;
+  const JobDev &J = jobs[blockIdx.y];
+  if (converged(J.conv) || J.n == 0) return;  // uniform over the cluster: the flag changes between launches
+  const int rank = cluster_rank(), cs = cluster_size();
+  const int n = J.n, N = J.N, ld = J.ld, b = J.b;
+  const T *__restrict__ F = static_cast<const T *>(J.F);
+  extern __shared__ __align__(128) unsigned char sm[];
+  T *Ls = reinterpret_cast<T *>(sm + L::kLs);
+  T *Ds = reinterpret_cast<T *>(sm + L::kDs);
+  V(*Ys)[kMaxB] = reinterpret_cast<V(*)[kMaxB]>(sm + L::kYs);
+  V(*Rs)[kMaxB] = reinterpret_cast<V(*)[kMaxB]>(sm + L::kRs);
+  const int tid = threadIdx.x, r = tid & 63, cg = tid >> 6;
+  zero_pad_columns(Ys, b, BC);
+  zero_pad_columns(Rs, b, BC);
+
+  // Y_k = D_k R_k (D_k in Ds, R_k in Rs) into J.Y rows [k, k + kb)
+  auto diag_apply = [&](int k, int kb) {
+    if (r >= kb) return;
+    V acc[NJ];
+#pragma unroll
+    for (int j = 0; j < NJ; ++j) acc[j] = vzero<V>();
+    unit_product<T, V, NJ>(acc, Ds, Rs, 0, kb, r, cg);
+#pragma unroll
+    for (int j = 0; j < NJ; ++j) {
+      const int c = cg + 4 * j;
+      if (c < b) J.Y[(size_t)(k + r) + (size_t)c * ld] = to_d(acc[j]);
+    }
+  };
+
+  if (rank == 0) {  // Y_0
+    const int kb0 = min(64, n);
+    stage_block(Ds, F, ld, 0, 0, kb0);
+    cp_async_commit();
+    for (int e = tid; e < kb0 * b; e += 256)
+      Rs[e % kb0][e / kb0] = to_v<V>(__ldcg(J.R + (size_t)(e % kb0) + (size_t)(e / kb0) * ld));
+    cp_async_wait<0>();
+    __syncthreads();
+    diag_apply(0, kb0);
+  }
+  cluster_sync();
+
+  constexpr int kUnitElems = kUnitCols * 64;
+  ForwardUnits it{n, N, cs, rank};
+  it.begin();
+  ForwardUnits pf = it;
+  for (int s = 0; s < 2; ++s) {
+    if (!pf.done()) {
+      stage_block(Ls + s * kUnitElems, F, ld, pf.t * 64, pf.k + pf.h * kUnitCols, pf.ncol());
+      pf.next();
+    }
+    cp_async_commit();
+  }
+  int stage = 0;
+  for (int k = 0; k < n; k += 64) {
+    const int kb = min(64, n - k);
+    const int tnext = (k + 64) / 64;  // tile of the next diagonal block
+    const bool owner = k + 64 < n && tnext % cs == rank;
+    if (owner) {
+      stage_block(Ds, F, ld, k + 64, k + 64, min(64, n - k - 64));
+      cp_async_commit();
+    }
+    for (int e = tid; e < kb * b; e += 256) {
+      const int rr = e % kb, c = e / kb;
+      Ys[rr][c] = to_v<V>(__ldcg(J.Y + (size_t)(k + rr) + (size_t)c * ld));
+    }
+    while (!it.done() && it.k == k) {
+      const int t = it.t;
+      V acc[NJ];
+#pragma unroll
+      for (int j = 0; j < NJ; ++j) acc[j] = vzero<V>();
+      do {
+        cp_async_wait<1>();
+        __syncthreads();  // this unit has landed for every thread; Ys is complete
+        unit_product<T, V, NJ>(acc, Ls + stage * kUnitElems, Ys, it.h * kUnitCols, it.ncol(), r, cg);
+        __syncthreads();  // every thread is done with the stage before it is refilled
+        if (!pf.done()) {
+          stage_block(Ls + stage * kUnitElems, F, ld, pf.t * 64, pf.k + pf.h * kUnitCols, pf.ncol());
+          pf.next();
+        }
+        cp_async_commit();
+        stage ^= 1;
+        it.next();
+      } while (!it.done() && it.k == k && it.t == t && it.h != 0);
+      // R[tile] -= A21_k Y_k for the rows below the block
+      const int gr = t * 64 + r;
+      if (gr >= k + kb && gr < N) {
+#pragma unroll
+        for (int j = 0; j < NJ; ++j) {
+          const int c = cg + 4 * j;
+          if (c >= b) continue;
+          double2 *dst = J.R + (size_t)gr + (size_t)c * ld;
+          const V v = csub(to_v<V>(__ldcg(dst)), acc[j]);
+          *dst = to_d(v);
+          if (owner && t == tnext) Rs[r][c] = v;
+        }
+      }
+      if (owner && t == tnext) {  // Y_(k+1) for every CTA of the next step
+        cp_async_wait<0>();
+        __syncthreads();
+        diag_apply(k + 64, min(64, n - k - 64));
+      }
+    }
+    cluster_sync();  // R and Y of this step are final; Ys, Rs and Ds are free again
+  }
+  cp_async_wait<0>();
+}
+
+// Grid (cs, njobs), cluster (cs, 1, 1), 256 threads.  mode 0 sets X = Y, mode 1 adds X += Y
+// (and skips converged jobs).
+template <typename T, typename V, int BC>
+__global__ void __launch_bounds__(256) backward_sweep_kernel(const JobDev *__restrict__ jobs, int mode) {
+  constexpr int NJ = BC / 4;
+  using L = SweepSmem<T, V>;
   const JobDev &J = jobs[blockIdx.y];
   if (mode == 1 && converged(J.conv)) return;
-  const int rank = (int)cluster_rank();
+  const int rank = cluster_rank(), cs = cluster_size();
   const int n = J.n, ld = J.ld, b = J.b;
   const T *__restrict__ F = static_cast<const T *>(J.F);
-  __shared__ double2 Ys[kNb][kMaxB];
-  const int tid = threadIdx.x;
-  const int tr = tid & 63, tc = tid >> 6;
-  const int last = n > 0 ? ((n - 1) / kNb) * kNb : 0;
+  extern __shared__ __align__(128) unsigned char sm[];
+  T *Ls = reinterpret_cast<T *>(sm + L::kLs);
+  V(*Ys)[kMaxB] = reinterpret_cast<V(*)[kMaxB]>(sm + L::kDs);
+  const int tid = threadIdx.x, r = tid & 63, cg = tid >> 6;
+  zero_pad_columns(Ys, b, BC);
+
+  constexpr int kUnitElems = kUnitCols * 64;
+  BackwardUnits it{n, b, cs, rank};
+  it.begin();
+  BackwardUnits pf = it;
+  for (int s = 0; s < 2; ++s) {
+    if (!pf.done()) {
+      stage_block(Ls + s * kUnitElems, F, ld, pf.t * 64, pf.k + pf.h * kUnitCols, pf.ncol());
+      pf.next();
+    }
+    cp_async_commit();
+  }
+  int stage = 0;
   int k = n, kb = b;  // the central block first
   for (;;) {
     for (int e = tid; e < kb * b; e += 256) {
-      const int r = e % kb, c = e / kb;
-      const size_t idx = (size_t)(k + r) + (size_t)c * ld;
+      const int rr = e % kb, c = e / kb;
+      const size_t idx = (size_t)(k + rr) + (size_t)c * ld;
       const double2 y = __ldcg(J.Y + idx);
-      Ys[r][c] = y;
+      Ys[rr][c] = to_v<V>(y);
       if (rank == 0) {
         if (mode == 0) {
           J.X[idx] = y;
@@ -139,62 +337,112 @@ __global__ void __cluster_dims__(kClus, 1, 1) __launch_bounds__(256)
         }
       }
     }
-    __syncthreads();
-    // Y[0:k] -= F[0:k, k:k+kb] Y_k over absolute 64-row tiles
-    for (int t = rank; t * 64 < k; t += kClus) {
-      const int gr = t * 64 + tr;
-      if (gr >= k) continue;
-      double2 acc[kMaxB / 4];
+    while (!it.done() && it.k == k) {
+      const int t = it.t;
+      V acc[NJ];
 #pragma unroll
-      for (int j = 0; j < kMaxB / 4; ++j) acc[j] = make_double2(0.0, 0.0);
-      const T *urow = F + (size_t)gr + (size_t)k * ld;
-#pragma unroll 8
-      for (int jj = 0; jj < kb; ++jj) {
-        const double2 a = ldc(urow + (size_t)jj * ld);
+      for (int j = 0; j < NJ; ++j) acc[j] = vzero<V>();
+      do {
+        cp_async_wait<1>();
+        __syncthreads();
+        unit_product<T, V, NJ>(acc, Ls + stage * kUnitElems, Ys, it.h * kUnitCols, it.ncol(), r, cg);
+        __syncthreads();
+        if (!pf.done()) {
+          stage_block(Ls + stage * kUnitElems, F, ld, pf.t * 64, pf.k + pf.h * kUnitCols, pf.ncol());
+          pf.next();
+        }
+        cp_async_commit();
+        stage ^= 1;
+        it.next();
+      } while (!it.done() && it.k == k && it.t == t && it.h != 0);
+      // Y[tile] -= W[tile, k:k+kb] Y_k for the rows above the block
+      const int gr = t * 64 + r;
+      if (gr < k) {
 #pragma unroll
-        for (int j = 0; j < kMaxB / 4; ++j) {
-          const int c = tc + 4 * j;
-          if (c < b) acc[j] = cfma(a, Ys[jj][c], acc[j]);
+        for (int j = 0; j < NJ; ++j) {
+          const int c = cg + 4 * j;
+          if (c >= b) continue;
+          double2 *dst = J.Y + (size_t)gr + (size_t)c * ld;
+          *dst = to_d(csub(to_v<V>(__ldcg(dst)), acc[j]));
         }
       }
-#pragma unroll
-      for (int j = 0; j < kMaxB / 4; ++j) {
-        const int c = tc + 4 * j;
-        if (c >= b) continue;
-        double2 *dst = J.Y + (size_t)gr + (size_t)c * ld;
-        *dst = csub(__ldcg(dst), acc[j]);
-      }
     }
-    cluster_sync();  // Y_(next k) complete; Ys free again
+    cluster_sync();  // Y of the next block is final; Ys is free again
     if (k == 0) break;
-    k = (k == n) ? last : k - kNb;
-    kb = min(kNb, n - k);
+    k = (k == n) ? ((n - 1) / 64) * 64 : k - 64;
+    kb = min(64, n - k);
   }
+  cp_async_wait<0>();
 }
 
-template <typename T>
-cudaError_t sweep_impl(const JobDev *jobs, int njobs, bool forward, int mode, cudaStream_t s) {
-  const dim3 grid(kClus, njobs);
-  if (forward) {
-    const int smem = forward_smem_bytes<T>();
-    cudaError_t e = cudaFuncSetAttribute(forward_sweep_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         smem);
-    if (e != cudaSuccess) return e;
-    forward_sweep_kernel<T><<<grid, 256, smem, s>>>(jobs);
-  } else {
-    backward_sweep_kernel<T><<<grid, 256, 0, s>>>(jobs, mode);
+int g_num_sms = 0;
+
+// Cluster size for a wave of njobs: the largest power of two up to 8 with cs * njobs CTAs
+// resident at once (one CTA per SM at these shared-memory sizes).
+int pick_cluster(int njobs) {
+  if (g_num_sms == 0) {
+    int dev = 0, v = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess &&
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && v > 0)
+      g_num_sms = v;
+    else
+      g_num_sms = 148;
   }
-  return cudaGetLastError();
+  int cs = kMaxCluster;
+  while (cs > 1 && cs * njobs > g_num_sms) cs >>= 1;
+  return cs;
+}
+
+template <typename Kern, typename... Args>
+cudaError_t launch_cluster(Kern kern, int cs, int njobs, int smem, cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(cs, njobs, 1);
+  cfg.blockDim = dim3(256, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = cs;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
+template <typename T, typename V, int BC>
+cudaError_t sweep_impl(const JobDev *jobs, int njobs, bool forward, int mode, cudaStream_t s) {
+  const int cs = pick_cluster(njobs);
+  cudaError_t e;
+  if (forward) {
+    const int smem = SweepSmem<T, V>::kForward;
+    if ((e = cudaFuncSetAttribute(forward_sweep_kernel<T, V, BC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  smem)) != cudaSuccess)
+      return e;
+    return launch_cluster(forward_sweep_kernel<T, V, BC>, cs, njobs, smem, s, jobs);
+  }
+  const int smem = SweepSmem<T, V>::kBackward;
+  if ((e = cudaFuncSetAttribute(backward_sweep_kernel<T, V, BC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                smem)) != cudaSuccess)
+    return e;
+  return launch_cluster(backward_sweep_kernel<T, V, BC>, cs, njobs, smem, s, jobs, mode);
+}
+
+template <typename T, typename V>
+cudaError_t sweep_b(const JobDev *jobs, int njobs, int b, bool forward, int mode, cudaStream_t s) {
+  return b <= 16 ? sweep_impl<T, V, 16>(jobs, njobs, forward, mode, s)
+                 : sweep_impl<T, V, 32>(jobs, njobs, forward, mode, s);
 }
 
 }  // namespace
 
 cudaError_t launch_sweep(FactorKind fk, const JobDev *jobs, int njobs, int b, bool forward, int mode,
-                         cudaStream_t s) {
+                         bool fp32_arith, cudaStream_t s) {
   if (njobs <= 0) return cudaSuccess;
-  if (b > kMaxB || (forward && mode != 1)) return cudaErrorInvalidValue;
-  return fk == kFactorFP64 ? sweep_impl<double2>(jobs, njobs, forward, mode, s)
-                           : sweep_impl<float2>(jobs, njobs, forward, mode, s);
+  if (b < 1 || b > kMaxB || (forward && mode != 1)) return cudaErrorInvalidValue;
+  if (fk == kFactorFP64) return sweep_b<double2, double2>(jobs, njobs, b, forward, mode, s);
+  if (fp32_arith) return sweep_b<float2, float2>(jobs, njobs, b, forward, mode, s);
+  return sweep_b<float2, double2>(jobs, njobs, b, forward, mode, s);
 }
 
 }  // namespace b200

@@ -38,6 +38,8 @@ PREC_FP64 = 0
 PREC_MIXED = 1
 ENGINE_TENSOR = 0
 ENGINE_SIMT = 1
+SWEEP_FP64 = 0
+SWEEP_FP32 = 1
 
 # Symbols declared in include/b200tau.h.
 EXPORTS = (
@@ -46,7 +48,7 @@ EXPORTS = (
     "b200tau_sync", "b200tau_solve_dense", "b200tau_build_kkr", "b200tau_last_launch_count",
     "b200tau_gaunt_numbers", "b200tau_set_refinement", "b200tau_set_profiling",
     "b200tau_profile_read", "b200tau_set_mixed_engine", "b200tau_solve_dense_noalloc",
-    "b200tau_profile_phases",
+    "b200tau_profile_phases", "b200tau_set_mixed_sweep",
 )
 
 
@@ -97,6 +99,7 @@ def load_library():
     lib.b200tau_set_mixed_engine.argtypes = [P, I]
     lib.b200tau_profile_read.argtypes = [P, P, P, P]
     lib.b200tau_profile_phases.argtypes = [P, P]
+    lib.b200tau_set_mixed_sweep.argtypes = [P, I]
     _lib = lib
     return lib
 
@@ -173,6 +176,10 @@ class TauSolver:
     def set_mixed_engine(self, engine: int):
         """Trailing-update engine of the mixed path: ENGINE_TENSOR (tcgen05) or ENGINE_SIMT."""
         self._check(self.lib.b200tau_set_mixed_engine(self.ctx, engine))
+
+    def set_mixed_sweep(self, sweep: int):
+        """Arithmetic of the mixed path's correction solve: SWEEP_FP32 (default) or SWEEP_FP64."""
+        self._check(self.lib.b200tau_set_mixed_sweep(self.ctx, sweep))
 
     def set_profiling(self, enable: bool):
         self._check(self.lib.b200tau_set_profiling(self.ctx, int(bool(enable))))

@@ -109,6 +109,24 @@ def test_n2160_contour_points_match_reference(solver_factory, ref):
         assert tau_err(prob, i, 0, mixed[k], want) <= TOL_MIXED, (i, tau_err(prob, i, 0, mixed[k], want))
 
 
+@pytest.mark.parametrize("sweep", [T.SWEEP_FP32, T.SWEEP_FP64])
+def test_n2160_full_contour_mixed_vs_fp64(solver_factory, sweep):
+    """Every point of the 31-point contour at N=2160 (condition numbers 4e2..5e4): the mixed path
+    after its adaptive refinement stays within 1e-10 of the FP64 path (which matches the
+    reference to 1e-12 at the sampled points above)."""
+    prob = W.config_n2160()
+    s = _solver(solver_factory, prob)
+    s.set_mixed_sweep(sweep)
+    try:
+        jobs = T.make_jobs([(0, i, 0, prob.energies[i]) for i in range(len(prob.energies))])
+        fp64 = s.solve_jobs(jobs, T.PREC_FP64)
+        mixed = s.solve_jobs(jobs, T.PREC_MIXED)
+    finally:
+        s.set_mixed_sweep(T.SWEEP_FP32)
+    errs = [tau_err(prob, i, 0, mixed[i], fp64[i]) for i in range(len(prob.energies))]
+    assert max(errs) <= TOL_MIXED, errs
+
+
 def test_batched_equals_one_at_a_time(solver_factory):
     prob = W.make_problem("fcc", 6.82, 4, 3, W.semicircle_contour(-0.3, 0.7, 6), 21, n_species=2)
     s = _solver(solver_factory, prob)
@@ -180,17 +198,21 @@ def test_errors_are_reported(solver_factory):
     fresh.close()
 
 
+@pytest.mark.parametrize("sweep", [T.SWEEP_FP32, T.SWEEP_FP64])
 @pytest.mark.parametrize("engine", [T.ENGINE_TENSOR, T.ENGINE_SIMT])
-def test_mixed_engines_match_reference(solver_factory, ref, engine):
-    """Both trailing-update engines of the mixed path (tcgen05 TF32 hi/lo and FP32 CUDA cores)
-    reach the mixed tolerance after refinement on an N=688 problem near the real axis."""
+def test_mixed_engines_match_reference(solver_factory, ref, engine, sweep):
+    """Both trailing-update engines of the mixed path (tcgen05 TF32 hi/lo and FP32 CUDA cores),
+    with the correction solve in FP32 or FP64 arithmetic, reach the mixed tolerance after
+    refinement on an N=688 problem near the real axis."""
     prob = W.make_problem("fcc", 6.82, 3, 3, [0.45 + 0.01j, 0.1 + 0.3j], 41, n_species=2)
     s = _solver(solver_factory, prob)
     s.set_mixed_engine(engine)
+    s.set_mixed_sweep(sweep)
     try:
         out = s.solve_jobs(T.make_jobs([(0, i, 0, prob.energies[i]) for i in range(2)]), T.PREC_MIXED)
     finally:
         s.set_mixed_engine(T.ENGINE_TENSOR)
+        s.set_mixed_sweep(T.SWEEP_FP32)
     for i in range(2):
         want = ref.calculate_tau(prob, i, 0, ref.ZBLOCKLU_CPP)
         assert tau_err(prob, i, 0, out[i], want) <= TOL_MIXED, (engine, i, tau_err(prob, i, 0, out[i], want))
@@ -205,7 +227,7 @@ def test_mixed_without_refinement_is_fp32_accurate(solver_factory, ref):
     try:
         out = s.calculate_tau_matrix(0, 0, prob.energies[0], 0, T.PREC_MIXED)
     finally:
-        s.set_refinement(T.PREC_MIXED, 3)
+        s.set_refinement(T.PREC_MIXED, 6)
     want = ref.calculate_tau(prob, 0, 0, ref.ZBLOCKLU_CPP)
     err = tau_err(prob, 0, 0, out, want)
     assert 1e-12 < err < 1e-3, err
