@@ -295,7 +295,7 @@ def main():
                                    "31-point semicircle contour -0.3..0.7 Ry, one atom per GPU",
                        "solves_per_step": ne, "l2": "inputs larger than L2 "
                        f"({ne} x {N * N * 16 / 1e6:.0f} MB KKR matrices per step)",
-                       "refinement_steps_mixed": "up to 6, per job until the correction estimate < 1e-13",
+                       "refinement_steps_mixed": "up to 6, per job until the correction estimate < 1e-12",
                        "refinement_steps_fp64": 1},
             "fp64": {"value": fp64_value, "unit": "solves/s", "ms_per_step": ms_fp64,
                      "mixed_over_fp64": value / fp64_value},

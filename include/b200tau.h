@@ -101,7 +101,7 @@ int b200tau_set_atom(b200tau_ctx *ctx, int atom, int num_liz,
  * solvers, linearSolvers_CPU.cpp:148-174, linearSolvers_CUDA.cu:424-469, on the N x b
  * system).  Defaults: FP64 1 step, MIXED 6 steps, of which each job runs only as many as it
  * needs: after every step but the last, a job whose estimated remaining error (the relative size
- * c of the correction just applied times its contraction c / c_previous) is below 1e-13 of
+ * c of the correction just applied times its contraction c / c_previous) is below 1e-12 of
  * tau00 stops.  FP64 with 0 steps takes tau00 directly from the Schur complement like
  * zblock_lu. */
 int b200tau_set_refinement(b200tau_ctx *ctx, int prec, int steps);
@@ -160,6 +160,23 @@ int b200tau_solve_dense_noalloc(const double *m, int n, int ldm, const double *t
  * path.  Returns B200TAU_ERR_ARG if m_out's n does not match. */
 int b200tau_build_kkr(b200tau_ctx *ctx, const b200tau_job *job, double *m_out,
                       int n);
+
+/* Reverse-mode derivatives, for each job, of tau00 and of ln det M with respect to the
+ * t-matrix t_j of every LIZ site j, from the FP64 block factors of the job's own forward solve
+ * (one factorisation; M^-1 is formed from the factors).  No counterpart in the reference.
+ *   taubar  (in)  b x b cotangent on the raw tau00 = [M^-1]_00 t_0 of each job (not minus t0,
+ *                 unrotated), jobs one after another (2 b^2 doubles per job).
+ *   tau00   (out) that tau00 per job, or NULL.
+ *   tbar    (out) sum_ab taubar_ab d tau00_ab / d (t_j)_xy as a b x b block per LIZ site
+ *                 (holomorphic convention: no conjugation);
+ *   dlogdet (out) d ln det M / d (t_j)_xy per LIZ site, same layout, or NULL.
+ * Gradient blocks are column-major b x b in the t-matrix store layout (row s kkrsz + lm; zero
+ * for lm >= (lmax_j + 1)^2), in LIZ order (site 0 first); job k's blocks start at block
+ * sum_{i<k} num_liz(atom of job i).  A caller wanting the torch/JAX convention for a real loss
+ * conjugates: grad_t = conj(tbar(conj(grad_tau))). */
+int b200tau_solve_vjp(b200tau_ctx *ctx, const b200tau_job *jobs, int njobs,
+                      const double *taubar, double *tau00, double *tbar,
+                      double *dlogdet);
 
 /* The Gaunt numbers this library builds its G0 tables from (host-only, no GPU needed):
  * cgnt[l3/2 + (lmax+1) * (j1 + kk * j2)], kk = (lmax+1)^2, the layout of the reference's

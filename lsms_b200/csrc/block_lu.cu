@@ -26,6 +26,7 @@
 
 #include "common.cuh"
 #include "cplx.cuh"
+#include "gj.cuh"
 
 namespace b200 {
 namespace {
@@ -292,64 +293,6 @@ __global__ void __launch_bounds__(256, 2) zgemm_tile_kernel(const JobDev *__rest
   }
 }
 
-// ---------------------------------------------------------------------------------------------
-// Small b x b solves by Gauss-Jordan on [A | rhs] in shared memory (FP64, partial pivoting).
-// A is kMaxB x (2 kMaxB + 1); on return columns [b, 2b) hold A^-1 rhs.  Returns singular.
-// ---------------------------------------------------------------------------------------------
-__device__ bool gj_solve_smem(double2 (*A)[2 * kMaxB + 1], int b, int *s_piv, double2 *s_dinv) {
-  const int tid = threadIdx.x;
-  bool singular = false;
-  for (int p = 0; p < b; ++p) {
-    if (tid < 32) {
-      double best = -1.0;
-      int bi = p;
-      for (int r = p + tid; r < b; r += 32) {
-        const double v = cabs1(A[r][p]);
-        if (v > best) {
-          best = v;
-          bi = r;
-        }
-      }
-      for (int o = 16; o > 0; o >>= 1) {
-        const double ob = __shfl_down_sync(0xffffffffu, best, o);
-        const int oi = __shfl_down_sync(0xffffffffu, bi, o);
-        if (ob > best || (ob == best && oi < bi)) {
-          best = ob;
-          bi = oi;
-        }
-      }
-      if (tid == 0) *s_piv = bi;
-    }
-    __syncthreads();
-    const int pv = *s_piv;
-    if (pv != p)
-      for (int c = tid; c < 2 * b; c += blockDim.x) {
-        const double2 t = A[p][c];
-        A[p][c] = A[pv][c];
-        A[pv][c] = t;
-      }
-    __syncthreads();
-    if (tid == 0) {
-      const double2 d = A[p][p];
-      *s_dinv = (d.x == 0.0 && d.y == 0.0) ? make_double2(0.0, 0.0) : crecip(d);
-    }
-    __syncthreads();
-    const double2 dinv = *s_dinv;
-    if (dinv.x == 0.0 && dinv.y == 0.0) singular = true;
-    for (int c = tid; c < 2 * b; c += blockDim.x) A[p][c] = cmul(A[p][c], dinv);
-    __syncthreads();
-    for (int e = tid; e < b * 2 * b; e += blockDim.x) {
-      const int r = e / (2 * b), c = e - r * 2 * b;
-      if (r == p || c <= p) continue;
-      A[r][c] = csub(A[r][c], cmul(A[r][p], A[p][c]));
-    }
-    __syncthreads();
-    for (int r = tid; r < b; r += blockDim.x)
-      if (r != p) A[r][p] = make_double2(0.0, 0.0);
-    __syncthreads();
-  }
-  return singular;
-}
 
 // out = tau00 (out_mode 1) or rotate(tau00 - t0) (out_mode 0), tau00 in A[r][b + c].
 __device__ void write_out(const JobDev &J, double2 (*A)[2 * kMaxB + 1], int ns, int kkrsz) {
@@ -685,7 +628,7 @@ cudaError_t launch_refine_round(FactorKind fk, const JobDev *jobs, int njobs, in
                                            : sweep_solve<float2>(jobs, njobs, b, 1, info, s, launches, fp32_sweep);
   if (e != cudaSuccess) return e;
   if (check) {
-    converge_check_kernel<<<njobs, 256, 0, s>>>(jobs, 1e-13);
+    converge_check_kernel<<<njobs, 256, 0, s>>>(jobs, kRefineTol);
     if (launches) *launches += 1;
   }
   return cudaGetLastError();

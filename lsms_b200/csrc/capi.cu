@@ -77,11 +77,17 @@ struct b200tau_ctx {
   double2 *d_out = nullptr;
   size_t out_cap = 0;
   double2 *d_t0 = nullptr;  // dense-solve t0
+  // adjoint (b200tau_solve_vjp): M^-1 per slot, and the call's cotangents / gradients
+  double2 *d_V = nullptr;
+  size_t v_elems = 0;
+  int v_slots = 0;
+  double2 *d_adj = nullptr;
+  size_t adj_cap = 0;
   unsigned char *d_tdiag = nullptr;  // per (store, energy, spin) t block: exactly diagonal
   long launches = 0;
   int max_slots = 64;
   // refinement rounds, FP64 and MIXED; MIXED stops early per job once the correction estimate
-  // is below 1e-13 of tau00 (block_lu.cu, converge_check_kernel)
+  // is below kRefineTol of tau00 (block_lu.cu, converge_check_kernel)
   int refine_steps[2] = {1, 6};
   // profiling of the trailing-update launches (b200tau_set_profiling)
   bool profiling = false;
@@ -200,13 +206,13 @@ int ensure_out(b200tau_ctx *ctx, size_t n) {
   return B200TAU_OK;
 }
 
-int choose_slots(b200tau_ctx *ctx, int ld, int njobs, const Plan &p) {
+int choose_slots(b200tau_ctx *ctx, int ld, int njobs, const Plan &p, size_t extra_per_slot = 0) {
   size_t freeb = 0, totalb = 0;
   if (cudaMemGetInfo(&freeb, &totalb) != cudaSuccess) freeb = (size_t)8 << 30;
   // memory already held by the context's workspace counts as available to it
   freeb += ctx->m_elems * ctx->slots * sizeof(double2) + ctx->f_bytes * ctx->slots;
   const size_t per = (size_t)ld * ld * (sizeof(double2) + (p.f_separate ? f_elem_bytes(p) : 0)) +
-                     (size_t)3 * ld * kMaxB * sizeof(double2);
+                     (size_t)3 * ld * kMaxB * sizeof(double2) + extra_per_slot;
   const size_t budget = freeb / 2;
   int s = (int)std::max<size_t>(1, budget / std::max<size_t>(per, 1));
   s = std::min(s, ctx->max_slots);
@@ -248,6 +254,7 @@ BuildParams build_params(const b200tau_ctx *ctx, const Plan &p) {
   bp.f_kind = !p.f_separate ? 0 : (p.fk == kFactorFP32 ? 2 : 1);
   bp.tdiag = ctx->d_tdiag;
   bp.group = ctx->group_size;
+  bp.g_mode = 0;
   return bp;
 }
 
@@ -464,8 +471,16 @@ int run_pipeline(b200tau_ctx *ctx, const std::vector<JobDev> &h, int nw, int max
   return phase_end(ctx, 2);
 }
 
+// Device buffers of one b200tau_solve_vjp call (job-indexed in the caller's order).
+struct AdjointBufs {
+  const double2 *taubar;   // njobs x b x b
+  double2 *tbar;           // sum of L over jobs, x b x b
+  double2 *dlogdet;        // same, or null
+  const long *site_off;    // host: first output block of each job
+};
+
 int run_wave(b200tau_ctx *ctx, const b200tau_job *jobs, const int *idx, int nw, int ld, const Plan &p,
-             double2 *out_base) {
+             double2 *out_base, const AdjointBufs *adj = nullptr) {
   std::vector<JobDev> h(nw);
   int maxL = 0, maxN = 0, maxn = 0;
   for (int w = 0; w < nw; ++w) {
@@ -492,6 +507,14 @@ int run_wave(b200tau_ctx *ctx, const b200tau_job *jobs, const int *idx, int nw, 
     J.t0_ld = ctx->b;
     J.out = out_base + (size_t)idx[w] * ctx->b * ctx->b;
     J.out_mode = 0;
+    if (adj) {  // raw tau00 out; M^-1 workspace; this job's cotangent and gradient blocks
+      const size_t bb = (size_t)ctx->b * ctx->b;
+      J.out_mode = 1;
+      J.V = ctx->d_V + (size_t)w * ctx->v_elems;
+      J.taubar = adj->taubar + (size_t)idx[w] * bb;
+      J.tbar = adj->tbar + (size_t)adj->site_off[idx[w]] * bb;
+      J.dlogdet = adj->dlogdet ? adj->dlogdet + (size_t)adj->site_off[idx[w]] * bb : nullptr;
+    }
     for (int k = 0; k < 4; ++k) {
       J.ubr[k] = a.ubr[k];
       J.ubrd[k] = a.ubrd[k];
@@ -506,7 +529,17 @@ int run_wave(b200tau_ctx *ctx, const b200tau_job *jobs, const int *idx, int nw, 
   CK(launch_kkr_build(ctx->d_jobs, nw, maxL, build_params(ctx, p), ctx->d_err, ctx->stream, &ctx->launches));
   if ((rc = phase_end(ctx, 0))) return rc;
   if (ctx->profiling) ctx->prof_flops += trailing_flops(h);
-  return run_pipeline(ctx, h, nw, maxn, maxN, ld, ctx->ns, ctx->kkrsz, ctx->b, p);
+  if ((rc = run_pipeline(ctx, h, nw, maxn, maxN, ld, ctx->ns, ctx->kkrsz, ctx->b, p))) return rc;
+  if (!adj) return B200TAU_OK;
+  // adjoint: G into M's storage (M is no longer needed once X is refined), M^-1 from the factors,
+  // then the per-site contractions
+  BuildParams gp = build_params(ctx, p);
+  gp.f_kind = 0;
+  gp.g_mode = 1;
+  CK(launch_kkr_build(ctx->d_jobs, nw, maxL, gp, ctx->d_err, ctx->stream, &ctx->launches));
+  CK(launch_inverse(ctx->d_jobs, nw, maxn, maxN, ctx->stream, &ctx->launches));
+  CK(launch_vjp_assemble(ctx->d_jobs, nw, maxL, ctx->kkrsz, ctx->ns, ctx->stream, &ctx->launches));
+  return B200TAU_OK;
 }
 
 int check_info(b200tau_ctx *ctx, const std::vector<int> &info, const int *idx, int nw) {
@@ -643,6 +676,8 @@ void b200tau_destroy(b200tau_ctx *ctx) {
   cudaFree(ctx->d_t0);
   cudaFree(ctx->d_tdiag);
   cudaFree(ctx->d_pack);
+  cudaFree(ctx->d_V);
+  cudaFree(ctx->d_adj);
   for (auto &e : ctx->events) cudaEventDestroy(e);
   for (auto &e : ctx->pev) cudaEventDestroy(e);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -917,6 +952,75 @@ int b200tau_solve_dense(b200tau_ctx *ctx, const double *m, int n, int ldm, const
   CK(cudaStreamSynchronize(ctx->stream));
   if (info) return fail(ctx, B200TAU_ERR_SINGULAR, "solve_dense: singular pivot (info %d)", info);
   return B200TAU_OK;
+}
+
+int b200tau_solve_vjp(b200tau_ctx *ctx, const b200tau_job *jobs, int njobs, const double *taubar,
+                      double *tau00, double *tbar, double *dlogdet) {
+  if (!ctx) return B200TAU_ERR_ARG;
+  if (njobs < 0 || (njobs > 0 && (!jobs || !taubar || !tbar)))
+    return fail(ctx, B200TAU_ERR_ARG, "solve_vjp: bad arguments");
+  if (njobs == 0) return B200TAU_OK;
+  CK(cudaSetDevice(ctx->device));
+  int rc = validate_jobs(ctx, jobs, njobs);
+  if (rc) return rc;
+  Plan p = plan_for(ctx, B200TAU_PREC_FP64);
+  p.steps = std::max(p.steps, 1);  // X refined against M before the adjoint uses it
+  p.f_separate = true;
+  std::vector<int> order(njobs);
+  for (int j = 0; j < njobs; ++j) order[j] = j;
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) {
+    return ctx->atoms[jobs[a].atom].N > ctx->atoms[jobs[b].atom].N;
+  });
+  const int maxN = ctx->atoms[jobs[order[0]].atom].N;
+  const int ld = round_up(maxN, 64);
+  const size_t v_need = (size_t)ld * ld;
+  const int slots = choose_slots(ctx, ld, njobs, p, v_need * sizeof(double2));
+  if ((rc = ensure_workspace(ctx, ld, slots, p))) return rc;
+  if ((rc = ensure_jobs(ctx, slots))) return rc;
+  if (!ctx->d_V || v_need > ctx->v_elems || slots > ctx->v_slots) {
+    CK(cudaStreamSynchronize(ctx->stream));
+    cudaFree(ctx->d_V);
+    ctx->d_V = nullptr;
+    ctx->v_elems = std::max(v_need, ctx->v_elems);
+    ctx->v_slots = std::max(slots, ctx->v_slots);
+    CK(cudaMalloc(&ctx->d_V, sizeof(double2) * ctx->v_elems * ctx->v_slots));
+  }
+  // output blocks: job j's sites start at block site_off[j] (caller's job order)
+  std::vector<long> site_off(njobs + 1, 0);
+  for (int j = 0; j < njobs; ++j) site_off[j + 1] = site_off[j] + ctx->atoms[jobs[j].atom].L;
+  const size_t bb = (size_t)ctx->b * ctx->b;
+  const size_t nblk = (size_t)site_off[njobs];
+  const size_t need = bb * (njobs + nblk * (dlogdet ? 2 : 1));
+  if (need > ctx->adj_cap) {
+    CK(cudaStreamSynchronize(ctx->stream));
+    cudaFree(ctx->d_adj);
+    ctx->d_adj = nullptr;
+    CK(cudaMalloc(&ctx->d_adj, sizeof(double2) * need));
+    ctx->adj_cap = need;
+  }
+  AdjointBufs adj;
+  adj.taubar = ctx->d_adj;
+  adj.tbar = ctx->d_adj + bb * njobs;
+  adj.dlogdet = dlogdet ? adj.tbar + bb * nblk : nullptr;
+  adj.site_off = site_off.data();
+  if ((rc = ensure_out(ctx, bb * njobs))) return rc;
+  CK(cudaMemcpyAsync(ctx->d_adj, taubar, sizeof(double2) * bb * njobs, cudaMemcpyHostToDevice, ctx->stream));
+  ctx->launches = 0;
+  std::vector<int> info(slots);
+  for (int w0 = 0; w0 < njobs; w0 += slots) {
+    const int nw = std::min(slots, njobs - w0);
+    if ((rc = run_wave(ctx, jobs, &order[w0], nw, ld, p, ctx->d_out, &adj))) return rc;
+    CK(cudaMemcpyAsync(info.data(), ctx->d_info, sizeof(int) * nw, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if ((rc = check_info(ctx, info, &order[w0], nw))) return rc;
+  }
+  if (tau00)
+    CK(cudaMemcpyAsync(tau00, ctx->d_out, sizeof(double2) * bb * njobs, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(tbar, adj.tbar, sizeof(double2) * bb * nblk, cudaMemcpyDeviceToHost, ctx->stream));
+  if (dlogdet)
+    CK(cudaMemcpyAsync(dlogdet, adj.dlogdet, sizeof(double2) * bb * nblk, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return check_err_flags(ctx);
 }
 
 int b200tau_build_kkr(b200tau_ctx *ctx, const b200tau_job *job, double *m_out, int n) {

@@ -17,6 +17,9 @@ constexpr int kNdlm = (kMaxLend + 1) * (kMaxLend + 2) / 2;       // 28 P_lm valu
 constexpr int kNdlj = (kMaxLend + 1) * (kMaxLend + 1);           // 49 D_lm values
 constexpr int kMaxTerms = kMaxLmax + 1;                          // Gaunt terms per G element
 constexpr int kNb = 64;                                         // elimination block width
+// A refining job stops once its estimated remaining error on tau00 is below this fraction of
+// max|tau00|: 100x below the mixed path's 1e-10 accuracy target.
+constexpr double kRefineTol = 1e-12;
 
 // Angular-momentum tables for G_ij (makegij_c.f:79-128, buildKKRMatrix_CPU.cpp:144-176),
 // laid out as a gather list: G(lm2, lm1) = pi4 * i^rot * sum_q coef[q] * D[didx[q]]
@@ -78,6 +81,11 @@ struct JobDev {
   int t0_ld;
   int out_mode;          // 0: tau00_l (tau00 - t0, rotated); 1: raw tau00
   int pad_[3];
+  // adjoint (b200tau_solve_vjp) only
+  double2 *V;            // N x N workspace for M^-1 (ld)
+  const double2 *taubar; // b x b cotangent on tau00
+  double2 *tbar;         // L blocks of b x b, LIZ site order: d<taubar, tau00>/d t_site
+  double2 *dlogdet;      // L blocks of b x b: d ln det M / d t_site (may be null)
 };
 
 struct BuildParams {
@@ -91,6 +99,8 @@ struct BuildParams {
   int f_kind;                   // 0: no F copy (F aliases M), 1: FP64 copy, 2: FP32 copy
   const unsigned char *tdiag;   // [(store * group + iie) * 2 + ispin]: t block exactly diagonal
   int group;                    // energies in the uploaded tmatStore group
+  int g_mode;                   // 1: write the structure constants G (no t factor, zero diagonal
+                                // blocks) into M instead of M = 1 - t G (adjoint)
 };
 
 enum FactorKind { kFactorFP64 = 0, kFactorFP32 = 1 };
@@ -150,5 +160,10 @@ cudaError_t launch_refine_end(const JobDev *jobs, int njobs, int ns, int kkrsz, 
 // X (+)= Y).  `fp32_arith` selects FP32 arithmetic on FP32 factors.
 cudaError_t launch_sweep(FactorKind fk, const JobDev *jobs, int njobs, int b, bool forward, int mode,
                          bool fp32_arith, cudaStream_t s);
+// Adjoint (adjoint.cu), FP64 factors: V = M^-1 from the block factors in F, then per LIZ site the
+// tau00 cotangent pull-back and d ln det M / d t (needs G in M, X refined, V).
+cudaError_t launch_inverse(const JobDev *jobs, int njobs, int max_n, int max_N, cudaStream_t s, long *launches);
+cudaError_t launch_vjp_assemble(const JobDev *jobs, int njobs, int max_L, int kkrsz, int ns, cudaStream_t s,
+                                long *launches);
 
 }  // namespace b200

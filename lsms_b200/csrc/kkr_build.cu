@@ -142,10 +142,11 @@ __global__ void __launch_bounds__(kThreads)
     const int kki = (li + 1) * (li + 1);
     const int row0 = J.off[pr];
     const int nr = ns * kki, nc = ns * kkj;
-    if (pr == pc) {  // diagonal block: identity (buildKKRMatrix_CPU.cpp:266-268)
+    if (pr == pc) {  // diagonal block: identity (buildKKRMatrix_CPU.cpp:266-268); G_ii = 0
+      const double one = p.g_mode ? 0.0 : 1.0;
       for (int c = 0; c < nc; ++c)
         for (int r = lane; r < nr; r += 32)
-          put((size_t)(row0 + r) + (size_t)(col0 + c) * ld, make_double2(r == c ? 1.0 : 0.0, 0.0));
+          put((size_t)(row0 + r) + (size_t)(col0 + c) * ld, make_double2(r == c ? one : 0.0, 0.0));
       continue;
     }
     // rij = pos(ir1) - pos(ir2), ir1 = row site (calculateTauMatrix.cpp:206-208)
@@ -253,6 +254,17 @@ __global__ void __launch_bounds__(kThreads)
       sm.G[warp][lm2 * kMaxKK + lm1] = g;
     }
     __syncwarp();
+    if (p.g_mode) {  // G itself, spin-diagonal (setgij.f:29-38 without the t factor)
+      for (int rr = lane & 15; rr < nr; rr += 16) {
+        const int sr = rr / kki, rp = rr - sr * kki;
+        for (int sc = 0; sc < ns; ++sc)
+          for (int cp = lane >> 4; cp < kkj; cp += 2)
+            put((size_t)(row0 + rr) + (size_t)(col0 + sc * kkj + cp) * ld,
+                sc == sr ? sm.G[warp][rp * kMaxKK + cp] : make_double2(0.0, 0.0));
+      }
+      __syncwarp();
+      continue;
+    }
     // M block = -t_i * diag_s(G): rows (s_r, r'), columns (s_c, c') (setgij.f:29-38)
     const double2 *__restrict__ tb =
         p.tmat + (long)J.store[i] * p.tmat_ld + (long)J.iie * p.blk + jsm;

@@ -48,7 +48,7 @@ EXPORTS = (
     "b200tau_sync", "b200tau_solve_dense", "b200tau_build_kkr", "b200tau_last_launch_count",
     "b200tau_gaunt_numbers", "b200tau_set_refinement", "b200tau_set_profiling",
     "b200tau_profile_read", "b200tau_set_mixed_engine", "b200tau_solve_dense_noalloc",
-    "b200tau_profile_phases", "b200tau_set_mixed_sweep",
+    "b200tau_profile_phases", "b200tau_set_mixed_sweep", "b200tau_solve_vjp",
 )
 
 
@@ -100,6 +100,7 @@ def load_library():
     lib.b200tau_profile_read.argtypes = [P, P, P, P]
     lib.b200tau_profile_phases.argtypes = [P, P]
     lib.b200tau_set_mixed_sweep.argtypes = [P, I]
+    lib.b200tau_solve_vjp.argtypes = [P, P, I, P, P, P, P]
     _lib = lib
     return lib
 
@@ -262,6 +263,28 @@ class TauSolver:
                                                  t0f.ctypes.data_as(ctypes.c_void_p), b, prec,
                                                  out.ctypes.data_as(ctypes.c_void_p)))
         return np.array(out)
+
+    def solve_vjp(self, jobs, taubar: np.ndarray, num_liz, want_logdet: bool = True):
+        """Adjoint of each job's raw tau00 (b200tau_solve_vjp).
+
+        taubar: (njobs, b, b) cotangents ([row, col]).  num_liz: LIZ size of each job's atom.
+        Returns (tau00 (njobs, b, b), tbar, dlogdet) with tbar / dlogdet a list per job of
+        (L, b, b) arrays [site, row, col] in the store layout (holomorphic: no conjugation)."""
+        n = len(jobs)
+        b = self.kkrsz_ns
+        tb = np.ascontiguousarray(np.asarray(taubar, np.complex128).reshape(n, b, b).transpose(0, 2, 1))
+        tau = np.zeros((n, b, b), np.complex128)
+        nblk = int(np.sum(num_liz))
+        g = np.zeros((nblk, b, b), np.complex128)
+        d = np.zeros((nblk, b, b), np.complex128) if want_logdet else None
+        self._check(self.lib.b200tau_solve_vjp(self.ctx, ctypes.cast(jobs, ctypes.c_void_p), n, _ptr(tb),
+                                               _ptr(tau), _ptr(g), None if d is None else _ptr(d)))
+        offs = np.concatenate([[0], np.cumsum(num_liz)]).astype(int)
+        # stored column-major: [blk, col, row] -> [blk, row, col]
+        tau = tau.transpose(0, 2, 1)
+        gl = [g[offs[k]:offs[k + 1]].transpose(0, 2, 1).copy() for k in range(n)]
+        dl = None if d is None else [d[offs[k]:offs[k + 1]].transpose(0, 2, 1).copy() for k in range(n)]
+        return tau.copy(), gl, dl
 
     def build_kkr(self, atom: int, iie: int, ispin: int, energy: complex, n: int) -> np.ndarray:
         """The device-built KKR matrix in the reference's site order (numpy [row, col])."""
