@@ -164,6 +164,102 @@ def cpu_baseline(prob, seconds_budget=20.0):
             "sample": f"{n} of the 31 contour solves at N=2160, one after another, OpenBLAS on {cores} threads"}
 
 
+WORKLOADS = {
+    "batched": "256 atoms x 32 energies, random fcc alloy with 5% vacancies, LIZ sizes 43..135 "
+               "(N=688..2160), lmax 3, FP64 (and mixed) in one batched call",
+    "noncollinear": "64 atoms x 16 energies, non-collinear kkrsz_ns=32, fcc LIZ 135 sites (N=4320), "
+                    "mixed vs FP64",
+    "adjoint": "64 atoms x 16 energies, fcc LIZ 87 sites (N=1392): tau00 plus d tau00/d t and "
+               "d ln det M/d t for every LIZ site (b200tau_solve_vjp, FP64)",
+}
+
+
+def run_workload(args, world, rank, local):
+    """The other configurations of the benchmark's table, one JSON line each (not the headline):
+    one step = every job of the configuration in one batched call."""
+    import torch
+    from lsms_b200 import tau as T
+    from lsms_b200 import workloads as W
+    torch.cuda.set_device(local)
+    kind = args.workload
+    wl = {"batched": W.config_batched, "noncollinear": W.config_noncollinear_batch,
+          "adjoint": W.config_adjoint_batch}[kind](seed=3 + rank)
+    b = wl.kkrsz_ns
+    s = T.TauSolver(wl.lmax, wl.n_spin_cant, wl.n_spin_pola, device=local)
+    s.upload_tmat(wl.tmat_store)
+    for a, at in enumerate(wl.atoms):
+        s.set_atom(a, at.liz_pos, at.liz_lmax, at.liz_store_idx, at.ubr, at.ubrd)
+    nspin = 2 if wl.n_spin_pola != wl.n_spin_cant else 1
+    specs = [(a, iie, sp, e) for a in range(len(wl.atoms)) for iie, e in enumerate(wl.energies)
+             for sp in range(nspin)]
+    jobs = T.make_jobs(specs)
+    nj = len(specs)
+    flops = sum(algorithmic_flops(wl.nrmat_ns(a), b, wl.atoms[a].num_liz) for a, _, _, _ in specs)
+    stream = torch.cuda.ExternalStream(s.stream, device=f"cuda:{local}")
+    steps, warmup = max(1, args.steps), max(1, min(args.warmup, 1))
+
+    def timed(fn):
+        for _ in range(warmup):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    line = {"metric": f"{kind}: tau00 solves/s", "unit": "solves/s", "n_gpus": world, "steps": steps,
+            "warmup": warmup, "higher_is_better": True, "data": "synthetic",
+            "config": {"workload": WORKLOADS[kind], "jobs_per_step": nj}}
+    if kind == "adjoint":
+        rng = np.random.default_rng(7)
+        tb = rng.normal(size=(nj, b, b)) + 1j * rng.normal(size=(nj, b, b))
+        Ls = [wl.atoms[a].num_liz for a, _, _, _ in specs]
+        res = {}
+
+        def vjp():
+            res["out"] = s.solve_vjp(jobs, tb, Ls)
+        ms = timed(vjp)
+        tau = res["out"][0]
+        fwd = s.solve_jobs(jobs, T.PREC_FP64)
+        t0 = np.stack([wl.tmat_store[wl.atoms[a].liz_store_idx[0], iie, :b * b].reshape(b, b).T
+                       for a, iie, _, _ in specs])
+        fwd = fwd.reshape(nj, b, b).transpose(0, 2, 1) + t0
+        line.update({"metric": "adjoint: tau00 + gradients per site, solves/s", "value": nj / (ms * 1e-3),
+                     "ms_per_step": ms, "dtype": "c128",
+                     "tau00_vs_forward_fp64": float(np.abs(tau - fwd).max() / np.abs(fwd).max()),
+                     "note": "host buffers in and out (taubar, tau00, L gradient blocks per job)"})
+        print(json.dumps(line))
+        s.close()
+        return
+    out = torch.empty(nj * b * b * 2, dtype=torch.float64, device=f"cuda:{local}")
+    res = {}
+    fallbacks = 0
+    for name, prec in (("fp64", T.PREC_FP64), ("mixed", T.PREC_MIXED)):
+        ms = timed(lambda: s.solve_jobs_device(jobs, out.data_ptr(), prec))
+        s.sync()
+        res[name] = (ms, out.cpu().numpy().view(np.complex128).reshape(nj, -1).copy())
+        if name == "mixed":
+            fallbacks = s.last_fallback_count
+    f, m = res["fp64"][1], res["mixed"][1]
+    err = float(max(np.abs(m[j] - f[j]).max() / np.abs(f[j]).max() for j in range(nj)))
+    head = "mixed" if kind == "noncollinear" else "fp64"
+    ms = res[head][0]
+    line.update({"value": nj / (res[head][0] * 1e-3), "ms_per_step": ms,
+                 "dtype": "c64 trailing updates + c128 refinement" if head == "mixed" else "c128",
+                 "fp64": {"value": nj / (res["fp64"][0] * 1e-3), "ms_per_step": res["fp64"][0],
+                          "effective_tflops": flops / (res["fp64"][0] * 1e-3) / 1e12},
+                 "mixed": {"value": nj / (res["mixed"][0] * 1e-3), "ms_per_step": res["mixed"][0],
+                           "effective_tflops": flops / (res["mixed"][0] * 1e-3) / 1e12},
+                 "err_mixed_vs_fp64_on_tau00_l": err,
+                 "mixed_jobs_resolved_in_fp64": fallbacks,
+                 "algorithmic_flops_per_step": flops})
+    print(json.dumps(line))
+    s.close()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -171,6 +267,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="contour2160", choices=["contour2160", *WORKLOADS],
+                    help="contour2160 = the headline line; the others print their own line")
     ap.add_argument("--energies", type=int, default=N_ENERGIES,
                     help="contour points solved per step (31 = the benchmark; fewer for small profiling cases)")
     args = ap.parse_args()
@@ -179,6 +277,9 @@ def main():
 
     if args.impl == "reference":
         run_reference(args, world, rank)
+        return
+    if args.workload != "contour2160":
+        run_workload(args, world, rank, local)
         return
 
     import torch

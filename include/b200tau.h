@@ -100,10 +100,11 @@ int b200tau_set_atom(b200tau_ctx *ctx, int atom, int num_liz,
  * stored block factors (the refinement of the reference's zcgesv / cusolverDnIRSXgesv
  * solvers, linearSolvers_CPU.cpp:148-174, linearSolvers_CUDA.cu:424-469, on the N x b
  * system).  Defaults: FP64 1 step, MIXED 6 steps, of which each job runs only as many as it
- * needs: after every step but the last, a job whose estimated remaining error (the relative size
- * c of the correction just applied times its contraction c / c_previous) is below 1e-12 of
- * tau00 stops.  FP64 with 0 steps takes tau00 directly from the Schur complement like
- * zblock_lu. */
+ * needs: after every step, a job whose estimated remaining error (the relative size c of the
+ * correction just applied times its contraction c / c_previous) is below 1e-12 of tau00 stops.
+ * A MIXED job whose corrections stop shrinking, or that has not converged after the last step,
+ * is re-solved by FP64 block LU (b200tau_last_fallback_count).  FP64 with 0 steps takes tau00
+ * directly from the Schur complement like zblock_lu. */
 int b200tau_set_refinement(b200tau_ctx *ctx, int prec, int steps);
 
 /* Engine of the mixed path's trailing update (B200TAU_ENGINE_*). */
@@ -197,6 +198,15 @@ int b200tau_profile_phases(b200tau_ctx *ctx, double *ms3);
 
 /* Number of kernel launches the last solve issued (for launch accounting). */
 long b200tau_last_launch_count(const b200tau_ctx *ctx);
+
+/* Number of jobs of the last solve whose mixed-precision refinement did not converge (the FP32
+ * factors cannot refine a condition number much beyond ~1e5) and that were re-solved by FP64
+ * block LU of their KKR matrix instead. */
+long b200tau_last_fallback_count(const b200tau_ctx *ctx);
+
+/* Turn that FP64 re-solve off (0) or on (1, the default).  Off, an unconverged MIXED job
+ * returns its last refinement iterate. */
+int b200tau_set_mixed_fallback(b200tau_ctx *ctx, int enable);
 
 #ifdef __cplusplus
 }

@@ -532,7 +532,9 @@ cudaError_t sweep_solve(const JobDev *jobs, int njobs, int b, int mode, int *inf
   return cudaSuccess;
 }
 
-// After a refinement round: c = max|correction| / max|tau00| on the tau00 block.  The error left
+// After a refinement round: c = max|correction| / max|tau00| on the tau00 block.  A job whose
+// correction stops shrinking (c >= c_prev) is marked kDiverged and skipped from then on; the
+// host re-solves such jobs, and those not converged after the last round, by FP64 block LU.  The error left
 // after applying the correction is about c times the contraction factor of the refinement,
 // estimated as c / c_prev from the previous round; the job is converged when c * min(1, c / c_prev)
 // is below tol, and later rounds skip it.
@@ -562,7 +564,8 @@ __global__ void __launch_bounds__(256) converge_check_kernel(const JobDev *__res
     const double c = sx[0] > 0.0 ? sy[0] / sx[0] : 0.0;
     const double prev = J.cnorm ? *J.cnorm : 0.0;
     const double est = prev > 0.0 ? c * fmin(1.0, c / prev) : c;
-    if (est <= tol) *J.conv = 1;
+    if (est <= tol) *J.conv = kConverged;
+    else if (prev > 0.0 && c >= prev) *J.conv = kDiverged;  // no contraction: stop refining
     if (J.cnorm) *J.cnorm = c;
   }
 }

@@ -85,6 +85,10 @@ struct b200tau_ctx {
   size_t adj_cap = 0;
   unsigned char *d_tdiag = nullptr;  // per (store, energy, spin) t block: exactly diagonal
   long launches = 0;
+  long fallbacks = 0;  // mixed-precision jobs re-solved in FP64 by the last solve call
+  bool fallback_on = true;
+  double2 *d_ffb = nullptr;  // FP64 factor storage of those re-solves (kFallbackChunk jobs)
+  size_t ffb_elems = 0;
   int max_slots = 64;
   // refinement rounds, FP64 and MIXED; MIXED stops early per job once the correction estimate
   // is below kRefineTol of tau00 (block_lu.cu, converge_check_kernel)
@@ -392,6 +396,8 @@ double trailing_flops(const std::vector<JobDev> &h) {
 // Refinement rounds run on every job of the wave until this many are done; then the host reads the
 // converged flags once and the remaining rounds run on the unconverged jobs only.
 constexpr int kCompactAfterRounds = 2;
+// FP64 re-solves of unconverged mixed jobs run this many jobs at a time.
+constexpr int kFallbackChunk = 8;
 
 int ensure_jobs2(b200tau_ctx *ctx, int n) {
   if (n <= ctx->jobs2_cap) return B200TAU_OK;
@@ -437,10 +443,55 @@ int run_refinement(b200tau_ctx *ctx, const std::vector<JobDev> &h, int nw, int m
         cur_info = ctx->d_info + ctx->slots;  // the compacted list's own pivot flags
       }
     }
-    CK(launch_refine_round(p.fk, cur, ncur, cmaxn, cmaxN, b, it + 1 < p.steps, cur_info, ctx->stream,
-                           &ctx->launches, fp32_sweep));
+    CK(launch_refine_round(p.fk, cur, ncur, cmaxn, cmaxN, b, true, cur_info, ctx->stream, &ctx->launches,
+                           fp32_sweep));
   }
   CK(launch_refine_end(ctx->d_jobs, nw, ns, kkrsz, ctx->stream, &ctx->launches));
+  if (p.fk != kFactorFP32 || !ctx->fallback_on) return B200TAU_OK;
+  // Jobs whose FP32-factor refinement did not converge (condition numbers beyond what FP32 block
+  // factors can refine, e.g. energies next to the real axis) take the FP64 path instead: an FP64
+  // copy of the unmodified M, FP64 block elimination, the FP64 refinement rounds, tau00 from X -
+  // the same kernels and arithmetic as a PREC_FP64 solve of the job.
+  std::vector<int> conv(nw);
+  CK(cudaMemcpyAsync(conv.data(), ctx->d_conv, sizeof(int) * nw, cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  std::vector<JobDev> fb;
+  for (int w = 0; w < nw; ++w)
+    if (conv[w] != kConverged) fb.push_back(h[w]);
+  if (fb.empty()) return B200TAU_OK;
+  int rc = ensure_jobs2(ctx, ctx->slots);
+  if (rc) return rc;
+  const int ld = fb[0].ld;
+  const size_t f64 = (size_t)ld * ld;
+  const int chunk = std::min((int)fb.size(), kFallbackChunk);
+  if (!ctx->d_ffb || f64 * chunk > ctx->ffb_elems) {
+    CK(cudaStreamSynchronize(ctx->stream));
+    cudaFree(ctx->d_ffb);
+    ctx->d_ffb = nullptr;
+    ctx->ffb_elems = std::max(f64 * chunk, ctx->ffb_elems);
+    CK(cudaMalloc(&ctx->d_ffb, sizeof(double2) * ctx->ffb_elems));
+  }
+  for (size_t c0 = 0; c0 < fb.size(); c0 += chunk) {
+    const int nc = (int)std::min(fb.size() - c0, (size_t)chunk);
+    int cmaxn2 = 0, cmaxN2 = 0;
+    for (int i = 0; i < nc; ++i) {
+      JobDev &J = fb[c0 + i];
+      J.F = ctx->d_ffb + (size_t)i * f64;
+      J.conv = nullptr;  // the FP64 rounds run unconditionally
+      J.cnorm = nullptr;
+      CK(launch_copy_to_factor(kFactorFP64, J.M, J.F, J.N, J.ld, ctx->stream));
+      cmaxn2 = std::max(cmaxn2, J.n);
+      cmaxN2 = std::max(cmaxN2, J.N);
+    }
+    // (the host copy of this chunk stays valid: the pageable upload is staged before returning)
+    CK(cudaMemcpyAsync(ctx->d_jobs2, fb.data() + c0, sizeof(JobDev) * nc, cudaMemcpyHostToDevice, ctx->stream));
+    int *finfo = ctx->d_info + ctx->slots;
+    CK(launch_eliminate(kFactorFP64, ctx->d_jobs2, nc, cmaxn2, cmaxN2, finfo, ctx->stream, &ctx->launches,
+                        nullptr, nullptr, ctx->d_err));
+    CK(launch_solve_refine(kFactorFP64, ctx->d_jobs2, nc, cmaxn2, cmaxN2, b, std::max(1, ctx->refine_steps[0]),
+                           ns, kkrsz, finfo, ctx->stream, &ctx->launches));
+  }
+  ctx->fallbacks += (long)fb.size();
   return B200TAU_OK;
 }
 
@@ -591,6 +642,7 @@ int solve_impl(b200tau_ctx *ctx, const b200tau_job *jobs, int njobs, int prec, d
   if ((rc = ensure_workspace(ctx, ld, slots, p))) return rc;
   if ((rc = ensure_jobs(ctx, slots))) return rc;
   ctx->launches = 0;
+  ctx->fallbacks = 0;
   std::vector<int> info(slots);
   for (int w0 = 0; w0 < njobs; w0 += slots) {
     const int nw = std::min(slots, njobs - w0);
@@ -678,6 +730,7 @@ void b200tau_destroy(b200tau_ctx *ctx) {
   cudaFree(ctx->d_pack);
   cudaFree(ctx->d_V);
   cudaFree(ctx->d_adj);
+  cudaFree(ctx->d_ffb);
   for (auto &e : ctx->events) cudaEventDestroy(e);
   for (auto &e : ctx->pev) cudaEventDestroy(e);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -689,6 +742,8 @@ const char *b200tau_last_error(const b200tau_ctx *ctx) { return ctx ? ctx->err.c
 void *b200tau_stream(b200tau_ctx *ctx) { return ctx ? (void *)ctx->stream : nullptr; }
 
 long b200tau_last_launch_count(const b200tau_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+long b200tau_last_fallback_count(const b200tau_ctx *ctx) { return ctx ? ctx->fallbacks : 0; }
 
 int b200tau_gaunt_numbers(int lmax, double *cgnt) {
   if (lmax < 0 || lmax > kMaxLmax || !cgnt) return B200TAU_ERR_ARG;
@@ -743,6 +798,12 @@ int b200tau_set_mixed_engine(b200tau_ctx *ctx, int engine) {
   if (engine != B200TAU_ENGINE_TENSOR && engine != B200TAU_ENGINE_SIMT)
     return fail(ctx, B200TAU_ERR_ARG, "unknown engine %d", engine);
   ctx->mixed_engine = engine;
+  return B200TAU_OK;
+}
+
+int b200tau_set_mixed_fallback(b200tau_ctx *ctx, int enable) {
+  if (!ctx) return B200TAU_ERR_ARG;
+  ctx->fallback_on = enable != 0;
   return B200TAU_OK;
 }
 

@@ -20,6 +20,9 @@ constexpr int kNb = 64;                                         // elimination b
 // A refining job stops once its estimated remaining error on tau00 is below this fraction of
 // max|tau00|: 100x below the mixed path's 1e-10 accuracy target.
 constexpr double kRefineTol = 1e-12;
+// JobDev::conv values (0: still refining)
+constexpr int kConverged = 1;
+constexpr int kDiverged = 2;
 
 // Angular-momentum tables for G_ij (makegij_c.f:79-128, buildKKRMatrix_CPU.cpp:144-176),
 // laid out as a gather list: G(lm2, lm1) = pi4 * i^rot * sum_q coef[q] * D[didx[q]]

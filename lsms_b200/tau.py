@@ -49,6 +49,7 @@ EXPORTS = (
     "b200tau_gaunt_numbers", "b200tau_set_refinement", "b200tau_set_profiling",
     "b200tau_profile_read", "b200tau_set_mixed_engine", "b200tau_solve_dense_noalloc",
     "b200tau_profile_phases", "b200tau_set_mixed_sweep", "b200tau_solve_vjp",
+    "b200tau_last_fallback_count", "b200tau_set_mixed_fallback",
 )
 
 
@@ -101,6 +102,9 @@ def load_library():
     lib.b200tau_profile_phases.argtypes = [P, P]
     lib.b200tau_set_mixed_sweep.argtypes = [P, I]
     lib.b200tau_solve_vjp.argtypes = [P, P, I, P, P, P, P]
+    lib.b200tau_last_fallback_count.argtypes = [P]
+    lib.b200tau_last_fallback_count.restype = L
+    lib.b200tau_set_mixed_fallback.argtypes = [P, I]
     _lib = lib
     return lib
 
@@ -170,6 +174,11 @@ class TauSolver:
     def last_launch_count(self) -> int:
         return int(self.lib.b200tau_last_launch_count(self.ctx))
 
+    @property
+    def last_fallback_count(self) -> int:
+        """Mixed-precision jobs of the last solve re-solved by FP64 block LU."""
+        return int(self.lib.b200tau_last_fallback_count(self.ctx))
+
     def set_refinement(self, prec: int, steps: int):
         """FP64 refinement steps of a precision (see b200tau_set_refinement)."""
         self._check(self.lib.b200tau_set_refinement(self.ctx, prec, steps))
@@ -177,6 +186,10 @@ class TauSolver:
     def set_mixed_engine(self, engine: int):
         """Trailing-update engine of the mixed path: ENGINE_TENSOR (tcgen05) or ENGINE_SIMT."""
         self._check(self.lib.b200tau_set_mixed_engine(self.ctx, engine))
+
+    def set_mixed_fallback(self, enable: bool):
+        """Re-solve unconverged mixed-precision jobs by FP64 block LU (default on)."""
+        self._check(self.lib.b200tau_set_mixed_fallback(self.ctx, int(bool(enable))))
 
     def set_mixed_sweep(self, sweep: int):
         """Arithmetic of the mixed path's correction solve: SWEEP_FP32 (default) or SWEEP_FP64."""

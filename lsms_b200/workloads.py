@@ -225,3 +225,127 @@ def config_noncollinear(seed: int = 4, npts: int = 16, nshells: int = 7) -> Prob
     """fcc LIZ, kkrsz_ns = 32 (non-collinear), N = 32 * L."""
     return make_problem("fcc", 6.82, nshells, 3, semicircle_contour(-0.3, 0.7, npts), seed,
                         n_species=None, n_spin_cant=2, n_spin_pola=2)
+
+
+@dataclasses.dataclass
+class AtomLIZ:
+    """One local atom: AtomData's LIZPos (3, L), LIZlmax, LIZStoreIdx and spin frame."""
+    liz_pos: np.ndarray
+    liz_lmax: np.ndarray
+    liz_store_idx: np.ndarray
+    ubr: np.ndarray
+    ubrd: np.ndarray
+
+    @property
+    def num_liz(self) -> int:
+        return int(self.liz_pos.shape[1])
+
+
+@dataclasses.dataclass
+class Batch:
+    """Many local atoms sharing one tmatStore and one energy group (calculateAllTauMatrices)."""
+    lmax: int
+    n_spin_cant: int
+    n_spin_pola: int
+    tmat_store: np.ndarray       # (nstore, group_size, blk) complex128
+    energies: np.ndarray
+    atoms: list
+
+    @property
+    def kkrsz_ns(self) -> int:
+        return self.n_spin_cant * (self.lmax + 1) ** 2
+
+    def nrmat_ns(self, a: int) -> int:
+        return self.n_spin_cant * int(((self.atoms[a].liz_lmax + 1) ** 2).sum())
+
+    def problem(self, a: int) -> "Problem":
+        """Atom a as a single-atom Problem (for the oracle)."""
+        at = self.atoms[a]
+        return Problem(lmax=self.lmax, n_spin_cant=self.n_spin_cant, n_spin_pola=self.n_spin_pola,
+                       liz_pos=at.liz_pos, liz_lmax=at.liz_lmax, liz_store_idx=at.liz_store_idx,
+                       tmat_store=self.tmat_store, energies=self.energies, ubr=at.ubr, ubrd=at.ubrd)
+
+
+def _phase_shift_store(rng, nstore: int, energies, lmax: int, n_spin_cant: int,
+                       delta_range=(0.0, 1.2)) -> tuple[np.ndarray, np.ndarray]:
+    """tmatStore of phase-shift t-matrices (non-collinear: a random moment per store column,
+    t = U^+ diag(t_up, t_dn) U per L element).  Returns (store, moment directions)."""
+    kkrsz = (lmax + 1) ** 2
+    b = n_spin_cant * kkrsz
+    blk = (2 * kkrsz) ** 2
+    deltas = rng.uniform(delta_range[0], delta_range[1], size=(nstore, 2, lmax + 1))
+    evecs = rng.normal(size=(nstore, 3))
+    evecs /= np.linalg.norm(evecs, axis=1, keepdims=True)
+    store = np.zeros((nstore, len(energies), blk), np.complex128)
+    for s in range(nstore):
+        for ie, e in enumerate(energies):
+            p = prel_of(e)
+            if n_spin_cant == 2:
+                tu, td = t_diagonal(deltas[s, 0], lmax, p), t_diagonal(deltas[s, 1], lmax, p)
+                u, ud = spin_trafo(evecs[s])
+                U, Ud = u.reshape(2, 2, order="F"), ud.reshape(2, 2, order="F")
+                tg = np.zeros((b, b), np.complex128)
+                loc = [[tu, 0 * tu], [0 * tu, td]]
+                for is_ in range(2):
+                    for js in range(2):
+                        acc = sum(Ud[is_, p_] * loc[p_][q] * U[q, js] for p_ in range(2) for q in range(2))
+                        tg[is_ * kkrsz:(is_ + 1) * kkrsz, js * kkrsz:(js + 1) * kkrsz] = acc
+                store[s, ie, :b * b] = tg.T.reshape(-1)
+            else:
+                store[s, ie, :b * b] = t_diagonal(deltas[s, 0], lmax, p).T.reshape(-1)
+    return store, evecs
+
+
+def config_batched(seed: int = 3, n_atoms: int = 256) -> Batch:
+    """Random fcc alloy (a = 6.82 bohr, two species 50/50) with 5% vacancies: every local atom's
+    LIZ size is drawn from {43, 55, 79, 87, 135} (3..7 shells, N = 688..2160), lmax 3, 31-point
+    contour plus etop + i eibot (32 energies).  Store columns: 0, 1 species, 2 vacancy (small
+    phase shifts)."""
+    rng = np.random.default_rng(seed)
+    energies = semicircle_contour(-0.3, 0.7, 31, extra_point=True)
+    store, _ = _phase_shift_store(rng, 3, energies, 3, 1)
+    vac, _ = _phase_shift_store(rng, 1, energies, 3, 1, delta_range=(0.0, 0.05))
+    store[2] = vac[0]
+    shells = {3: 43, 4: 55, 5: 79, 6: 87, 7: 135}
+    geo = {sh: lattice_shells("fcc", 6.82, sh) for sh in shells}
+    atoms = []
+    u0, ud0 = spin_trafo((0.0, 0.0, 1.0))
+    for _ in range(n_atoms):
+        sh = int(rng.choice(list(shells)))
+        pos = geo[sh]
+        L = pos.shape[1]
+        st = rng.choice(3, size=L, p=[0.475, 0.475, 0.05]).astype(np.int32)
+        st[0] = rng.integers(0, 2)
+        atoms.append(AtomLIZ(pos, np.full(L, 3, np.int32), st, u0, ud0))
+    return Batch(3, 1, 1, store, energies, atoms)
+
+
+def config_noncollinear_batch(seed: int = 4, n_atoms: int = 64, npts: int = 16) -> Batch:
+    """Non-collinear (kkrsz_ns = 32), fcc LIZ of 135 sites (N = 4320), 64 atoms x 16 contour
+    energies.  135 store columns with spin-dependent phase shifts and a random moment each;
+    atom a sees column (site + 7 a) mod 135 at each LIZ site."""
+    rng = np.random.default_rng(seed)
+    energies = semicircle_contour(-0.3, 0.7, npts)
+    pos = lattice_shells("fcc", 6.82, 7)
+    L = pos.shape[1]
+    store, evecs = _phase_shift_store(rng, L, energies, 3, 2)
+    atoms = []
+    for a in range(n_atoms):
+        st = ((np.arange(L) + 7 * a) % L).astype(np.int32)
+        u, ud = spin_trafo(evecs[st[0]])
+        atoms.append(AtomLIZ(pos, np.full(L, 3, np.int32), st, u, ud))
+    return Batch(3, 2, 2, store, energies, atoms)
+
+
+def config_adjoint_batch(seed: int = 5, n_atoms: int = 64, npts: int = 16) -> Batch:
+    """fcc LIZ of 87 sites (N = 1392), lmax 3, 64 atoms x 16 contour energies; every LIZ site
+    of every atom has its own store column (phase shifts drawn per column)."""
+    rng = np.random.default_rng(seed)
+    energies = semicircle_contour(-0.3, 0.7, npts)
+    pos = lattice_shells("fcc", 6.82, 6)
+    L = pos.shape[1]
+    store, _ = _phase_shift_store(rng, L * n_atoms, energies, 3, 1)
+    u0, ud0 = spin_trafo((0.0, 0.0, 1.0))
+    atoms = [AtomLIZ(pos, np.full(L, 3, np.int32), np.arange(a * L, (a + 1) * L, dtype=np.int32), u0, ud0)
+             for a in range(n_atoms)]
+    return Batch(3, 1, 1, store, energies, atoms)

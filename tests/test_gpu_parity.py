@@ -79,6 +79,7 @@ def test_tau00_mixed_matches_golden(solver_factory, name):
     g = np.load(os.path.join(GOLDEN, f"{name}.npz"))
     specs = [(0, iie, ispin, prob.energies[iie]) for iie, ispin in runs]
     out = s.solve_jobs(T.make_jobs(specs), T.PREC_MIXED)
+    assert s.last_fallback_count == 0, name  # the refinement itself converged
     for k, (iie, ispin) in enumerate(runs):
         err = tau_err(prob, iie, ispin, out[k], g[f"tau_blocklu_{iie}_{ispin}"])
         assert err <= TOL_MIXED, (name, iie, ispin, err)
@@ -121,6 +122,7 @@ def test_n2160_full_contour_mixed_vs_fp64(solver_factory, sweep):
         jobs = T.make_jobs([(0, i, 0, prob.energies[i]) for i in range(len(prob.energies))])
         fp64 = s.solve_jobs(jobs, T.PREC_FP64)
         mixed = s.solve_jobs(jobs, T.PREC_MIXED)
+        assert s.last_fallback_count == 0
     finally:
         s.set_mixed_sweep(T.SWEEP_FP32)
     errs = [tau_err(prob, i, 0, mixed[i], fp64[i]) for i in range(len(prob.energies))]
@@ -210,6 +212,7 @@ def test_mixed_engines_match_reference(solver_factory, ref, engine, sweep):
     s.set_mixed_sweep(sweep)
     try:
         out = s.solve_jobs(T.make_jobs([(0, i, 0, prob.energies[i]) for i in range(2)]), T.PREC_MIXED)
+        assert s.last_fallback_count == 0
     finally:
         s.set_mixed_engine(T.ENGINE_TENSOR)
         s.set_mixed_sweep(T.SWEEP_FP32)
@@ -245,3 +248,77 @@ def test_solver_parity_on_the_reference_matrix(solver_factory, ref):
     s = solver_factory(3, 1, 1)
     assert relerr(s.solve_tau00_dense(m, t0), want) <= TOL_FP64
     assert relerr(s.solve_tau00_dense(m, t0, T.PREC_MIXED), want) <= TOL_MIXED
+
+
+def test_batched_alloy_with_vacancies_matches_reference(solver_factory, ref):
+    """The batched configuration's inputs (random fcc alloy, 5% vacancies, LIZ sizes 43..135):
+    a sample of atoms and energies solved in one call, each against the reference."""
+    wl = W.config_batched(n_atoms=12)
+    s = solver_factory(3, 1, 1)
+    s.upload_tmat(wl.tmat_store)
+    for a, at in enumerate(wl.atoms):
+        s.set_atom(a, at.liz_pos, at.liz_lmax, at.liz_store_idx, at.ubr, at.ubrd)
+    picks = [(a, iie) for a, iie in zip(range(12), [0, 5, 9, 14, 20, 31, 3, 7, 11, 17, 25, 30])]
+    specs = [(a, iie, 0, wl.energies[iie]) for a, iie in picks]
+    fp64 = s.solve_jobs(T.make_jobs(specs), T.PREC_FP64)
+    mixed = s.solve_jobs(T.make_jobs(specs), T.PREC_MIXED)
+    assert len({wl.atoms[a].num_liz for a, _ in picks}) >= 3
+    for k, (a, iie) in enumerate(picks):
+        prob = wl.problem(a)
+        want = ref.calculate_tau(prob, iie, 0, ref.ZBLOCKLU_CPP)
+        assert tau_err(prob, iie, 0, fp64[k], want) <= TOL_FP64, (a, iie)
+        assert tau_err(prob, iie, 0, mixed[k], want) <= TOL_MIXED, (a, iie)
+
+
+def cond1(m: np.ndarray) -> float:
+    """1-norm condition number."""
+    return float(np.abs(m).sum(0).max() * np.abs(np.linalg.inv(m)).sum(0).max())
+
+
+def test_noncollinear_n4320_matches_reference(solver_factory, ref):
+    """Non-collinear kkrsz_ns = 32 over the 135-site fcc LIZ (N = 4320), spin-dependent phase
+    shifts with a random moment per site, two energies:
+    * FP64 agreement within 1e-12 or kappa_1(M) x 1e-16, whichever is larger, both for the
+      solver alone on the reference's own M and for the full path (device-built M): these
+      matrices have kappa_1 ~ 1e5..1e7, and two FP64 block-LU solves that differ only in their
+      blocking or in the rounding of sin/cos/exp in the build differ by about kappa x eps;
+    * the mixed path stays within 1e-10 of the FP64 path (refinement, or the FP64 re-solve of
+      jobs it cannot refine)."""
+    wl = W.config_noncollinear_batch(n_atoms=2)
+    s = solver_factory(3, 2, 2)
+    s.upload_tmat(wl.tmat_store)
+    for a, at in enumerate(wl.atoms):
+        s.set_atom(a, at.liz_pos, at.liz_lmax, at.liz_store_idx, at.ubr, at.ubrd)
+    picks = [(0, 2), (1, 9)]
+    specs = [(a, iie, 0, wl.energies[iie]) for a, iie in picks]
+    fp64 = s.solve_jobs(T.make_jobs(specs), T.PREC_FP64)
+    mixed = s.solve_jobs(T.make_jobs(specs), T.PREC_MIXED)
+    for k, (a, iie) in enumerate(picks):
+        prob = wl.problem(a)
+        assert prob.nrmat_ns == 4320
+        m = ref.build_kkr(prob, iie)
+        t0 = prob.t_block(int(prob.liz_store_idx[0]), iie)
+        want_raw = ref.calculate_tau(prob, iie, 0, ref.ZBLOCKLU_CPP)
+        dense = s.solve_tau00_dense(m, t0)
+        raw_ref = port_tau00_raw(prob, iie, want_raw)
+        tol = max(TOL_FP64, cond1(m) * 1e-16)
+        assert relerr(dense, raw_ref) <= tol, (a, iie, relerr(dense, raw_ref), tol)
+        assert tau_err(prob, iie, 0, fp64[k], want_raw) <= tol, (a, iie, tau_err(prob, iie, 0, fp64[k], want_raw), tol)
+        assert tau_err(prob, iie, 0, mixed[k], fp64[k]) <= TOL_MIXED, (a, iie, tau_err(prob, iie, 0, mixed[k], fp64[k]))
+
+
+def port_tau00_raw(prob, iie, tau00_l):
+    """The reference's raw tau00 (global frame, not minus t0) from its returned tau00_l, by
+    undoing the trgtol rotation (u is unitary: mg = ud ml u, blockwise) and adding t0."""
+    b = prob.kkrsz_ns
+    kk = b // 2
+    ml = tau00_l.reshape(4, kk, kk).transpose(0, 2, 1)  # block k, [row, col]
+    U = prob.ubr.reshape(2, 2, order="F")
+    Ud = prob.ubrd.reshape(2, 2, order="F")
+    big_l = np.zeros((b, b), np.complex128)
+    for k, (p, q) in enumerate([(0, 0), (1, 0), (0, 1), (1, 1)]):
+        big_l[p * kk:(p + 1) * kk, q * kk:(q + 1) * kk] = ml[k]
+    Ub = np.kron(U, np.eye(kk))
+    Udb = np.kron(Ud, np.eye(kk))
+    mg = Udb @ big_l @ Ub
+    return mg + prob.t_block(int(prob.liz_store_idx[0]), iie)
