@@ -24,6 +24,8 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "common.cuh"
 #include "cplx.cuh"
 #include "gj.cuh"
@@ -57,7 +59,7 @@ __global__ void __launch_bounds__(kDiagThreads) diag_inverse_kernel(const JobDev
                                                                     int *info) {
   constexpr int NB = kNb;
   const JobDev &J = jobs[blockIdx.x];
-  if (k >= J.n) return;
+  if (k >= J.n || J.inactive) return;
   const int kb = min(NB, J.n - k);
   extern __shared__ __align__(16) double2 dyn_smem[];
   double2(*As)[NB + 1] = reinterpret_cast<double2(*)[NB + 1]>(dyn_smem);  // staging As[row][col]
@@ -180,28 +182,25 @@ constexpr int kKc = 16;
 enum { kOverwrite = 0, kSubtract = 1 };
 
 template <typename S, int MODE>
-// Two resident CTAs per SM: with K = 64 per step each CTA runs only four K-chunks, so its operand
-// prologue and C read-modify-write latencies are hidden by the other CTA's FMAs.
-__global__ void __launch_bounds__(256, 2) zgemm_tile_kernel(const JobDev *__restrict__ jobs, int k) {
+__device__ __forceinline__ void zgemm_tile_body(const JobDev &J, int k, int bx, int by) {
   using T = typename Vec2<S>::t;
-  const JobDev &J = jobs[blockIdx.z];
   const int N = J.N, ld = J.ld;
-  if (k >= J.n) return;
+  if (k >= J.n || J.inactive) return;
   const int kb = min(kNb, J.n - k);
   const int K = kb;
   T *__restrict__ F = static_cast<T *>(J.F);
   int row0, m;
   const T *Ab;
-  const int col0 = k + kb + blockIdx.x * kTile;
+  const int col0 = k + kb + bx * kTile;
   int n = N - col0;
   if (n <= 0) return;
   if (MODE == kOverwrite) {
-    if (blockIdx.y != 0) return;
+    if (by != 0) return;
     row0 = k;
     m = kb;
     Ab = F + (size_t)k + (size_t)k * ld;  // D (kb x kb)
   } else {
-    row0 = k + kb + blockIdx.y * kTile;
+    row0 = k + kb + by * kTile;
     m = N - row0;
     if (m <= 0) return;
     Ab = F + (size_t)row0 + (size_t)k * ld;  // A21
@@ -293,6 +292,22 @@ __global__ void __launch_bounds__(256, 2) zgemm_tile_kernel(const JobDev *__rest
   }
 }
 
+// One output tile per (bx, by, job).  Launched either with that 3-D grid, or with a smaller 1-D
+// grid whose CTAs loop over the tiles (the FP64 re-solve of a mixed wave, where most jobs are
+// inactive and a full grid would spend its time launching CTAs that exit at once).
+// Two resident CTAs per SM: with K = 64 per step each CTA runs only four K-chunks, so its operand
+// prologue and C read-modify-write latencies are hidden by the other CTA's FMAs.
+template <typename S, int MODE>
+__global__ void __launch_bounds__(256, 2) zgemm_tile_kernel(const JobDev *__restrict__ jobs, int k, int tx, int ty,
+                                                            int nj) {
+  const int total = tx * ty * nj;
+  const int nblk = gridDim.x * gridDim.y * gridDim.z;
+  for (int vb = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z); vb < total; vb += nblk) {
+    const int bx = vb % tx, by = (vb / tx) % ty, bz = vb / (tx * ty);
+    zgemm_tile_body<S, MODE>(jobs[bz], k, bx, by);
+  }
+}
+
 
 // out = tau00 (out_mode 1) or rotate(tau00 - t0) (out_mode 0), tau00 in A[r][b + c].
 __device__ void write_out(const JobDev &J, double2 (*A)[2 * kMaxB + 1], int ns, int kkrsz) {
@@ -361,6 +376,7 @@ __global__ void __launch_bounds__(256) finalize_direct_kernel(const JobDev *__re
 __global__ void __launch_bounds__(256) finalize_from_x_kernel(const JobDev *__restrict__ jobs, int ns,
                                                               int kkrsz) {
   const JobDev &J = jobs[blockIdx.x];
+  if (J.inactive) return;
   const int b = J.b;
   __shared__ double2 A[kMaxB][2 * kMaxB + 1];
   for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
@@ -384,68 +400,88 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
 
 // R = B - M X with B = [0; t0] (rows n..N-1 hold t0), FP64.  The product is FP64-FMA bound
 // (b complex multiply-adds per 16-byte element of M), so each thread keeps one row x 16 columns of
-// accumulators and every M element it loads feeds 16 complex FMAs: M streams through registers
-// (a batch of RB columns in flight ahead of use), X through a two-stage cp.async ring in shared
-// memory, read as broadcasts.  BC = 16 or 32 is the padded column count (b <= BC).
+// accumulators and every M element it loads feeds 16 complex FMAs.  M and X stream through a
+// three-stage cp.async ring in shared memory (kResK columns of M and rows of X per stage), so two
+// stages of loads are in flight while one is multiplied; X is read as broadcasts.
+// BC = 16 or 32 is the padded column count (b <= BC).
+constexpr int kResK = 8;       // K per stage
+constexpr int kResStages = 3;
+
+template <int BC>
+__host__ __device__ constexpr int residual_rows() {
+  return 256 * 16 / BC;
+}
+template <int BC>
+__host__ __device__ constexpr int residual_smem_bytes() {
+  return kResStages * kResK * (residual_rows<BC>() + BC) * (int)sizeof(double2);
+}
+
 template <int BC>
 __global__ void __launch_bounds__(256, 2) residual_kernel(const JobDev *__restrict__ jobs) {
-  constexpr int NC = 16;            // columns per thread
-  constexpr int ROWS = 256 * NC / BC;  // rows per CTA
-  constexpr int KC = 32;            // X rows per stage
-  constexpr int RB = 4;             // M columns per register batch
+  constexpr int NC = 16;                  // columns per thread
+  constexpr int ROWS = residual_rows<BC>();  // rows per CTA
   const JobDev &J = jobs[blockIdx.y];
-  if (converged(J)) return;
+  if (converged(J) || J.inactive) return;
   const int N = J.N, ld = J.ld, b = J.b;
   const int row0 = blockIdx.x * ROWS;
   if (row0 >= N) return;
-  __shared__ __align__(16) double2 Xs[2][KC][BC];
+  extern __shared__ __align__(16) unsigned char rsm[];
+  double2(*Ms)[kResK][ROWS] = reinterpret_cast<double2(*)[kResK][ROWS]>(rsm);
+  double2(*Xs)[kResK][BC] =
+      reinterpret_cast<double2(*)[kResK][BC]>(rsm + sizeof(double2) * kResStages * kResK * ROWS);
   const int tid = threadIdx.x;
   const int r = tid % ROWS, cg = tid / ROWS;
   const int gr = row0 + r;
-  const double2 *__restrict__ Mrow = J.M + min(gr, N - 1);
+  const double2 *__restrict__ M = J.M;
   const double2 *__restrict__ X = J.X;
-  // X rows [kc, kc + KC) into stage st; columns >= b and rows >= N read as zero
-  auto stage_x = [&](int kc, int st) {
-    for (int e = tid; e < KC * BC; e += 256) {
-      const int kk = e % KC, c = e / KC;
-      if (c < b && kc + kk < N) cp_async16(&Xs[st][kk][c], X + (size_t)(kc + kk) + (size_t)c * ld);
-      else Xs[st][kk][c] = make_double2(0.0, 0.0);
+  const double2 zero = make_double2(0.0, 0.0);
+  // columns [k0, k0 + kResK) of M (rows of the CTA) and rows [k0, k0 + kResK) of X into stage st;
+  // entries past N or b read as zero
+  auto stage = [&](int k0, int st) {
+    for (int e = tid; e < kResK * ROWS; e += 256) {
+      const int kk = e / ROWS, rr = e - kk * ROWS;
+      const int gk = k0 + kk, grr = row0 + rr;
+      if (gk < N && grr < N) cp_async16(&Ms[st][kk][rr], M + (size_t)grr + (size_t)gk * ld);
+      else Ms[st][kk][rr] = zero;
+    }
+    for (int e = tid; e < kResK * BC; e += 256) {
+      const int kk = e % kResK, c = e / kResK;
+      const int gk = k0 + kk;
+      if (c < b && gk < N) cp_async16(&Xs[st][kk][c], X + (size_t)gk + (size_t)c * ld);
+      else Xs[st][kk][c] = zero;
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
   };
-  auto load_m = [&](double2 (&m)[RB], int k0) {
-#pragma unroll
-    for (int i = 0; i < RB; ++i) m[i] = (k0 + i < N) ? Mrow[(size_t)(k0 + i) * ld] : make_double2(0.0, 0.0);
-  };
   double2 acc[NC];
 #pragma unroll
-  for (int j = 0; j < NC; ++j) acc[j] = make_double2(0.0, 0.0);
-  double2 mc[RB], mn[RB];
-  stage_x(0, 0);
-  load_m(mc, 0);
-  for (int k0 = 0; k0 < N; k0 += RB) {
-    const int st = (k0 / KC) & 1;
-    if (k0 % KC == 0) {
-      asm volatile("cp.async.wait_group 0;" ::: "memory");
-      __syncthreads();  // stage st complete for all threads; the other stage is no longer read
-      if (k0 + KC < N) stage_x(k0 + KC, st ^ 1);
-    }
-    if (k0 + RB < N) load_m(mn, k0 + RB);
-    const int kr = k0 % KC;
+  for (int j = 0; j < NC; ++j) acc[j] = zero;
+  const int nst = (N + kResK - 1) / kResK;
 #pragma unroll
-    for (int i = 0; i < RB; ++i) {
-#pragma unroll
-      for (int j = 0; j < NC; ++j) acc[j] = cfma(mc[i], Xs[st][kr + i][cg * NC + j], acc[j]);
-    }
-#pragma unroll
-    for (int i = 0; i < RB; ++i) mc[i] = mn[i];
+  for (int q = 0; q < kResStages - 1; ++q) {
+    if (q < nst) stage(q * kResK, q);
+    else asm volatile("cp.async.commit_group;" ::: "memory");
   }
+  for (int q = 0; q < nst; ++q) {
+    asm volatile("cp.async.wait_group %0;" ::"n"(kResStages - 2) : "memory");
+    __syncthreads();  // stage q landed for every thread; stage q - 1 is no longer read
+    const int nq = q + kResStages - 1;
+    if (nq < nst) stage(nq * kResK, nq % kResStages);
+    else asm volatile("cp.async.commit_group;" ::: "memory");
+    const int st = q % kResStages;
+#pragma unroll
+    for (int kk = 0; kk < kResK; ++kk) {
+      const double2 a = Ms[st][kk][r];
+#pragma unroll
+      for (int j = 0; j < NC; ++j) acc[j] = cfma(a, Xs[st][kk][cg * NC + j], acc[j]);
+    }
+  }
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
   if (gr >= N) return;
 #pragma unroll
   for (int j = 0; j < NC; ++j) {
     const int c = cg * NC + j;
     if (c >= b) continue;
-    const double2 bv = (gr >= J.n) ? J.t0[(gr - J.n) + (size_t)c * J.t0_ld] : make_double2(0.0, 0.0);
+    const double2 bv = (gr >= J.n) ? J.t0[(gr - J.n) + (size_t)c * J.t0_ld] : zero;
     J.R[(size_t)gr + (size_t)c * ld] = csub(bv, acc[j]);
   }
 }
@@ -455,7 +491,7 @@ template <typename T>
 __global__ void __launch_bounds__(256) schur_solve_kernel(const JobDev *__restrict__ jobs, int mode,
                                                           int *info) {
   const JobDev &J = jobs[blockIdx.x];
-  if (mode == 1 && converged(J)) return;
+  if ((mode == 1 && converged(J)) || J.inactive) return;
   const int b = J.b, n = J.n, ld = J.ld;
   __shared__ double2 A[kMaxB][2 * kMaxB + 1];
   __shared__ int s_piv;
@@ -479,9 +515,12 @@ __global__ void __launch_bounds__(256) schur_solve_kernel(const JobDev *__restri
   }
 }
 
+// CTAs of the looping trailing-update grid (two per SM)
+constexpr int kSparseGrid = 2 * 148;
+
 template <typename T, typename S>
 cudaError_t eliminate_impl(const JobDev *jobs, int njobs, int max_n, int max_N, int *info, cudaStream_t s,
-                           long *launches, KernelTimer *timer, const TcMaps *tc, int *err) {
+                           long *launches, KernelTimer *timer, const TcMaps *tc, int *err, bool sparse_jobs) {
   const int smem_diag = kNb * (kNb + 1) * (int)sizeof(double2);
   const int smem_gemm = 4 * kKc * kTile * (int)sizeof(T);
   cudaError_t e;
@@ -500,14 +539,19 @@ cudaError_t eliminate_impl(const JobDev *jobs, int njobs, int max_n, int max_N, 
     const int tiles = (rest + kTile - 1) / kTile;
     if (launches) *launches += 1;
     if (tiles > 0) {
-      zgemm_tile_kernel<S, kOverwrite><<<dim3(tiles, 1, njobs), 256, smem_gemm, s>>>(jobs, k);
+      zgemm_tile_kernel<S, kOverwrite><<<dim3(tiles, 1, njobs), 256, smem_gemm, s>>>(jobs, k, tiles, 1, njobs);
       const bool timed = timer && timer->used + 2 <= timer->cap;
       if (timed) cudaEventRecord(timer->ev[timer->used++], s);
       if (tc != nullptr) {
         if ((e = launch_tc_step(*tc, jobs, njobs, k, max_N, err, s)) != cudaSuccess) return e;
         if (launches) *launches += 1;  // pack + update
       } else {
-        zgemm_tile_kernel<S, kSubtract><<<dim3(tiles, tiles, njobs), 256, smem_gemm, s>>>(jobs, k);
+        if (sparse_jobs)
+          zgemm_tile_kernel<S, kSubtract><<<std::min(tiles * tiles * njobs, kSparseGrid), 256, smem_gemm, s>>>(
+              jobs, k, tiles, tiles, njobs);
+        else
+          zgemm_tile_kernel<S, kSubtract><<<dim3(tiles, tiles, njobs), 256, smem_gemm, s>>>(jobs, k, tiles, tiles,
+                                                                                           njobs);
       }
       if (timed) cudaEventRecord(timer->ev[timer->used++], s);
       if (launches) *launches += 2;
@@ -540,7 +584,7 @@ cudaError_t sweep_solve(const JobDev *jobs, int njobs, int b, int mode, int *inf
 // is below tol, and later rounds skip it.
 __global__ void __launch_bounds__(256) converge_check_kernel(const JobDev *__restrict__ jobs, double tol) {
   const JobDev &J = jobs[blockIdx.x];
-  if (J.conv == nullptr || converged(J)) return;
+  if (J.conv == nullptr || converged(J) || J.inactive) return;
   const int b = J.b, n = J.n, ld = J.ld;
   double my = 0.0, mx = 0.0;
   for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
@@ -579,7 +623,44 @@ __global__ void copy_to_factor_kernel(const double2 *__restrict__ M, T *__restri
   }
 }
 
+// The FP64 re-solve records of a mixed wave (launch_fallback_prepare).
+__global__ void fallback_prepare_kernel(const JobDev *__restrict__ jobs, JobDev *__restrict__ out, int njobs,
+                                        double2 *f64, size_t f64_stride, int *count) {
+  const int w = blockIdx.x * blockDim.x + threadIdx.x;
+  if (w >= njobs) return;
+  JobDev J = jobs[w];
+  const bool conv = J.conv != nullptr && *J.conv == kConverged;
+  if (conv) {
+    J.inactive = 1;
+  } else {
+    J.F = f64 + (size_t)w * f64_stride;
+    J.conv = nullptr;  // the FP64 rounds run unconditionally
+    J.cnorm = nullptr;
+    atomicAdd(count, 1);
+  }
+  out[w] = J;
+}
+
+// F = M (FP64, N x N) for the active records; CTAs (blockIdx.x) stride over the columns of job
+// blockIdx.y
+__global__ void __launch_bounds__(256) copy_jobs_to_factor_kernel(const JobDev *__restrict__ jobs) {
+  const JobDev &J = jobs[blockIdx.y];
+  if (J.inactive) return;
+  double2 *F = static_cast<double2 *>(J.F);
+  for (int c = blockIdx.x; c < J.N; c += gridDim.x)
+    for (int r = threadIdx.x; r < J.N; r += 256) F[(size_t)r + (size_t)c * J.ld] = J.M[(size_t)r + (size_t)c * J.ld];
+}
+
 }  // namespace
+
+cudaError_t launch_fallback_prepare(const JobDev *jobs, JobDev *out, int njobs, double2 *f64, size_t f64_stride,
+                                    int max_N, int *count, cudaStream_t s, long *launches) {
+  if (njobs <= 0) return cudaSuccess;
+  fallback_prepare_kernel<<<(njobs + 63) / 64, 64, 0, s>>>(jobs, out, njobs, f64, f64_stride, count);
+  copy_jobs_to_factor_kernel<<<dim3(std::min(max_N, 64), njobs), 256, 0, s>>>(out);
+  if (launches) *launches += 2;
+  return cudaGetLastError();
+}
 
 cudaError_t launch_copy_to_factor(FactorKind fk, const double2 *M, void *F, int n, int ld, cudaStream_t s) {
   const int blocks = 148 * 8;
@@ -592,14 +673,15 @@ cudaError_t launch_copy_to_factor(FactorKind fk, const double2 *M, void *F, int 
 
 cudaError_t launch_eliminate(FactorKind fk, const JobDev *jobs, int njobs, int max_n, int max_N, int *info,
                              cudaStream_t s, long *launches, KernelTimer *timer, const TcMaps *tc,
-                             int *err) {
+                             int *err, bool sparse_jobs) {
   if (fk == kFactorFP64)
-    return eliminate_impl<double2, double>(jobs, njobs, max_n, max_N, info, s, launches, timer, nullptr, err);
+    return eliminate_impl<double2, double>(jobs, njobs, max_n, max_N, info, s, launches, timer, nullptr, err,
+                                           sparse_jobs);
   if (tc) {
     cudaError_t e = tc_prepare();
     if (e != cudaSuccess) return e;
   }
-  return eliminate_impl<float2, float>(jobs, njobs, max_n, max_N, info, s, launches, timer, tc, err);
+  return eliminate_impl<float2, float>(jobs, njobs, max_n, max_N, info, s, launches, timer, tc, err, sparse_jobs);
 }
 
 cudaError_t launch_finalize_direct(FactorKind fk, const JobDev *jobs, int njobs, int ns, int kkrsz, int *info,
@@ -624,8 +706,20 @@ cudaError_t launch_refine_begin(FactorKind fk, const JobDev *jobs, int njobs, in
 cudaError_t launch_refine_round(FactorKind fk, const JobDev *jobs, int njobs, int max_n, int max_N, int b,
                                 bool check, int *info, cudaStream_t s, long *launches, bool fp32_sweep) {
   (void)max_n;
-  if (b <= 16) residual_kernel<16><<<dim3((max_N + 255) / 256, njobs), 256, 0, s>>>(jobs);
-  else residual_kernel<32><<<dim3((max_N + 127) / 128, njobs), 256, 0, s>>>(jobs);
+  cudaError_t e0;
+  if (b <= 16) {
+    constexpr int sm16 = residual_smem_bytes<16>();
+    if ((e0 = cudaFuncSetAttribute(residual_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm16)) !=
+        cudaSuccess)
+      return e0;
+    residual_kernel<16><<<dim3((max_N + residual_rows<16>() - 1) / residual_rows<16>(), njobs), 256, sm16, s>>>(jobs);
+  } else {
+    constexpr int sm32 = residual_smem_bytes<32>();
+    if ((e0 = cudaFuncSetAttribute(residual_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm32)) !=
+        cudaSuccess)
+      return e0;
+    residual_kernel<32><<<dim3((max_N + residual_rows<32>() - 1) / residual_rows<32>(), njobs), 256, sm32, s>>>(jobs);
+  }
   if (launches) *launches += 1;
   const cudaError_t e = fk == kFactorFP64 ? sweep_solve<double2>(jobs, njobs, b, 1, info, s, launches, false)
                                            : sweep_solve<float2>(jobs, njobs, b, 1, info, s, launches, fp32_sweep);

@@ -85,10 +85,10 @@ struct b200tau_ctx {
   size_t adj_cap = 0;
   unsigned char *d_tdiag = nullptr;  // per (store, energy, spin) t block: exactly diagonal
   long launches = 0;
-  long fallbacks = 0;  // mixed-precision jobs re-solved in FP64 by the last solve call
   bool fallback_on = true;
-  double2 *d_ffb = nullptr;  // FP64 factor storage of those re-solves (kFallbackChunk jobs)
+  double2 *d_ffb = nullptr;  // FP64 factor storage of those re-solves, one per slot
   size_t ffb_elems = 0;
+  int *d_fbcount = nullptr;  // their number (device counter of the last solve call)
   int max_slots = 64;
   // refinement rounds, FP64 and MIXED; MIXED stops early per job once the correction estimate
   // is below kRefineTol of tau00 (block_lu.cu, converge_check_kernel)
@@ -393,11 +393,6 @@ double trailing_flops(const std::vector<JobDev> &h) {
   return f;
 }
 
-// Refinement rounds run on every job of the wave until this many are done; then the host reads the
-// converged flags once and the remaining rounds run on the unconverged jobs only.
-constexpr int kCompactAfterRounds = 2;
-// FP64 re-solves of unconverged mixed jobs run this many jobs at a time.
-constexpr int kFallbackChunk = 8;
 
 int ensure_jobs2(b200tau_ctx *ctx, int n) {
   if (n <= ctx->jobs2_cap) return B200TAU_OK;
@@ -405,6 +400,26 @@ int ensure_jobs2(b200tau_ctx *ctx, int n) {
   ctx->d_jobs2 = nullptr;
   CK(cudaMalloc(&ctx->d_jobs2, sizeof(JobDev) * n));
   ctx->jobs2_cap = n;
+  return B200TAU_OK;
+}
+
+// Refinement rounds run on every job of the wave until this many are done.
+constexpr int kCompactAfterRounds = 2;
+
+// FP64 storage for re-solving any job of a mixed wave (one ld x ld block per slot) and the
+// device counter of re-solved jobs.
+int ensure_fallback(b200tau_ctx *ctx, int ld) {
+  const size_t need = (size_t)ld * ld * ctx->slots;
+  if (!ctx->d_fbcount) {
+    CK(cudaMalloc(&ctx->d_fbcount, sizeof(int)));
+    CK(cudaMemsetAsync(ctx->d_fbcount, 0, sizeof(int), ctx->stream));
+  }
+  if (ctx->d_ffb && need <= ctx->ffb_elems) return B200TAU_OK;
+  CK(cudaStreamSynchronize(ctx->stream));
+  cudaFree(ctx->d_ffb);
+  ctx->d_ffb = nullptr;
+  CK(cudaMalloc(&ctx->d_ffb, sizeof(double2) * need));
+  ctx->ffb_elems = need;
   return B200TAU_OK;
 }
 
@@ -416,6 +431,9 @@ int run_refinement(b200tau_ctx *ctx, const std::vector<JobDev> &h, int nw, int m
   const bool fp32_sweep = p.fk == kFactorFP32 && ctx->mixed_sweep == B200TAU_SWEEP_FP32;
   CK(launch_refine_begin(p.fk, ctx->d_jobs, nw, maxn, maxN, b, ctx->d_info, ctx->stream, &ctx->launches,
                          fp32_sweep));
+  // The kernels skip converged jobs.  After kCompactAfterRounds rounds the host reads the converged
+  // flags once (the only wait inside a wave; the rest of the wave is queued right after it) and
+  // the remaining rounds run on the unconverged jobs alone, with launches sized for them.
   const JobDev *cur = ctx->d_jobs;
   int ncur = nw, cmaxn = maxn, cmaxN = maxN;
   int *cur_info = ctx->d_info;
@@ -451,47 +469,18 @@ int run_refinement(b200tau_ctx *ctx, const std::vector<JobDev> &h, int nw, int m
   // Jobs whose FP32-factor refinement did not converge (condition numbers beyond what FP32 block
   // factors can refine, e.g. energies next to the real axis) take the FP64 path instead: an FP64
   // copy of the unmodified M, FP64 block elimination, the FP64 refinement rounds, tau00 from X -
-  // the same kernels and arithmetic as a PREC_FP64 solve of the job.
-  std::vector<int> conv(nw);
-  CK(cudaMemcpyAsync(conv.data(), ctx->d_conv, sizeof(int) * nw, cudaMemcpyDeviceToHost, ctx->stream));
-  CK(cudaStreamSynchronize(ctx->stream));
-  std::vector<JobDev> fb;
-  for (int w = 0; w < nw; ++w)
-    if (conv[w] != kConverged) fb.push_back(h[w]);
-  if (fb.empty()) return B200TAU_OK;
-  int rc = ensure_jobs2(ctx, ctx->slots);
-  if (rc) return rc;
-  const int ld = fb[0].ld;
-  const size_t f64 = (size_t)ld * ld;
-  const int chunk = std::min((int)fb.size(), kFallbackChunk);
-  if (!ctx->d_ffb || f64 * chunk > ctx->ffb_elems) {
-    CK(cudaStreamSynchronize(ctx->stream));
-    cudaFree(ctx->d_ffb);
-    ctx->d_ffb = nullptr;
-    ctx->ffb_elems = std::max(f64 * chunk, ctx->ffb_elems);
-    CK(cudaMalloc(&ctx->d_ffb, sizeof(double2) * ctx->ffb_elems));
-  }
-  for (size_t c0 = 0; c0 < fb.size(); c0 += chunk) {
-    const int nc = (int)std::min(fb.size() - c0, (size_t)chunk);
-    int cmaxn2 = 0, cmaxN2 = 0;
-    for (int i = 0; i < nc; ++i) {
-      JobDev &J = fb[c0 + i];
-      J.F = ctx->d_ffb + (size_t)i * f64;
-      J.conv = nullptr;  // the FP64 rounds run unconditionally
-      J.cnorm = nullptr;
-      CK(launch_copy_to_factor(kFactorFP64, J.M, J.F, J.N, J.ld, ctx->stream));
-      cmaxn2 = std::max(cmaxn2, J.n);
-      cmaxN2 = std::max(cmaxN2, J.N);
-    }
-    // (the host copy of this chunk stays valid: the pageable upload is staged before returning)
-    CK(cudaMemcpyAsync(ctx->d_jobs2, fb.data() + c0, sizeof(JobDev) * nc, cudaMemcpyHostToDevice, ctx->stream));
-    int *finfo = ctx->d_info + ctx->slots;
-    CK(launch_eliminate(kFactorFP64, ctx->d_jobs2, nc, cmaxn2, cmaxN2, finfo, ctx->stream, &ctx->launches,
-                        nullptr, nullptr, ctx->d_err));
-    CK(launch_solve_refine(kFactorFP64, ctx->d_jobs2, nc, cmaxn2, cmaxN2, b, std::max(1, ctx->refine_steps[0]),
-                           ns, kkrsz, finfo, ctx->stream, &ctx->launches));
-  }
-  ctx->fallbacks += (long)fb.size();
+  // the same kernels and arithmetic as a PREC_FP64 solve of the job.  The selection happens on the
+  // device (converged jobs become inactive records), so the host never waits inside a wave.
+  const int ld = h[0].ld;
+  int rc = ensure_fallback(ctx, ld);
+  if (rc || (rc = ensure_jobs2(ctx, ctx->slots))) return rc;
+  int *finfo = ctx->d_info + ctx->slots;
+  CK(launch_fallback_prepare(ctx->d_jobs, ctx->d_jobs2, nw, ctx->d_ffb, (size_t)ld * ld, maxN, ctx->d_fbcount,
+                             ctx->stream, &ctx->launches));
+  CK(launch_eliminate(kFactorFP64, ctx->d_jobs2, nw, maxn, maxN, finfo, ctx->stream, &ctx->launches, nullptr,
+                      nullptr, ctx->d_err, true));
+  CK(launch_solve_refine(kFactorFP64, ctx->d_jobs2, nw, maxn, maxN, b, std::max(1, ctx->refine_steps[0]), ns, kkrsz,
+                         finfo, ctx->stream, &ctx->launches));
   return B200TAU_OK;
 }
 
@@ -576,6 +565,7 @@ int run_wave(b200tau_ctx *ctx, const b200tau_job *jobs, const int *idx, int nw, 
   }
   CK(cudaMemcpyAsync(ctx->d_jobs, h.data(), sizeof(JobDev) * nw, cudaMemcpyHostToDevice, ctx->stream));
   int rc = reset_slot_status(ctx, nw);
+  if (rc) return rc;
   if (rc || (rc = phase_begin(ctx))) return rc;
   CK(launch_kkr_build(ctx->d_jobs, nw, maxL, build_params(ctx, p), ctx->d_err, ctx->stream, &ctx->launches));
   if ((rc = phase_end(ctx, 0))) return rc;
@@ -638,11 +628,13 @@ int solve_impl(b200tau_ctx *ctx, const b200tau_job *jobs, int njobs, int prec, d
   });
   const int maxN = ctx->atoms[jobs[order[0]].atom].N;
   const int ld = round_up(maxN, 64);
-  const int slots = choose_slots(ctx, ld, njobs, p);
+  // mixed with the FP64 re-solve enabled also holds an FP64 copy of M per slot
+  const size_t extra = (p.fk == kFactorFP32 && ctx->fallback_on) ? (size_t)ld * ld * sizeof(double2) : 0;
+  const int slots = choose_slots(ctx, ld, njobs, p, extra);
   if ((rc = ensure_workspace(ctx, ld, slots, p))) return rc;
   if ((rc = ensure_jobs(ctx, slots))) return rc;
   ctx->launches = 0;
-  ctx->fallbacks = 0;
+  if (ctx->d_fbcount) CK(cudaMemsetAsync(ctx->d_fbcount, 0, sizeof(int), ctx->stream));
   std::vector<int> info(slots);
   for (int w0 = 0; w0 < njobs; w0 += slots) {
     const int nw = std::min(slots, njobs - w0);
@@ -731,6 +723,7 @@ void b200tau_destroy(b200tau_ctx *ctx) {
   cudaFree(ctx->d_V);
   cudaFree(ctx->d_adj);
   cudaFree(ctx->d_ffb);
+  cudaFree(ctx->d_fbcount);
   for (auto &e : ctx->events) cudaEventDestroy(e);
   for (auto &e : ctx->pev) cudaEventDestroy(e);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
@@ -743,7 +736,14 @@ void *b200tau_stream(b200tau_ctx *ctx) { return ctx ? (void *)ctx->stream : null
 
 long b200tau_last_launch_count(const b200tau_ctx *ctx) { return ctx ? ctx->launches : 0; }
 
-long b200tau_last_fallback_count(const b200tau_ctx *ctx) { return ctx ? ctx->fallbacks : 0; }
+long b200tau_last_fallback_count(const b200tau_ctx *ctx) {
+  if (!ctx || !ctx->d_fbcount) return 0;
+  int n = 0;
+  if (cudaSetDevice(ctx->device) != cudaSuccess ||
+      cudaMemcpy(&n, ctx->d_fbcount, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+    return -1;
+  return n;
+}
 
 int b200tau_gaunt_numbers(int lmax, double *cgnt) {
   if (lmax < 0 || lmax > kMaxLmax || !cgnt) return B200TAU_ERR_ARG;

@@ -83,7 +83,8 @@ struct JobDev {
   int iie, ispin;
   int t0_ld;
   int out_mode;          // 0: tau00_l (tau00 - t0, rotated); 1: raw tau00
-  int pad_[3];
+  int inactive;          // 1: every kernel skips this record (a converged job in the FP64 re-solve)
+  int pad_[2];
   // adjoint (b200tau_solve_vjp) only
   double2 *V;            // N x N workspace for M^-1 (ld)
   const double2 *taubar; // b x b cotangent on tau00
@@ -136,11 +137,18 @@ cudaError_t launch_kkr_build(const JobDev *jobs, int njobs, int max_L, const Bui
                              int *err_flags, cudaStream_t s, long *launches);
 // Block elimination of F over the first n columns (all jobs of the wave).
 // With FP32 factors and `tc` non-null the trailing update runs on the tensor cores (tc_update.cu).
+// `sparse_jobs`: most records are inactive (the FP64 re-solve), so the trailing update runs on a
+// small looping grid instead of one CTA per tile.
 cudaError_t launch_eliminate(FactorKind fk, const JobDev *jobs, int njobs, int max_n, int max_N,
                              int *info, cudaStream_t s, long *launches, KernelTimer *timer,
-                             const TcMaps *tc, int *err);
+                             const TcMaps *tc, int *err, bool sparse_jobs = false);
 // F = M (n x n, leading dimension ld) converted to the factor type.
 cudaError_t launch_copy_to_factor(FactorKind fk, const double2 *M, void *F, int n, int ld, cudaStream_t s);
+// FP64 re-solve of the mixed jobs whose refinement did not converge, on the device: out[w] is
+// jobs[w] with F at f64 + w * f64_stride (an FP64 copy of M is made there) and no converged flag,
+// or an inactive record when jobs[w] converged; `count` accumulates the re-solved jobs.
+cudaError_t launch_fallback_prepare(const JobDev *jobs, JobDev *out, int njobs, double2 *f64, size_t f64_stride,
+                                    int max_N, int *count, cudaStream_t s, long *launches);
 // tau00 from the Schur block directly (no refinement): out = S^-1 t0 (- t0, rotated).
 cudaError_t launch_finalize_direct(FactorKind fk, const JobDev *jobs, int njobs, int ns, int kkrsz,
                                    int *info, cudaStream_t s, long *launches);

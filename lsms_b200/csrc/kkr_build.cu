@@ -26,14 +26,21 @@ namespace {
 constexpr int kWarps = 8;
 constexpr int kThreads = kWarps * 32;
 
+// Per-pair prologue values, one column per lane of a warp (lane q holds row-site pair q of the
+// warp's batch): hfn_l (re, im), normalised P_lm, cos(m phi), sin(m phi).
+constexpr int kProH = 0;                          // 2 (kMaxLend + 1) doubles
+constexpr int kProP = kProH + 2 * (kMaxLend + 1);  // kNdlm
+constexpr int kProC = kProP + kNdlm;               // kMaxLend + 1
+constexpr int kProS = kProC + kMaxLend + 1;        // kMaxLend + 1
+constexpr int kProN = kProS + kMaxLend + 1;
+
+constexpr int kBatch = 16;  // pairs per prologue batch of a warp
+
 struct BuildSmem {
   AngularTables tab;
   double2 D[kWarps][kNdlj];
-  double2 G[kWarps][kMaxKK * kMaxKK];
-  double2 H[kWarps][kMaxLend + 2];
-  double P[kWarps][kNdlm + 4];
-  double C[kWarps][kMaxLend + 2];
-  double S[kWarps][kMaxLend + 2];
+  double2 G[kWarps][kMaxKK * kMaxKK];  // staged only for a non-diagonal t
+  double pro[kWarps][kProN][kBatch];
   unsigned long long bar;
 };
 
@@ -136,7 +143,93 @@ __global__ void __launch_bounds__(kThreads)
   // collinear spin-polarised: spin block offset kkrsz^2 * ispin (buildKKRMatrix_CPU.cpp:402)
   const long jsm = (p.npola != p.ns) ? (long)kkrsz * kkrsz * J.ispin : 0;
 
-  for (int pr = warp; pr < J.L; pr += kWarps) {
+  // The warp's row sites are pr = warp + kWarps q.  For a batch of kBatch of them, lane q first
+  // computes pair q's Hankel functions, Legendre functions and cos/sin(m phi) (the scalar
+  // prologue of each pair, in parallel across lanes); then the warp builds the pairs' blocks one
+  // after another from those values.
+  double(*pro)[kBatch] = sm.pro[warp];
+  for (int base = 0; warp + kWarps * base < J.L; base += kBatch) {
+    if (lane < kBatch) {
+      const int pr = warp + kWarps * (base + lane);
+      if (pr < J.L && pr != pc) {
+        const int i = J.perm[pr];
+        const int lend = J.lmax[i] + lj;
+        // rij = pos(ir1) - pos(ir2), ir1 = row site (calculateTauMatrix.cpp:206-208)
+        const double rx = J.pos[3 * i + 0] - J.pos[3 * j + 0];
+        const double ry = J.pos[3 * i + 1] - J.pos[3 * j + 1];
+        const double rz = J.pos[3 * i + 2] - J.pos[3 * j + 2];
+        const double r = sqrt(rx * rx + ry * ry + rz * rz);
+        // spherical Hankel recursion, hfn_l = -i^(l+1) h_l(kR) e^{ikR}/R (:23-40)
+        double2 H[kMaxLend + 1];
+        const double2 z = make_double2(prel.x * r, prel.y * r);
+        const double2 zi = cdiv(make_double2(1.0, 0.0), z);
+        H[0] = make_double2(0.0, -1.0);
+        {
+          const double2 t = cmul(make_double2(0.0, 1.0), zi);
+          H[1] = make_double2(-1.0 - t.x, -t.y);
+        }
+#pragma unroll
+        for (int l = 1; l < kMaxLend; ++l) {
+          const double2 a = cmul(H[l], zi);
+          H[l + 1] = make_double2((2.0 * l + 1.0) * a.x - H[l - 1].x, (2.0 * l + 1.0) * a.y - H[l - 1].y);
+        }
+        double sn, cs;
+        sincos(z.x, &sn, &cs);
+        const double e = exp(-z.y) / r;
+        const double2 f = make_double2(e * cs, e * sn);  // e^{iz}/r
+#pragma unroll
+        for (int l = 0; l <= kMaxLend; ++l) {
+          if (l > lend) break;
+          double2 h = cmul(H[l], f);
+          h = cmul(h, make_double2(T.ilp1_re[l], T.ilp1_im[l]));
+          pro[kProH + 2 * l][lane] = -h.x;
+          pro[kProH + 2 * l + 1][lane] = -h.y;
+        }
+        // normalised P_lm(cos theta) (associatedLegendreFunction.hpp:33-69)
+        double P[kNdlm];
+        const double x = rz / r;
+        const double y = sqrt(1.0 - x * x);
+        P[0] = sqrt(1.0 / (4.0 * 3.14159265358979323846));
+#pragma unroll
+        for (int m = 1; m <= kMaxLend; ++m) {
+          const int mm = m * (m + 1) / 2 + m, pm = (m - 1) * m / 2 + (m - 1);
+          P[mm] = -T.plm_mm[m] * y * P[pm];
+          P[mm - 1] = T.plm_m1[m] * x * P[pm];
+        }
+#pragma unroll
+        for (int m = 0; m < kMaxLend; ++m)
+#pragma unroll
+          for (int l = m + 2; l <= kMaxLend; ++l) {
+            const int k = l * (l + 1) / 2 + m;
+            P[k] = T.plm_a[k] * (x * P[(l - 1) * l / 2 + m] - T.plm_b[k] * P[(l - 2) * (l - 1) / 2 + m]);
+          }
+#pragma unroll
+        for (int k = 0; k < kNdlm; ++k) pro[kProP + k][lane] = P[k];
+        // cos(m phi), sin(m phi) (:42-59)
+        const double pmag = sqrt(rx * rx + ry * ry);
+        double c1 = 0.0, s1 = 0.0;
+        if (pmag > 1.0e-6) {
+          c1 = rx / pmag;
+          s1 = ry / pmag;
+        }
+        double C = 1.0, S = 0.0;
+        pro[kProC][lane] = 1.0;
+        pro[kProS][lane] = 0.0;
+#pragma unroll
+        for (int m = 1; m <= kMaxLend; ++m) {
+          const double Cm = m == 1 ? c1 : C * c1 - S * s1;
+          const double Sm = m == 1 ? s1 : S * c1 + C * s1;
+          C = Cm;
+          S = Sm;
+          pro[kProC + m][lane] = C;
+          pro[kProS + m][lane] = S;
+        }
+      }
+    }
+    __syncwarp();
+    for (int q = 0; q < kBatch; ++q) {
+    const int pr = warp + kWarps * (base + q);
+    if (pr >= J.L) break;
     const int i = J.perm[pr];
     const int li = J.lmax[i];
     const int kki = (li + 1) * (li + 1);
@@ -149,98 +242,40 @@ __global__ void __launch_bounds__(kThreads)
           put((size_t)(row0 + r) + (size_t)(col0 + c) * ld, make_double2(r == c ? one : 0.0, 0.0));
       continue;
     }
-    // rij = pos(ir1) - pos(ir2), ir1 = row site (calculateTauMatrix.cpp:206-208)
-    const double rx = J.pos[3 * i + 0] - J.pos[3 * j + 0];
-    const double ry = J.pos[3 * i + 1] - J.pos[3 * j + 1];
-    const double rz = J.pos[3 * i + 2] - J.pos[3 * j + 2];
-    const double r = sqrt(rx * rx + ry * ry + rz * rz);
     const int lend = li + lj;
-    if (lane == 0) {
-      // spherical Hankel recursion, hfn_l = -i^(l+1) h_l(kR) e^{ikR}/R (:23-40)
-      double2 *H = sm.H[warp];
-      const double2 z = make_double2(prel.x * r, prel.y * r);
-      const double2 zi = cdiv(make_double2(1.0, 0.0), z);
-      H[0] = make_double2(0.0, -1.0);
-      if (lend >= 1) {
-        const double2 t = cmul(make_double2(0.0, 1.0), zi);
-        H[1] = make_double2(-1.0 - t.x, -t.y);
-      }
-      for (int l = 1; l < lend; ++l) {
-        const double2 a = cmul(H[l], zi);
-        H[l + 1] = make_double2((2.0 * l + 1.0) * a.x - H[l - 1].x, (2.0 * l + 1.0) * a.y - H[l - 1].y);
-      }
-      double s, c;
-      sincos(z.x, &s, &c);
-      const double e = exp(-z.y) / r;
-      const double2 f = make_double2(e * c, e * s);  // e^{iz}/r
-      for (int l = 0; l <= lend; ++l) {
-        double2 h = cmul(H[l], f);
-        h = cmul(h, make_double2(T.ilp1_re[l], T.ilp1_im[l]));
-        H[l] = make_double2(-h.x, -h.y);
-      }
-    } else if (lane == 1) {
-      // normalised P_lm(cos theta) (associatedLegendreFunction.hpp:33-69)
-      double *P = sm.P[warp];
-      const double x = rz / r;
-      const double y = sqrt(1.0 - x * x);
-      P[0] = sqrt(1.0 / (4.0 * 3.14159265358979323846));
-      for (int m = 1; m <= lend; ++m) {
-        const int mm = m * (m + 1) / 2 + m, pm = (m - 1) * m / 2 + (m - 1);
-        P[mm] = -T.plm_mm[m] * y * P[pm];
-        P[mm - 1] = T.plm_m1[m] * x * P[pm];
-      }
-      for (int m = 0; m < lend; ++m)
-        for (int l = m + 2; l <= lend; ++l) {
-          const int k = l * (l + 1) / 2 + m;
-          P[k] = T.plm_a[k] * (x * P[(l - 1) * l / 2 + m] - T.plm_b[k] * P[(l - 2) * (l - 1) / 2 + m]);
-        }
-    } else if (lane == 2) {
-      // cos(m phi), sin(m phi) (:42-59)
-      double *C = sm.C[warp];
-      double *S = sm.S[warp];
-      const double pmag = sqrt(rx * rx + ry * ry);
-      C[0] = 1.0;
-      S[0] = 0.0;
-      double c1 = 0.0, s1 = 0.0;
-      if (pmag > 1.0e-6) {
-        c1 = rx / pmag;
-        s1 = ry / pmag;
-      }
-      if (lend >= 1) {
-        C[1] = c1;
-        S[1] = s1;
-      }
-      for (int m = 2; m <= lend; ++m) {
-        C[m] = C[m - 1] * c1 - S[m - 1] * s1;
-        S[m] = S[m - 1] * c1 + C[m - 1] * s1;
-      }
-    }
-    __syncwarp();
     // D_{l,m} = hfn_l P_l|m| (cos m phi -/+ i sin m phi), (-1)^m for m < 0 (:127-140)
-    for (int q = lane; q < (lend + 1) * (lend + 1); q += 32) {
-      int l = 0;
-      while ((l + 1) * (l + 1) <= q) ++l;
-      const int m = q - l * (l + 1);
+    for (int e = lane; e < (lend + 1) * (lend + 1); e += 32) {
+      const int l = (int)sqrtf((float)e);  // exact: e < 64 and squares are exact in FP32
+      const int m = e - l * (l + 1);
       const int am = m < 0 ? -m : m;
-      const double pl = sm.P[warp][l * (l + 1) / 2 + am];
-      const double2 h = sm.H[warp][l];
-      double2 f = make_double2(pl * sm.C[warp][am], -pl * sm.S[warp][am]);
+      const double pl = pro[kProP + l * (l + 1) / 2 + am][q];
+      const double2 h = make_double2(pro[kProH + 2 * l][q], pro[kProH + 2 * l + 1][q]);
+      const double cm = pro[kProC + am][q], sm_ = pro[kProS + am][q];
+      double2 f = make_double2(pl * cm, -pl * sm_);
       if (m < 0) {
         const double sg = (am & 1) ? -1.0 : 1.0;
-        f = make_double2(sg * pl * sm.C[warp][am], sg * pl * sm.S[warp][am]);
+        f = make_double2(sg * pl * cm, sg * pl * sm_);
       }
-      sm.D[warp][q] = cmul(h, f);
+      sm.D[warp][e] = cmul(h, f);
     }
     __syncwarp();
-    // G(lm2, lm1) = pi4 i^(l2-l1) sum_l3 cgnt(l3/2, lm1, lm2) D(l3, m2-m1) (:148-176)
+    // M block = -t_i * diag_s(G): rows (s_r, r'), columns (s_c, c') (setgij.f:29-38)
+    const double2 *__restrict__ tb =
+        p.tmat + (long)J.store[i] * p.tmat_ld + (long)J.iie * p.blk + jsm;
+    const bool tdiag = p.tdiag != nullptr && p.tdiag[((long)J.store[i] * p.group + J.iie) * 2 + J.ispin] != 0;
+    // With a diagonal t (spherical scatterer) or for G itself each G element gives its M
+    // elements directly; otherwise G is staged for the t G product.
+    const bool direct = tdiag || p.g_mode;
+    // G(lm2, lm1) = pi4 i^(l2-l1) sum_l3 cgnt(l3/2, lm1, lm2) D(l3, m2-m1) (:148-176); lanes run
+    // along lm2 (rows) so that the direct stores are column segments
     for (int e = lane; e < kki * kkj; e += 32) {
-      const int lm2 = e / kkj, lm1 = e - lm2 * kkj;
+      const int lm1 = e / kki, lm2 = e - lm1 * kki;
       const int te = lm2 * kMaxKK + lm1;
       double2 acc = make_double2(0.0, 0.0);
       const int nt = T.nterm[te];
-      for (int q = 0; q < nt; ++q) {
-        const double cg = T.coef[te * kMaxTerms + q];
-        const double2 d = sm.D[warp][T.didx[te * kMaxTerms + q]];
+      for (int q2 = 0; q2 < nt; ++q2) {
+        const double cg = T.coef[te * kMaxTerms + q2];
+        const double2 d = sm.D[warp][T.didx[te * kMaxTerms + q2]];
         acc.x += cg * d.x;
         acc.y += cg * d.y;
       }
@@ -251,45 +286,26 @@ __global__ void __launch_bounds__(kThreads)
       if (rot == 1) g = make_double2(-acc.y, acc.x);
       else if (rot == 2) g = make_double2(-acc.x, -acc.y);
       else if (rot == 3) g = make_double2(acc.y, -acc.x);
-      sm.G[warp][lm2 * kMaxKK + lm1] = g;
+      if (!direct) {
+        sm.G[warp][lm2 * kMaxKK + lm1] = g;
+        continue;
+      }
+      for (int sr = 0; sr < ns; ++sr) {
+        double2 v = g;
+        if (!p.g_mode) {  // -t_rr G, rounded as the general path's one nonzero term
+          const int trow = sr * kkrsz + lm2;
+          const double2 pr2 = cfma(__ldg(tb + trow + (long)trow * bstore), g, make_double2(0.0, 0.0));
+          v = make_double2(-pr2.x, -pr2.y);
+        }
+        for (int sc = 0; sc < ns; ++sc)
+          put((size_t)(row0 + sr * kki + lm2) + (size_t)(col0 + sc * kkj + lm1) * ld,
+              sc == sr ? v : make_double2(0.0, 0.0));
+      }
     }
     __syncwarp();
-    if (p.g_mode) {  // G itself, spin-diagonal (setgij.f:29-38 without the t factor)
-      for (int rr = lane & 15; rr < nr; rr += 16) {
-        const int sr = rr / kki, rp = rr - sr * kki;
-        for (int sc = 0; sc < ns; ++sc)
-          for (int cp = lane >> 4; cp < kkj; cp += 2)
-            put((size_t)(row0 + rr) + (size_t)(col0 + sc * kkj + cp) * ld,
-                sc == sr ? sm.G[warp][rp * kMaxKK + cp] : make_double2(0.0, 0.0));
-      }
-      __syncwarp();
-      continue;
-    }
-    // M block = -t_i * diag_s(G): rows (s_r, r'), columns (s_c, c') (setgij.f:29-38)
-    const double2 *__restrict__ tb =
-        p.tmat + (long)J.store[i] * p.tmat_ld + (long)J.iie * p.blk + jsm;
+    if (direct) continue;
     const int r_lo = lane & 15;
     const int c_par = lane >> 4;
-    const bool tdiag = p.tdiag != nullptr && p.tdiag[((long)J.store[i] * p.group + J.iie) * 2 + J.ispin] != 0;
-    if (tdiag) {
-      // t_i diagonal (spherical scatterer): M[(s, r'), (s', c')] = -delta_ss' t_rr G[r', c']
-      for (int rr = r_lo; rr < nr; rr += 16) {
-        const int sr = rr / kki, rp = rr - sr * kki;
-        const int trow = sr * kkrsz + rp;
-        const double2 tr = __ldg(tb + trow + (long)trow * bstore);
-        for (int sc = 0; sc < ns; ++sc)
-          for (int cp = c_par; cp < kkj; cp += 2) {
-            double2 v = make_double2(0.0, 0.0);
-            if (sc == sr) {  // the general path's one nonzero term, rounded the same way
-              const double2 pr = cfma(tr, sm.G[warp][rp * kMaxKK + cp], make_double2(0.0, 0.0));
-              v = make_double2(-pr.x, -pr.y);
-            }
-            put((size_t)(row0 + rr) + (size_t)(col0 + sc * kkj + cp) * ld, v);
-          }
-      }
-      __syncwarp();
-      continue;
-    }
     for (int rr = r_lo; rr < nr; rr += 16) {
       const int trow = (rr / kki) * kkrsz + (rr % kki);
       for (int sc = 0; sc < ns; ++sc) {
@@ -308,6 +324,7 @@ __global__ void __launch_bounds__(kThreads)
       }
     }
     __syncwarp();
+    }
   }
 }
 

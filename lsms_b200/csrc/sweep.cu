@@ -187,7 +187,8 @@ __global__ void __launch_bounds__(256) forward_sweep_kernel(const JobDev *__rest
   constexpr int NJ = BC / 4;
   using L = SweepSmem<T, V>;
   const JobDev &J = jobs[blockIdx.y];
-  if (converged(J.conv) || J.n == 0) return;  // uniform over the cluster: the flag changes between launches
+  // uniform over the cluster: the flag changes only between launches
+  if (converged(J.conv) || J.n == 0 || J.inactive) return;
   const int rank = cluster_rank(), cs = cluster_size();
   const int n = J.n, N = J.N, ld = J.ld, b = J.b;
   const T *__restrict__ F = static_cast<const T *>(J.F);
@@ -299,7 +300,7 @@ __global__ void __launch_bounds__(256) backward_sweep_kernel(const JobDev *__res
   constexpr int NJ = BC / 4;
   using L = SweepSmem<T, V>;
   const JobDev &J = jobs[blockIdx.y];
-  if (mode == 1 && converged(J.conv)) return;
+  if ((mode == 1 && converged(J.conv)) || J.inactive) return;
   const int rank = cluster_rank(), cs = cluster_size();
   const int n = J.n, ld = J.ld, b = J.b;
   const T *__restrict__ F = static_cast<const T *>(J.F);
