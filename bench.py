@@ -39,9 +39,10 @@ sys.path.insert(0, ROOT)
 
 METRIC = "tau00 solves/s at N=2160 c128: mixed vs plain FP64 at <=1e-10 rel err; %peak"
 N_ENERGIES = 31
-# DRAM bytes (read + write) per tc_update_kernel launch, from the ncu capture summarised in
-# profiles/ (None until captured).
-TRAFFIC_PER_LAUNCH = None
+# DRAM bytes (read + write) per tc_update_kernel launch of this workload: the ncu capture of a
+# 4-job launch at k = 320 (profiles/tc_update_contour2160_e4.md) measured 13.45 B per trailing-block
+# entry; scaled to 31 jobs and the average trailing block over the 34 steps (1.476e6 entries).
+TRAFFIC_PER_LAUNCH = 615.3e6
 
 
 def algorithmic_flops(N: int, b: int, L: int) -> float:
@@ -171,7 +172,59 @@ WORKLOADS = {
                     "mixed vs FP64",
     "adjoint": "64 atoms x 16 energies, fcc LIZ 87 sites (N=1392): tau00 plus d tau00/d t and "
                "d ln det M/d t for every LIZ site (b200tau_solve_vjp, FP64)",
+    "comparators": "library baselines on this GPU: cuSOLVER batched zgetrf+zgetrs (torch.linalg.solve) on "
+                   "the headline's 31 KKR matrices (N=2160, 16 right-hand sides), and cuBLAS "
+                   "DGEMM / ZGEMM / SGEMM peaks",
 }
+
+
+def run_comparators(args, local):
+    """The reference GPU comparator of the benchmark table (cuSOLVER LU on the same M) and the
+    FP64 / FP32 library GEMM rates used as roofline context."""
+    import torch
+    from lsms_b200 import tau as T
+    from lsms_b200 import workloads as W
+    torch.cuda.set_device(local)
+    prob = W.config_n2160(npts=N_ENERGIES)
+    N, b = prob.nrmat_ns, prob.kkrsz_ns
+    s = T.TauSolver(prob.lmax, prob.n_spin_cant, prob.n_spin_pola, device=local)
+    s.load_problem(prob)
+    ms = torch.empty(N_ENERGIES, N, N, dtype=torch.complex128, device=f"cuda:{local}")
+    rhs = torch.zeros(N_ENERGIES, N, b, dtype=torch.complex128, device=f"cuda:{local}")
+    for i in range(N_ENERGIES):
+        ms[i] = torch.from_numpy(s.build_kkr(0, i, 0, prob.energies[i], N))
+        rhs[i, :b] = torch.from_numpy(prob.t_block(int(prob.liz_store_idx[0]), i))
+    s.close()
+
+    def events(fn, reps):
+        for _ in range(max(1, args.warmup)):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        e1.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    sol = {}
+    t_lu = events(lambda: sol.update(x=torch.linalg.solve(ms, rhs)), max(1, args.steps))
+    del ms, rhs, sol
+
+    def gemm_tflops(dtype, n):
+        a = torch.randn(n, n, dtype=dtype, device=f"cuda:{local}")
+        bb = torch.randn(n, n, dtype=dtype, device=f"cuda:{local}")
+        t = events(lambda: a @ bb, 10)
+        return (8 if dtype.is_complex else 2) * n ** 3 / (t * 1e-3) / 1e12
+
+    line = {"metric": "comparators", "config": {"workload": WORKLOADS["comparators"]},
+            "cusolver_zgesv": {"value": N_ENERGIES / (t_lu * 1e-3), "unit": "solves/s", "ms_per_step": t_lu,
+                               "note": "factor + solve of the built M only (no build, no tau00 post-processing)"},
+            "cublas_dgemm_tflops": gemm_tflops(torch.float64, 8192),
+            "cublas_zgemm_tflops": gemm_tflops(torch.complex128, 4096),
+            "cublas_sgemm_tflops": gemm_tflops(torch.float32, 8192)}
+    print(json.dumps(line))
 
 
 def run_workload(args, world, rank, local):
@@ -277,6 +330,10 @@ def main():
 
     if args.impl == "reference":
         run_reference(args, world, rank)
+        return
+    if args.workload == "comparators":
+        if rank == 0:
+            run_comparators(args, local)
         return
     if args.workload != "contour2160":
         run_workload(args, world, rank, local)
