@@ -300,11 +300,18 @@ __device__ __forceinline__ void zgemm_tile_body(const JobDev &J, int k, int bx, 
 template <typename S, int MODE>
 __global__ void __launch_bounds__(256, 2) zgemm_tile_kernel(const JobDev *__restrict__ jobs, int k, int tx, int ty,
                                                             int nj) {
-  const int total = tx * ty * nj;
+  if (gridDim.z == (unsigned)nj && gridDim.x == (unsigned)tx && gridDim.y == (unsigned)ty) {
+    zgemm_tile_body<S, MODE>(jobs[blockIdx.z], k, blockIdx.x, blockIdx.y);
+    return;
+  }
+  // looping grid: jobs one after another (an inactive job costs one check), its tiles spread
+  // over the CTAs
   const int nblk = gridDim.x * gridDim.y * gridDim.z;
-  for (int vb = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z); vb < total; vb += nblk) {
-    const int bx = vb % tx, by = (vb / tx) % ty, bz = vb / (tx * ty);
-    zgemm_tile_body<S, MODE>(jobs[bz], k, bx, by);
+  const int b0 = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+  for (int bz = 0; bz < nj; ++bz) {
+    const JobDev &J = jobs[bz];
+    if (J.inactive || k >= J.n) continue;
+    for (int vb = b0; vb < tx * ty; vb += nblk) zgemm_tile_body<S, MODE>(J, k, vb % tx, vb / tx);
   }
 }
 

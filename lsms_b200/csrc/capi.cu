@@ -70,6 +70,8 @@ struct b200tau_ctx {
   int jobs_cap = 0;
   JobDev *d_jobs2 = nullptr;  // the jobs still refining after compaction (at most `slots`)
   int jobs2_cap = 0;
+  JobDev *d_jobs3 = nullptr;  // their FP64 re-solve records
+  int jobs3_cap = 0;
   int *d_info = nullptr;   // 2 x slots: the wave's jobs, then the compacted list
   int *d_conv = nullptr;   // per slot: refinement converged
   double *d_cnorm = nullptr;  // per slot: relative size of the last refinement correction
@@ -302,15 +304,15 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
 // 3-D float tensor (128 floats per row, `rows` rows per slot, `slots` slots) read in
-// 32 x box_rows boxes with 128-byte swizzle; out-of-range rows read as zero.
+// kTcChunk x box_rows boxes with 64-byte swizzle; out-of-range rows read as zero.
 int encode_pack_map(b200tau_ctx *ctx, EncodeTiledFn enc, CUtensorMap *map, float *base, int rows, int slots,
                     int box_rows) {
   const cuuint64_t dims[3] = {128, (cuuint64_t)rows, (cuuint64_t)slots};
   const cuuint64_t strides[2] = {128 * sizeof(float), (cuuint64_t)rows * 128 * sizeof(float)};
-  const cuuint32_t box[3] = {32, (cuuint32_t)box_rows, 1};
+  const cuuint32_t box[3] = {(cuuint32_t)kTcChunk, (cuuint32_t)box_rows, 1};
   const cuuint32_t estr[3] = {1, 1, 1};
   const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, estr,
-                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(ctx, B200TAU_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
   return B200TAU_OK;
@@ -450,7 +452,10 @@ int run_refinement(b200tau_ctx *ctx, const std::vector<JobDev> &h, int nw, int m
           cmaxn = std::max(cmaxn, h[w].n);
           cmaxN = std::max(cmaxN, h[w].N);
         }
-      if (keep.empty()) break;
+      if (keep.empty()) {  // every job converged: nothing left to refine or to re-solve
+        ncur = 0;
+        break;
+      }
       if ((int)keep.size() < nw) {
         int rc = ensure_jobs2(ctx, ctx->slots);
         if (rc) return rc;
@@ -465,22 +470,29 @@ int run_refinement(b200tau_ctx *ctx, const std::vector<JobDev> &h, int nw, int m
                            fp32_sweep));
   }
   CK(launch_refine_end(ctx->d_jobs, nw, ns, kkrsz, ctx->stream, &ctx->launches));
-  if (p.fk != kFactorFP32 || !ctx->fallback_on) return B200TAU_OK;
+  if (p.fk != kFactorFP32 || !ctx->fallback_on || ncur == 0) return B200TAU_OK;
   // Jobs whose FP32-factor refinement did not converge (condition numbers beyond what FP32 block
   // factors can refine, e.g. energies next to the real axis) take the FP64 path instead: an FP64
   // copy of the unmodified M, FP64 block elimination, the FP64 refinement rounds, tau00 from X -
   // the same kernels and arithmetic as a PREC_FP64 solve of the job.  The selection happens on the
   // device (converged jobs become inactive records), so the host never waits inside a wave.
+  // (only the jobs still refining after the compaction can need it)
   const int ld = h[0].ld;
   int rc = ensure_fallback(ctx, ld);
   if (rc || (rc = ensure_jobs2(ctx, ctx->slots))) return rc;
+  if (ctx->jobs3_cap < ctx->slots) {
+    cudaFree(ctx->d_jobs3);
+    ctx->d_jobs3 = nullptr;
+    CK(cudaMalloc(&ctx->d_jobs3, sizeof(JobDev) * ctx->slots));
+    ctx->jobs3_cap = ctx->slots;
+  }
   int *finfo = ctx->d_info + ctx->slots;
-  CK(launch_fallback_prepare(ctx->d_jobs, ctx->d_jobs2, nw, ctx->d_ffb, (size_t)ld * ld, maxN, ctx->d_fbcount,
+  CK(launch_fallback_prepare(cur, ctx->d_jobs3, ncur, ctx->d_ffb, (size_t)ld * ld, cmaxN, ctx->d_fbcount,
                              ctx->stream, &ctx->launches));
-  CK(launch_eliminate(kFactorFP64, ctx->d_jobs2, nw, maxn, maxN, finfo, ctx->stream, &ctx->launches, nullptr,
+  CK(launch_eliminate(kFactorFP64, ctx->d_jobs3, ncur, cmaxn, cmaxN, finfo, ctx->stream, &ctx->launches, nullptr,
                       nullptr, ctx->d_err, true));
-  CK(launch_solve_refine(kFactorFP64, ctx->d_jobs2, nw, maxn, maxN, b, std::max(1, ctx->refine_steps[0]), ns, kkrsz,
-                         finfo, ctx->stream, &ctx->launches));
+  CK(launch_solve_refine(kFactorFP64, ctx->d_jobs3, ncur, cmaxn, cmaxN, b, std::max(1, ctx->refine_steps[0]), ns,
+                         kkrsz, finfo, ctx->stream, &ctx->launches));
   return B200TAU_OK;
 }
 
@@ -712,6 +724,7 @@ void b200tau_destroy(b200tau_ctx *ctx) {
   cudaFree(ctx->d_vec);
   cudaFree(ctx->d_jobs);
   cudaFree(ctx->d_jobs2);
+  cudaFree(ctx->d_jobs3);
   cudaFree(ctx->d_info);
   cudaFree(ctx->d_conv);
   cudaFree(ctx->d_cnorm);

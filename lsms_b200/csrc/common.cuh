@@ -125,7 +125,10 @@ struct TcMaps {
   float *a_hi = nullptr, *a_lo = nullptr, *b_hi = nullptr, *b_lo = nullptr;
   size_t a_slot = 0, b_slot = 0;  // floats per slot
 };
+// K floats per TMA box of the operand packs (64-byte rows, 64-byte swizzle)
+constexpr int kTcChunk = 16;
 size_t tc_smem_bytes();
+int tc_num_sms();
 cudaError_t tc_prepare();
 // Pack + tensor-core update A22 -= A21 W for step k of every job in the wave (FP32 factors).
 cudaError_t launch_tc_step(const TcMaps &maps, const JobDev *jobs, int njobs, int k, int max_N, int *err,

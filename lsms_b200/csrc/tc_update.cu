@@ -35,13 +35,15 @@ namespace {
 
 constexpr int kTM = 128;          // real rows per tile (64 complex rows)
 constexpr int kTN = 256;          // columns per tile
-constexpr int kTK = 32;           // floats per K chunk (128 bytes: one swizzle span)
+constexpr int kTK = kTcChunk;     // floats per K chunk (64 bytes: one 64-byte swizzle span)
 constexpr int kKReal = 2 * kNb;   // 128 real K per step
 constexpr int kChunks = kKReal / kTK;
-constexpr int kStages = 2;
-constexpr int kABytes = kTM * kTK * 4;  // 16 KB
-constexpr int kBBytes = kTN * kTK * 4;  // 32 KB
+constexpr int kStages = 3;
+constexpr int kABytes = kTM * kTK * 4;  // 8 KB
+constexpr int kBBytes = kTN * kTK * 4;  // 16 KB
 constexpr int kStageBytes = 2 * kABytes + 2 * kBBytes;
+constexpr int kPieceCols = 64;          // epilogue: columns per TMA reduce-add
+constexpr int kAccCols = kTN;           // TMEM columns per accumulator (two of them)
 constexpr long kWaitBound = 1L << 22;
 
 struct __align__(1024) TcSmem {
@@ -49,11 +51,15 @@ struct __align__(1024) TcSmem {
   float a_lo[kStages][kTM * kTK];
   float b_hi[kStages][kTN * kTK];
   float b_lo[kStages][kTN * kTK];
+  float ep[2][kPieceCols * kTM];  // epilogue staging, [column][128 real rows]
   unsigned long long full[kStages];
   unsigned long long empty[kStages];
-  unsigned long long accum;
+  unsigned long long acc_full[2];
+  unsigned long long acc_empty[2];
+  unsigned long long drain;
   unsigned tmem_base;
-  int abort;
+  volatile int abort;
+  volatile int ep_ok;  // the epilogue issuer's last accumulator wait succeeded
 };
 
 __device__ __forceinline__ unsigned su32(const void *p) { return static_cast<unsigned>(__cvta_generic_to_shared(p)); }
@@ -89,16 +95,16 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, i
       : "memory");
 }
 
-// K-major, 128-byte-swizzled operand: rows 128 B apart, 8-row groups 1024 B apart (SBO),
-// LBO unused (1), descriptor version 1 (sm_100), layout type 2 = SWIZZLE_128B.
+// K-major, 64-byte-swizzled operand: rows 64 B apart, 8-row groups 512 B apart (SBO),
+// LBO unused (1), descriptor version 1 (sm_100), layout type 4 = SWIZZLE_64B.
 __device__ __forceinline__ uint64_t smem_desc(const void *p) {
   const uint64_t addr = su32(p);
   uint64_t d = 0;
   d |= (addr >> 4) & 0x3FFFull;
   d |= (uint64_t)1 << 16;              // LBO (ignored for swizzled K-major)
-  d |= (uint64_t)(1024 >> 4) << 32;    // SBO
+  d |= (uint64_t)(512 >> 4) << 32;     // SBO
   d |= (uint64_t)1 << 46;              // version
-  d |= (uint64_t)2 << 61;              // SWIZZLE_128B
+  d |= (uint64_t)4 << 61;              // SWIZZLE_64B
   return d;
 }
 
@@ -124,20 +130,43 @@ __device__ __forceinline__ float tf32_hi(float x) {
   return __uint_as_float(r);
 }
 
+// Tiles of one launch: t = ((z * tiles_m) + tm) * tiles_n + tn (tn fastest, so consecutive CTAs
+// share the A row block), sized for the largest trailing block of the wave; tiles outside a job's
+// own trailing block are skipped identically by every role.
+struct TileSpace {
+  int tiles_m, tiles_n, total;
+};
+__device__ __forceinline__ bool tile_of(const JobDev *jobs, const TileSpace &ts, int k, int t, int &z, int &row0,
+                                        int &col0, int &kb) {
+  z = t / (ts.tiles_m * ts.tiles_n);
+  const int rem = t - z * ts.tiles_m * ts.tiles_n;
+  const int tm = rem / ts.tiles_n, tn = rem - tm * ts.tiles_n;
+  const JobDev &J = jobs[z];
+  if (k >= J.n) return false;
+  kb = min(kNb, J.n - k);
+  const int rest = J.N - k - kb;
+  row0 = tm * kTM;
+  col0 = tn * kTN;
+  return row0 < 2 * rest && col0 < rest;
+}
+
+__device__ __forceinline__ void mbar_arrive(unsigned long long *b) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(su32(b)) : "memory");
+}
+
+// Persistent: one CTA per SM loops over the launch's tiles.  Warp 0 (one thread) streams the
+// operand chunks through a 3-stage ring; warp 1 owns TMEM (2 x 256 columns) and issues the MMAs
+// of tile i into accumulator i % 2; warps 2..5 drain the other accumulator meanwhile (tcgen05.ld ->
+// negated -> shared-memory staging -> TMA reduce-add onto F), so one tile's epilogue overlaps
+// the next tile's MMAs.
 __global__ void __launch_bounds__(192, 1)
     tc_update_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_constant__ CUtensorMap tA_lo,
                      const __grid_constant__ CUtensorMap tB_hi, const __grid_constant__ CUtensorMap tB_lo,
-                     const __grid_constant__ CUtensorMap tF, const JobDev *__restrict__ jobs, int k, int *err) {
+                     const __grid_constant__ CUtensorMap tF, const JobDev *__restrict__ jobs, int k, TileSpace ts,
+                     int *err) {
   extern __shared__ __align__(1024) unsigned char tc_raw[];
   // the dynamic window is 1024-aligned by the launch (extra 1 KB requested)
   TcSmem &sm = *reinterpret_cast<TcSmem *>((reinterpret_cast<uintptr_t>(tc_raw) + 1023) & ~uintptr_t(1023));
-  const JobDev &J = jobs[blockIdx.z];
-  if (k >= J.n) return;
-  const int kb = min(kNb, J.n - k);
-  const int rest = J.N - k - kb;  // complex rows / columns of the trailing block
-  const int row0 = blockIdx.y * kTM;  // real rows
-  const int col0 = blockIdx.x * kTN;
-  if (row0 >= 2 * rest || col0 >= rest) return;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
   if (threadIdx.x == 0) {
@@ -145,14 +174,18 @@ __global__ void __launch_bounds__(192, 1)
       mbar_init(&sm.full[s], 1);
       mbar_init(&sm.empty[s], 1);
     }
-    mbar_init(&sm.accum, 1);
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(&sm.acc_full[a], 1);
+      mbar_init(&sm.acc_empty[a], 4);  // one arrival per epilogue warp
+    }
+    mbar_init(&sm.drain, 1);
     sm.abort = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
   }
   if (warp == 1) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(su32(&sm.tmem_base)),
-                 "r"(kTN)
+                 "r"(2 * kAccCols)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
@@ -160,101 +193,152 @@ __global__ void __launch_bounds__(192, 1)
   __syncthreads();
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const uint32_t tmem = sm.tmem_base;
-  const int zslot = blockIdx.z;
 
   if (warp == 0) {
     if (lane == 0) {
-      // producer: chunk c of K into stage c % 2
-      for (int c = 0; c < kChunks; ++c) {
-        const int s = c % kStages;
-        if (c >= kStages && !mbar_wait(&sm.empty[s], ((c / kStages) - 1) & 1)) {
-          atomicExch(err, 2);
-          sm.abort = 1;
-          break;
+      long g = 0;  // chunks issued
+      for (int t = blockIdx.x; t < ts.total && !sm.abort; t += gridDim.x) {
+        int z, row0, col0, kb;
+        if (!tile_of(jobs, ts, k, t, z, row0, col0, kb)) continue;
+        for (int c = 0; c < kChunks; ++c, ++g) {
+          const int s = (int)(g % kStages);
+          if (g >= kStages && !mbar_wait(&sm.empty[s], (unsigned)(((g / kStages) - 1) & 1))) {
+            atomicExch(err, 2);
+            sm.abort = 1;
+            break;
+          }
+          mbar_expect_tx(&sm.full[s], kStageBytes);
+          tma_load_3d(sm.a_hi[s], &tA_hi, c * kTK, row0, z, &sm.full[s]);
+          tma_load_3d(sm.a_lo[s], &tA_lo, c * kTK, row0, z, &sm.full[s]);
+          tma_load_3d(sm.b_hi[s], &tB_hi, c * kTK, col0, z, &sm.full[s]);
+          tma_load_3d(sm.b_lo[s], &tB_lo, c * kTK, col0, z, &sm.full[s]);
         }
-        mbar_expect_tx(&sm.full[s], kStageBytes);
-        tma_load_3d(sm.a_hi[s], &tA_hi, c * kTK, row0, zslot, &sm.full[s]);
-        tma_load_3d(sm.a_lo[s], &tA_lo, c * kTK, row0, zslot, &sm.full[s]);
-        tma_load_3d(sm.b_hi[s], &tB_hi, c * kTK, col0, zslot, &sm.full[s]);
-        tma_load_3d(sm.b_lo[s], &tB_lo, c * kTK, col0, zslot, &sm.full[s]);
       }
+      // every issued load has landed before the CTA can exit (bounded; normally already true)
+      for (long q = g > kStages ? g - kStages : 0; q < g; ++q)
+        mbar_wait(&sm.full[q % kStages], (unsigned)((q / kStages) & 1));
     }
   } else if (warp == 1) {
     if (lane == 0) {
-      bool ok = true;
-      for (int c = 0; c < kChunks && ok; ++c) {
-        const int s = c % kStages;
-        if (!mbar_wait(&sm.full[s], (c / kStages) & 1)) {
-          atomicExch(err, 3);
-          ok = false;
+      long g = 0;
+      int li = 0;
+      for (int t = blockIdx.x; t < ts.total && !sm.abort; t += gridDim.x) {
+        int z, row0, col0, kb;
+        if (!tile_of(jobs, ts, k, t, z, row0, col0, kb)) continue;
+        const int a = li & 1;
+        if (li >= 2 && !mbar_wait(&sm.acc_empty[a], (unsigned)(((li >> 1) - 1) & 1))) {
+          atomicExch(err, 5);
+          sm.abort = 1;
           break;
         }
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint64_t dah = smem_desc(sm.a_hi[s]), dal = smem_desc(sm.a_lo[s]);
-        const uint64_t dbh = smem_desc(sm.b_hi[s]), dbl = smem_desc(sm.b_lo[s]);
+        const uint32_t d = tmem + (uint32_t)(a * kAccCols);
+        bool ok = true;
+        for (int c = 0; c < kChunks; ++c, ++g) {
+          const int s = (int)(g % kStages);
+          if (!mbar_wait(&sm.full[s], (unsigned)((g / kStages) & 1))) {
+            atomicExch(err, 3);
+            sm.abort = 1;
+            ok = false;
+            break;
+          }
+          asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+          const uint64_t dah = smem_desc(sm.a_hi[s]), dal = smem_desc(sm.a_lo[s]);
+          const uint64_t dbh = smem_desc(sm.b_hi[s]), dbl = smem_desc(sm.b_lo[s]);
 #pragma unroll
-        for (int kk = 0; kk < kTK / 8; ++kk) {
-          const uint64_t off = (uint64_t)((kk * 32) >> 4);  // 8 tf32 = 32 bytes along K
-          const uint32_t acc0 = (c > 0 || kk > 0) ? 1u : 0u;
-          umma_tf32(tmem, dal + off, dbh + off, acc0);
-          umma_tf32(tmem, dah + off, dbl + off, 1u);
-          umma_tf32(tmem, dah + off, dbh + off, 1u);
+          for (int kk = 0; kk < kTK / 8; ++kk) {
+            const uint64_t off = (uint64_t)((kk * 32) >> 4);  // 8 tf32 = 32 bytes along K
+            const uint32_t acc0 = (c > 0 || kk > 0) ? 1u : 0u;
+            umma_tf32(d, dal + off, dbh + off, acc0);
+            umma_tf32(d, dah + off, dbl + off, 1u);
+            umma_tf32(d, dah + off, dbh + off, 1u);
+          }
+          umma_commit(&sm.empty[s]);
         }
-        umma_commit(&sm.empty[s]);
+        if (!ok) break;
+        umma_commit(&sm.acc_full[a]);
+        ++li;
       }
-      umma_commit(&sm.accum);
+      // the MMAs issued are complete before TMEM is released (bounded)
+      umma_commit(&sm.drain);
+      mbar_wait(&sm.drain, 0);
     }
   } else {
-    // Epilogue, warps 2..5 -> TMEM lane quarter (warp % 4).  The accumulator is negated into the
-    // (now idle) operand ring as column-major [column][128 real rows] pieces of 64 columns, and
-    // each piece is added onto F by one TMA reduce-add (cp.reduce.async.bulk.tensor .add.f32): the
-    // read-modify-write of the C tile happens in L2, asynchronously to the SM.  Rows/columns of the
-    // tile beyond the trailing block land in F's padding (rows/columns N..ld-1, never read) or are
-    // clipped at the tensor bounds.
+    // Epilogue, warps 2..5 -> TMEM lane quarter (warp % 4), 32 real rows each.  Each 64-column
+    // piece of the accumulator is negated into a staging buffer (two, alternating) and added onto
+    // F by one TMA reduce-add (cp.reduce.async.bulk.tensor .add.f32): the read-modify-write of the
+    // C tile happens in L2, asynchronously to the SM.  Rows/columns of a tile beyond the trailing
+    // block land in F's padding (rows/columns N..ld-1, never read) or are clipped at the tensor
+    // bounds.
     const int q = warp & 3;
-    const bool ok = mbar_wait(&sm.accum, 0);
-    if (!ok) atomicExch(err, 4);
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    float *stage = &sm.a_hi[0][0];  // 192 KB ring, 4 pieces x 32 KB used
-    const int rl = q * 32 + lane;   // real row within the tile
+    const int rl = q * 32 + lane;  // real row within the tile
     const bool issuer = (warp == 2 && lane == 0);
-    const int fx = 2 * (k + kb) + row0;  // float row coordinate in F (multiple of 4)
-    const int fy = k + kb + col0;        // column coordinate in F
-    for (int piece = 0; piece < kTN / 64; ++piece) {
-      float *ps = stage + piece * 64 * kTM;
-#pragma unroll
-      for (int c16 = 0; c16 < 64; c16 += 16) {
-        uint32_t v[16];
-        const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(piece * 64 + c16);
-        asm volatile(
-            "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-            : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
-              "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
-              "=r"(v[15])
-            : "r"(taddr)
-            : "memory");
-        asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-        for (int j = 0; j < 16; ++j) ps[(c16 + j) * kTM + rl] = ok ? -__uint_as_float(v[j]) : 0.0f;
-      }
-      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-      asm volatile("bar.sync 1, 128;" ::: "memory");
+    int li = 0, pcount = 0;
+    // The four warps must take the same path through the named barriers below, so the loop runs
+    // over the same tiles for all of them and the one wait is taken by the issuer, whose outcome
+    // the others read after a barrier.
+    for (int t = blockIdx.x; t < ts.total; t += gridDim.x) {
+      int z, row0, col0, kb;
+      if (!tile_of(jobs, ts, k, t, z, row0, col0, kb)) continue;
+      const int a = li & 1;
       if (issuer) {
-        asm volatile(
-            "cp.reduce.async.bulk.tensor.3d.global.shared::cta.add.tile.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(
-                &tF),
-            "r"(fx), "r"(fy + piece * 64), "r"(zslot), "r"(su32(ps))
-            : "memory");
-        asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+        const bool ok = mbar_wait(&sm.acc_full[a], (unsigned)((li >> 1) & 1));
+        sm.ep_ok = ok ? 1 : 0;
+        if (!ok) {
+          atomicExch(err, 4);
+          sm.abort = 1;
+        }
       }
+      asm volatile("bar.sync 1, 128;" ::: "memory");
+      if (!sm.ep_ok) break;
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      const int fx = 2 * (k + kb) + row0;  // float row coordinate in F (multiple of 4)
+      const int fy = k + kb + col0;        // column coordinate in F
+      for (int piece = 0; piece < kTN / kPieceCols; ++piece, ++pcount) {
+        float *ps = sm.ep[pcount & 1];
+        if (issuer) asm volatile("cp.async.bulk.wait_group.read 1;" ::: "memory");  // ps is free again
+        asm volatile("bar.sync 1, 128;" ::: "memory");
+#pragma unroll
+        for (int c16 = 0; c16 < kPieceCols; c16 += 16) {
+          uint32_t v[16];
+          const uint32_t taddr =
+              tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(a * kAccCols + piece * kPieceCols + c16);
+          asm volatile(
+              "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+              "[%16];"
+              : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                "=r"(v[15])
+              : "r"(taddr)
+              : "memory");
+          asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+          for (int j = 0; j < 16; ++j) ps[(c16 + j) * kTM + rl] = -__uint_as_float(v[j]);
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        asm volatile("bar.sync 1, 128;" ::: "memory");
+        if (issuer) {
+          asm volatile(
+              "cp.reduce.async.bulk.tensor.3d.global.shared::cta.add.tile.bulk_group [%0, {%1, %2, %3}], [%4];" ::"l"(
+                  &tF),
+              "r"(fx), "r"(fy + piece * kPieceCols), "r"(z), "r"(su32(ps))
+              : "memory");
+          asm volatile("cp.async.bulk.commit_group;" ::: "memory");
+        }
+      }
+      // this accumulator has been read out: the MMA warp may reuse it
+      asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(&sm.acc_empty[a]);
+      ++li;
     }
-    if (issuer) asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory");
+    if (issuer) asm volatile("cp.async.bulk.wait_group 0;" ::: "memory");
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
   if (warp == 1) {
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTN) : "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * kAccCols) : "memory");
   }
 }
 
@@ -305,6 +389,18 @@ __global__ void __launch_bounds__(256) tc_pack_kernel(const JobDev *__restrict__
 
 size_t tc_smem_bytes() { return sizeof(TcSmem) + 1024; }
 
+int tc_num_sms() {
+  static int n = 0;
+  if (n == 0) {
+    int dev = 0, v = 0;
+    n = (cudaGetDevice(&dev) == cudaSuccess &&
+         cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && v > 0)
+            ? v
+            : 148;
+  }
+  return n;
+}
+
 cudaError_t launch_tc_step(const TcMaps &maps, const JobDev *jobs, int njobs, int k, int max_N, int *err,
                            cudaStream_t s) {
   const int rest = max_N - k - 1;  // upper bound of the trailing size over the wave
@@ -312,9 +408,13 @@ cudaError_t launch_tc_step(const TcMaps &maps, const JobDev *jobs, int njobs, in
   const int nA = (rest + 3) / 4, nB = (rest + 3) / 4;
   tc_pack_kernel<<<dim3(nA + nB, njobs), 256, 0, s>>>(jobs, k, nA, maps.a_hi, maps.a_lo, maps.b_hi, maps.b_lo,
                                                       maps.a_slot, maps.b_slot);
-  const dim3 grid((rest + kTN - 1) / kTN, (2 * rest + kTM - 1) / kTM, njobs);
-  tc_update_kernel<<<grid, 192, tc_smem_bytes(), s>>>(maps.tA_hi, maps.tA_lo, maps.tB_hi, maps.tB_lo, maps.tF,
-                                                      jobs, k, err);
+  TileSpace ts;
+  ts.tiles_n = (rest + kTN - 1) / kTN;
+  ts.tiles_m = (2 * rest + kTM - 1) / kTM;
+  ts.total = ts.tiles_m * ts.tiles_n * njobs;
+  const int grid = ts.total < tc_num_sms() ? ts.total : tc_num_sms();
+  tc_update_kernel<<<grid, 192, tc_smem_bytes(), s>>>(maps.tA_hi, maps.tA_lo, maps.tB_hi, maps.tB_lo, maps.tF, jobs,
+                                                      k, ts, err);
   return cudaGetLastError();
 }
 
