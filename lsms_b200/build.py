@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "_lib")
 LIB_PATH = os.path.join(LIB_DIR, "libb200tau.so")
-SOURCES = ["capi.cu", "kkr_build.cu", "block_lu.cu", "tc_update.cu", "sweep.cu", "adjoint.cu", "noalloc.cu", "angular.cpp"]
+SOURCES = ["capi.cu", "kkr_build.cu", "block_lu.cu", "tc_update.cu", "sweep.cu", "sweep_flow.cu", "adjoint.cu", "noalloc.cu", "angular.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -28,6 +28,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(LIB_DIR, exist_ok=True)
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
     deps = srcs + [os.path.join(CSRC, "common.cuh"), os.path.join(CSRC, "cplx.cuh"), os.path.join(CSRC, "gj.cuh"),
+                   os.path.join(CSRC, "cluster.cuh"),
                    os.path.join(HERE, "..", "include", "b200tau.h")]
     if (not force and os.path.exists(LIB_PATH)
             and all(os.path.getmtime(LIB_PATH) >= os.path.getmtime(d) for d in deps)):

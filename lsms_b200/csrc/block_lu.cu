@@ -568,17 +568,17 @@ cudaError_t eliminate_impl(const JobDev *jobs, int njobs, int max_n, int max_N, 
 }
 
 template <typename T>
-cudaError_t sweep_solve(const JobDev *jobs, int njobs, int b, int mode, int *info, cudaStream_t s,
+cudaError_t sweep_solve(const JobDev *jobs, int njobs, int b, int max_N, int mode, int *info, cudaStream_t s,
                         long *launches, bool fp32) {
   const FactorKind fk = sizeof(T) == sizeof(double2) ? kFactorFP64 : kFactorFP32;
   cudaError_t e;
   // forward (skipped for the initial solve: B is zero above the central block)
   if (mode == 1) {
-    if ((e = launch_sweep(fk, jobs, njobs, b, true, mode, fp32, s)) != cudaSuccess) return e;
+    if ((e = launch_sweep(fk, jobs, njobs, b, max_N, true, mode, fp32, s)) != cudaSuccess) return e;
     if (launches) *launches += 1;
   }
   schur_solve_kernel<T><<<njobs, 256, 0, s>>>(jobs, mode, info);
-  if ((e = launch_sweep(fk, jobs, njobs, b, false, mode, fp32, s)) != cudaSuccess) return e;
+  if ((e = launch_sweep(fk, jobs, njobs, b, max_N, false, mode, fp32, s)) != cudaSuccess) return e;
   if (launches) *launches += 2;
   return cudaSuccess;
 }
@@ -704,9 +704,8 @@ cudaError_t launch_finalize_direct(FactorKind fk, const JobDev *jobs, int njobs,
 cudaError_t launch_refine_begin(FactorKind fk, const JobDev *jobs, int njobs, int max_n, int max_N, int b,
                                 int *info, cudaStream_t s, long *launches, bool fp32_sweep) {
   (void)max_n;
-  (void)max_N;
-  const cudaError_t e = fk == kFactorFP64 ? sweep_solve<double2>(jobs, njobs, b, 0, info, s, launches, false)
-                                           : sweep_solve<float2>(jobs, njobs, b, 0, info, s, launches, fp32_sweep);
+  const cudaError_t e = fk == kFactorFP64 ? sweep_solve<double2>(jobs, njobs, b, max_N, 0, info, s, launches, false)
+                                           : sweep_solve<float2>(jobs, njobs, b, max_N, 0, info, s, launches, fp32_sweep);
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 
@@ -728,8 +727,8 @@ cudaError_t launch_refine_round(FactorKind fk, const JobDev *jobs, int njobs, in
     residual_kernel<32><<<dim3((max_N + residual_rows<32>() - 1) / residual_rows<32>(), njobs), 256, sm32, s>>>(jobs);
   }
   if (launches) *launches += 1;
-  const cudaError_t e = fk == kFactorFP64 ? sweep_solve<double2>(jobs, njobs, b, 1, info, s, launches, false)
-                                           : sweep_solve<float2>(jobs, njobs, b, 1, info, s, launches, fp32_sweep);
+  const cudaError_t e = fk == kFactorFP64 ? sweep_solve<double2>(jobs, njobs, b, max_N, 1, info, s, launches, false)
+                                           : sweep_solve<float2>(jobs, njobs, b, max_N, 1, info, s, launches, fp32_sweep);
   if (e != cudaSuccess) return e;
   if (check) {
     converge_check_kernel<<<njobs, 256, 0, s>>>(jobs, kRefineTol);

@@ -171,9 +171,16 @@ cudaError_t launch_refine_round(FactorKind fk, const JobDev *jobs, int njobs, in
 cudaError_t launch_refine_end(const JobDev *jobs, int njobs, int ns, int kkrsz, cudaStream_t s, long *launches);
 // One block sweep of the correction solve for all jobs, one thread-block cluster per job
 // (sweep.cu): forward (R -> Y over the D_k, A21_k factors) or backward (Y over the W_k factors,
-// X (+)= Y).  `fp32_arith` selects FP32 arithmetic on FP32 factors.
-cudaError_t launch_sweep(FactorKind fk, const JobDev *jobs, int njobs, int b, bool forward, int mode,
+// X (+)= Y).  `fp32_arith` selects FP32 arithmetic on FP32 factors.  max_N bounds the jobs' N.
+cudaError_t launch_sweep(FactorKind fk, const JobDev *jobs, int njobs, int b, int max_N, bool forward, int mode,
                          bool fp32_arith, cudaStream_t s);
+// Cluster size of the sweeps for a wave of njobs (sweep.cu).
+int sweep_cluster_size(int njobs);
+// The dataflow sweeps for FP32 factors in FP32 arithmetic with b <= 16 (sweep_flow.cu).  Sets
+// *launched when it took the launch; false (and cudaSuccess) when the shape does not fit its
+// shared-memory layout, and the caller runs launch_sweep's step-synchronous kernels instead.
+cudaError_t launch_flow_sweep(const JobDev *jobs, int njobs, int b, int max_N, bool forward, int mode,
+                              cudaStream_t s, bool *launched);
 // Adjoint (adjoint.cu), FP64 factors: V = M^-1 from the block factors in F, then per LIZ site the
 // tau00 cotangent pull-back and d ln det M / d t (needs G in M, X refined, V).
 cudaError_t launch_inverse(const JobDev *jobs, int njobs, int max_n, int max_N, cudaStream_t s, long *launches);

@@ -21,55 +21,17 @@
 #include <cuda_runtime.h>
 
 #include "common.cuh"
+#include "cluster.cuh"
 #include "cplx.cuh"
 
 namespace b200 {
 namespace {
 
 using namespace cx;
+using namespace cl;
 
 constexpr int kUnitCols = 32;  // operand columns per pipeline unit
 constexpr int kMaxCluster = 8;
-
-__device__ __forceinline__ int cluster_rank() {
-  unsigned r;
-  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
-  return (int)r;
-}
-__device__ __forceinline__ int cluster_size() {
-  unsigned r;
-  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
-  return (int)r;
-}
-// Every thread of every CTA of the cluster; orders the global writes made before it.
-__device__ __forceinline__ void cluster_sync() {
-  asm volatile(
-      "barrier.cluster.arrive.release.aligned;\n\t"
-      "barrier.cluster.wait.acquire.aligned;" ::
-          : "memory");
-}
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
-  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
-// Copies the 64 x ncol block of F at (row0, col0) into shared memory, column-major with 64 rows
-// per column (dst[c * 64 + r]).  The rows past N up to the leading dimension are inside the
-// allocation (ld >= N rounded up to 64) and are never used by the arithmetic.
-template <typename T>
-__device__ __forceinline__ void stage_block(T *dst, const T *F, int ld, int row0, int col0, int ncol) {
-  constexpr int kPer = 16 / (int)sizeof(T);  // elements per 16-byte copy
-  constexpr int kCpc = 64 / kPer;            // copies per column
-  for (int e = threadIdx.x; e < ncol * kCpc; e += blockDim.x) {
-    const int c = e / kCpc, part = e - c * kCpc;
-    cp_async16(dst + c * 64 + part * kPer, F + (size_t)row0 + part * kPer + (size_t)(col0 + c) * ld);
-  }
-}
 
 // Shared-memory layout of the sweep kernels.
 // T: factor storage type; V: arithmetic type of the sweep (double2, or float2 for a correction
@@ -376,44 +338,9 @@ __global__ void __launch_bounds__(256) backward_sweep_kernel(const JobDev *__res
   cp_async_wait<0>();
 }
 
-int g_num_sms = 0;
-
-// Cluster size for a wave of njobs: the largest power of two up to 8 with cs * njobs CTAs
-// resident at once (one CTA per SM at these shared-memory sizes).
-int pick_cluster(int njobs) {
-  if (g_num_sms == 0) {
-    int dev = 0, v = 0;
-    if (cudaGetDevice(&dev) == cudaSuccess &&
-        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) == cudaSuccess && v > 0)
-      g_num_sms = v;
-    else
-      g_num_sms = 148;
-  }
-  int cs = kMaxCluster;
-  while (cs > 1 && cs * njobs > g_num_sms) cs >>= 1;
-  return cs;
-}
-
-template <typename Kern, typename... Args>
-cudaError_t launch_cluster(Kern kern, int cs, int njobs, int smem, cudaStream_t s, Args... args) {
-  cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(cs, njobs, 1);
-  cfg.blockDim = dim3(256, 1, 1);
-  cfg.dynamicSmemBytes = smem;
-  cfg.stream = s;
-  cudaLaunchAttribute attr[1];
-  attr[0].id = cudaLaunchAttributeClusterDimension;
-  attr[0].val.clusterDim.x = cs;
-  attr[0].val.clusterDim.y = 1;
-  attr[0].val.clusterDim.z = 1;
-  cfg.attrs = attr;
-  cfg.numAttrs = 1;
-  return cudaLaunchKernelEx(&cfg, kern, args...);
-}
-
 template <typename T, typename V, int BC>
 cudaError_t sweep_impl(const JobDev *jobs, int njobs, bool forward, int mode, cudaStream_t s) {
-  const int cs = pick_cluster(njobs);
+  const int cs = sweep_cluster_size(njobs);
   cudaError_t e;
   if (forward) {
     const int smem = SweepSmem<T, V>::kForward;
@@ -437,12 +364,25 @@ cudaError_t sweep_b(const JobDev *jobs, int njobs, int b, bool forward, int mode
 
 }  // namespace
 
-cudaError_t launch_sweep(FactorKind fk, const JobDev *jobs, int njobs, int b, bool forward, int mode,
+// The largest power of two up to 8 with cs * njobs CTAs resident at once (one CTA per SM at
+// the sweeps' shared-memory sizes), so that one wave of jobs fills the GPU once.
+int sweep_cluster_size(int njobs) {
+  int cs = kMaxCluster;
+  while (cs > 1 && cs * njobs > tc_num_sms()) cs >>= 1;
+  return cs;
+}
+
+cudaError_t launch_sweep(FactorKind fk, const JobDev *jobs, int njobs, int b, int max_N, bool forward, int mode,
                          bool fp32_arith, cudaStream_t s) {
   if (njobs <= 0) return cudaSuccess;
   if (b < 1 || b > kMaxB || (forward && mode != 1)) return cudaErrorInvalidValue;
   if (fk == kFactorFP64) return sweep_b<double2, double2>(jobs, njobs, b, forward, mode, s);
-  if (fp32_arith) return sweep_b<float2, float2>(jobs, njobs, b, forward, mode, s);
+  if (fp32_arith) {
+    bool done = false;
+    const cudaError_t e = launch_flow_sweep(jobs, njobs, b, max_N, forward, mode, s, &done);
+    if (e != cudaSuccess || done) return e;
+    return sweep_b<float2, float2>(jobs, njobs, b, forward, mode, s);
+  }
   return sweep_b<float2, double2>(jobs, njobs, b, forward, mode, s);
 }
 
