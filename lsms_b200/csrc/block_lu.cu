@@ -84,16 +84,19 @@ __global__ void __launch_bounds__(kDiagThreads) diag_inverse_kernel(const JobDev
   }
   unsigned long long used = 0;  // rows already pivoted on (the same in every thread)
   bool singular = false;
+  if (tid < NB) s_inv[tid] = tid;  // every entry in range whatever the pivots
   for (int p = 0; p < kb; ++p) {
     const int par = p & 1;
     if (c == p) {  // this row group's candidate, and the multipliers
+      // the first unused row is the candidate until a larger one is seen, so that a NaN column
+      // still yields an unused row in range (NaN compares false)
       double best = -1.0;
       int bi = NB;
 #pragma unroll
       for (int q = 0; q < kRq; ++q) {
         const int r = g + kRg * q;
         const double v = cabs1(a[q]);
-        if (r < kb && !((used >> r) & 1ull) && v > best) {
+        if (r < kb && !((used >> r) & 1ull) && (bi == NB || v > best)) {
           best = v;
           bi = r;
         }
@@ -109,11 +112,13 @@ __global__ void __launch_bounds__(kDiagThreads) diag_inverse_kernel(const JobDev
     for (int i = 1; i < kRg; ++i) {
       const double v = s_cval[par][i];
       const int ix = s_cidx[par][i];
-      if (v > best || (v == best && ix < pv)) {
+      if (ix != NB && (pv == NB || v > best || (v == best && ix < pv))) {
         best = v;
         pv = ix;
       }
     }
+    // kb - p unused rows remain, so some group has one: pv < kb
+    pv = min(pv, kb - 1);
     used |= 1ull << pv;
     const double2 d = s_f[par][pv];
     double2 dinv = make_double2(0.0, 0.0);

@@ -18,10 +18,9 @@
 //  * Operand panels (A21, D or W; 64 rows x 32 columns per unit) stream through a cp.async ring
 //    several units ahead.  The D_(j+1) multiply of the forward sweep is just two more units in
 //    the producing CTA's stream.
-//  * Each unit's 32 columns are split over four groups of 64 threads (one row per thread, all
-//    16 right-hand-side columns in registers), so a thread does 64 FMAs per 9 shared-memory
-//    loads and the loop runs at the FMA rate; the four partial sums meet in shared memory at
-//    the end of a tile.
+//  * Each unit's 32 columns are split over four groups of 64 threads; a thread holds a 4 x 4
+//    register tile of the 64 x 16 product (6 shared-memory loads per 64 FMAs), and the four
+//    partial sums meet in shared memory at the end of a tile.
 //
 // Every barrier wait is bounded.  A wait that runs out marks the job diverged (JobDev::conv),
 // which also ends the other CTAs' waits, and the refinement re-solves that job in FP64.
@@ -67,48 +66,74 @@ __host__ __device__ inline FlowLayout flow_layout(int cs, int own) {
   return L;
 }
 
-// acc[c] += sum over columns kk in [k0, k1) of unit A: A[kk][r] * Y[y0 + kk][c], with the
-// right-hand side row-major (a ring slot; each row read as 8 broadcast float4).
-__device__ __forceinline__ void row_step(float2 (&acc)[kCols], const float2 *__restrict__ A,
-                                         const float2 *__restrict__ Y, int y0, int kk, int r) {
-  const float2 a = A[kk * 64 + r];
-  const float4 *y = reinterpret_cast<const float4 *>(Y + (y0 + kk) * kCols);
+// Register tile of a thread: rows rq + 16 i (i < 4) and columns 4 cq + m (m < 4) of the 64 x 16
+// product, over its group's columns kk of each unit.  Per column kk a warp loads 4 operand values
+// and 2 x 4 right-hand-side values per lane for 64 FMAs, which balances the shared-memory pipe
+// (128 B of register payload per clock, broadcasts included) against the FMA pipe.
+struct Frag {
+  float2 v[4][4];  // [i][m]
+};
+
+// acc += A[kk][row] * Y[y0 + kk][col] over kk in [k0, k1) of unit A, with the right-hand side
+// row-major (a ring slot).
+__device__ __forceinline__ void row_step(Frag &acc, const float2 *__restrict__ A, const float2 *__restrict__ Y,
+                                         int y0, int kk, int rq, int cq) {
+  float2 a[4];
 #pragma unroll
-  for (int p = 0; p < kCols / 2; ++p) {
-    const float4 v = y[p];
-    acc[2 * p] = cfma(a, make_float2(v.x, v.y), acc[2 * p]);
-    acc[2 * p + 1] = cfma(a, make_float2(v.z, v.w), acc[2 * p + 1]);
-  }
+  for (int i = 0; i < 4; ++i) a[i] = A[kk * 64 + rq + 16 * i];
+  const float4 *y = reinterpret_cast<const float4 *>(Y + (y0 + kk) * kCols + 4 * cq);
+  const float4 y01 = y[0], y23 = y[1];
+  const float2 yv[4] = {make_float2(y01.x, y01.y), make_float2(y01.z, y01.w), make_float2(y23.x, y23.y),
+                        make_float2(y23.z, y23.w)};
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int m = 0; m < 4; ++m) acc.v[i][m] = cfma(a[i], yv[m], acc.v[i][m]);
 }
-__device__ __forceinline__ void product_rows(float2 (&acc)[kCols], const float2 *__restrict__ A,
-                                             const float2 *__restrict__ Y, int y0, int k0, int k1, int r) {
+__device__ __forceinline__ void product_rows(Frag &acc, const float2 *__restrict__ A, const float2 *__restrict__ Y,
+                                             int y0, int k0, int k1, int rq, int cq) {
   if (k1 - k0 == kUnit / kGroups) {
 #pragma unroll
-    for (int i = 0; i < kUnit / kGroups; ++i) row_step(acc, A, Y, y0, k0 + i, r);
+    for (int i = 0; i < kUnit / kGroups; ++i) row_step(acc, A, Y, y0, k0 + i, rq, cq);
   } else {
-    for (int kk = k0; kk < k1; ++kk) row_step(acc, A, Y, y0, kk, r);
+    for (int kk = k0; kk < k1; ++kk) row_step(acc, A, Y, y0, kk, rq, cq);
   }
 }
 // The same with the right-hand side column-major (a resident tile, Yc[c * 64 + row]).
-__device__ __forceinline__ void col_step(float2 (&acc)[kCols], const float2 *__restrict__ A,
-                                         const float2 *__restrict__ Yc, int y0, int kk, int r) {
-  const float2 a = A[kk * 64 + r];
+__device__ __forceinline__ void col_step(Frag &acc, const float2 *__restrict__ A, const float2 *__restrict__ Yc,
+                                         int y0, int kk, int rq, int cq) {
+  float2 a[4], yv[4];
 #pragma unroll
-  for (int c = 0; c < kCols; ++c) acc[c] = cfma(a, Yc[c * 64 + y0 + kk], acc[c]);
+  for (int i = 0; i < 4; ++i) a[i] = A[kk * 64 + rq + 16 * i];
+#pragma unroll
+  for (int m = 0; m < 4; ++m) yv[m] = Yc[(4 * cq + m) * 64 + y0 + kk];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int m = 0; m < 4; ++m) acc.v[i][m] = cfma(a[i], yv[m], acc.v[i][m]);
 }
-__device__ __forceinline__ void product_cols(float2 (&acc)[kCols], const float2 *__restrict__ A,
-                                             const float2 *__restrict__ Yc, int y0, int k0, int k1, int r) {
+__device__ __forceinline__ void product_cols(Frag &acc, const float2 *__restrict__ A, const float2 *__restrict__ Yc,
+                                             int y0, int k0, int k1, int rq, int cq) {
   if (k1 - k0 == kUnit / kGroups) {
 #pragma unroll
-    for (int i = 0; i < kUnit / kGroups; ++i) col_step(acc, A, Yc, y0, k0 + i, r);
+    for (int i = 0; i < kUnit / kGroups; ++i) col_step(acc, A, Yc, y0, k0 + i, rq, cq);
   } else {
-    for (int kk = k0; kk < k1; ++kk) col_step(acc, A, Yc, y0, kk, r);
+    for (int kk = k0; kk < k1; ++kk) col_step(acc, A, Yc, y0, kk, rq, cq);
   }
 }
 
-__device__ __forceinline__ void store_partials(float2 *part, const float2 (&acc)[kCols], int g, int r) {
+__device__ __forceinline__ void zero(Frag &acc) {
 #pragma unroll
-  for (int c = 0; c < kCols; ++c) part[(g * kCols + c) * 64 + r] = acc[c];
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int m = 0; m < 4; ++m) acc.v[i][m] = make_float2(0.f, 0.f);
+}
+// Partial sums of group g, column-major per group: part[(g * 16 + col) * 64 + row].
+__device__ __forceinline__ void store_partials(float2 *part, const Frag &acc, int g, int rq, int cq) {
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int m = 0; m < 4; ++m) part[(g * kCols + 4 * cq + m) * 64 + rq + 16 * i] = acc.v[i][m];
 }
 __device__ __forceinline__ float2 sum_partials(const float2 *part, int c, int row) {
   float2 s = part[c * 64 + row];
@@ -305,7 +330,7 @@ __global__ void __launch_bounds__(kThreads, 1) forward_flow_kernel(const JobDev 
   const int n = J.n, N = J.N, ld = J.ld, b = J.b, ns = L.ns;
   const float2 *__restrict__ F = static_cast<const float2 *>(J.F);
   int *conv = J.conv;
-  const int tid = threadIdx.x, r = tid & 63, g = tid >> 6;
+  const int tid = threadIdx.x, r = tid & 63, g = tid >> 6, rq = tid & 15, cq = (tid >> 4) & 3;
   const int nsteps = (n + 63) / 64, T = (N + 63) / 64;
 
   init_barriers(S, ns, cs);
@@ -337,9 +362,8 @@ __global__ void __launch_bounds__(kThreads, 1) forward_flow_kernel(const JobDev 
     while (ok && !it.fin && it.j == j) {
       const int t = it.t;
       const bool dk = it.d;
-      float2 acc[kCols];
-#pragma unroll
-      for (int c = 0; c < kCols; ++c) acc[c] = make_float2(0.f, 0.f);
+      Frag acc;
+      zero(acc);
       do {
         cp_async_wait<kStages - 2>();
         __syncthreads();  // unit u has landed for every thread; the stage before it is free again
@@ -351,13 +375,13 @@ __global__ void __launch_bounds__(kThreads, 1) forward_flow_kernel(const JobDev 
         const float2 *A = S.ring + (u % kStages) * kUnitElems;
         const int k0 = 8 * g, k1 = min(k0 + 8, it.ncol());
         if (dk)
-          product_cols(acc, A, S.tiles + (t / cs) * kTileElems, it.h * kUnit, k0, k1, r);
+          product_cols(acc, A, S.tiles + (t / cs) * kTileElems, it.h * kUnit, k0, k1, rq, cq);
         else
-          product_rows(acc, A, S.slots + (j % ns) * kTileElems, it.h * kUnit, k0, k1, r);
+          product_rows(acc, A, S.slots + (j % ns) * kTileElems, it.h * kUnit, k0, k1, rq, cq);
         ++u;
         it.next();
       } while (!it.fin && it.j == j && it.t == t && it.d == dk && it.h != 0);
-      store_partials(S.part, acc, g, r);
+      store_partials(S.part, acc, g, rq, cq);
       __syncthreads();
       if (!dk) {
         // R[tile t] -= A21_j Y_j for the rows below the block
@@ -423,7 +447,7 @@ __global__ void __launch_bounds__(kThreads, 1) backward_flow_kernel(const JobDev
   const int n = J.n, ld = J.ld, b = J.b, ns = L.ns;
   const float2 *__restrict__ F = static_cast<const float2 *>(J.F);
   int *conv = J.conv;
-  const int tid = threadIdx.x, r = tid & 63, g = tid >> 6;
+  const int tid = threadIdx.x, r = tid & 63, g = tid >> 6, rq = tid & 15, cq = (tid >> 4) & 3;
   const int kstart = n > 0 ? ((n - 1) / 64) * 64 : 0;  // last block
   const int nsteps = n > 0 ? kstart / 64 + 2 : 1;       // central block + blocks kstart .. 0
   const int p0 = kstart / 64 + 1;
@@ -478,9 +502,8 @@ __global__ void __launch_bounds__(kThreads, 1) backward_flow_kernel(const JobDev
     const int tnext = s + 1 < nsteps ? (kstart - 64 * s) / 64 : -1;  // tile of block s + 1
     while (ok && !it.fin && it.s == s) {
       const int t = it.t;
-      float2 acc[kCols];
-#pragma unroll
-      for (int c = 0; c < kCols; ++c) acc[c] = make_float2(0.f, 0.f);
+      Frag acc;
+      zero(acc);
       do {
         cp_async_wait<kStages - 2>();
         __syncthreads();
@@ -491,11 +514,11 @@ __global__ void __launch_bounds__(kThreads, 1) backward_flow_kernel(const JobDev
         cp_async_commit();
         const float2 *A = S.ring + (u % kStages) * kUnitElems;
         const int k0 = 8 * g, k1 = min(k0 + 8, it.ncol());
-        product_rows(acc, A, S.slots + (s % ns) * kTileElems, it.h * kUnit, k0, k1, r);
+        product_rows(acc, A, S.slots + (s % ns) * kTileElems, it.h * kUnit, k0, k1, rq, cq);
         ++u;
         it.next();
       } while (!it.fin && it.s == s && it.t == t && it.h != 0);
-      store_partials(S.part, acc, g, r);
+      store_partials(S.part, acc, g, rq, cq);
       __syncthreads();
       // Y[tile t] -= W[tile t, block s] Y_s for the rows above the block
       float2 *Yt = S.tiles + (t / cs) * kTileElems;
