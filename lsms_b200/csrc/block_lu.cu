@@ -574,16 +574,16 @@ cudaError_t eliminate_impl(const JobDev *jobs, int njobs, int max_n, int max_N, 
 
 template <typename T>
 cudaError_t sweep_solve(const JobDev *jobs, int njobs, int b, int max_N, int mode, int *info, cudaStream_t s,
-                        long *launches, bool fp32) {
+                        long *launches, bool fp32, const CUtensorMap *fmap) {
   const FactorKind fk = sizeof(T) == sizeof(double2) ? kFactorFP64 : kFactorFP32;
   cudaError_t e;
   // forward (skipped for the initial solve: B is zero above the central block)
   if (mode == 1) {
-    if ((e = launch_sweep(fk, jobs, njobs, b, max_N, true, mode, fp32, s)) != cudaSuccess) return e;
+    if ((e = launch_sweep(fk, jobs, njobs, b, max_N, true, mode, fp32, fmap, s)) != cudaSuccess) return e;
     if (launches) *launches += 1;
   }
   schur_solve_kernel<T><<<njobs, 256, 0, s>>>(jobs, mode, info);
-  if ((e = launch_sweep(fk, jobs, njobs, b, max_N, false, mode, fp32, s)) != cudaSuccess) return e;
+  if ((e = launch_sweep(fk, jobs, njobs, b, max_N, false, mode, fp32, fmap, s)) != cudaSuccess) return e;
   if (launches) *launches += 2;
   return cudaSuccess;
 }
@@ -707,15 +707,17 @@ cudaError_t launch_finalize_direct(FactorKind fk, const JobDev *jobs, int njobs,
 }
 
 cudaError_t launch_refine_begin(FactorKind fk, const JobDev *jobs, int njobs, int max_n, int max_N, int b,
-                                int *info, cudaStream_t s, long *launches, bool fp32_sweep) {
+                                int *info, cudaStream_t s, long *launches, bool fp32_sweep,
+                                const CUtensorMap *fmap) {
   (void)max_n;
-  const cudaError_t e = fk == kFactorFP64 ? sweep_solve<double2>(jobs, njobs, b, max_N, 0, info, s, launches, false)
-                                           : sweep_solve<float2>(jobs, njobs, b, max_N, 0, info, s, launches, fp32_sweep);
+  const cudaError_t e = fk == kFactorFP64 ? sweep_solve<double2>(jobs, njobs, b, max_N, 0, info, s, launches, false, nullptr)
+                                           : sweep_solve<float2>(jobs, njobs, b, max_N, 0, info, s, launches, fp32_sweep, fmap);
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 
 cudaError_t launch_refine_round(FactorKind fk, const JobDev *jobs, int njobs, int max_n, int max_N, int b,
-                                bool check, int *info, cudaStream_t s, long *launches, bool fp32_sweep) {
+                                bool check, int *info, cudaStream_t s, long *launches, bool fp32_sweep,
+                                const CUtensorMap *fmap) {
   (void)max_n;
   cudaError_t e0;
   if (b <= 16) {
@@ -732,8 +734,8 @@ cudaError_t launch_refine_round(FactorKind fk, const JobDev *jobs, int njobs, in
     residual_kernel<32><<<dim3((max_N + residual_rows<32>() - 1) / residual_rows<32>(), njobs), 256, sm32, s>>>(jobs);
   }
   if (launches) *launches += 1;
-  const cudaError_t e = fk == kFactorFP64 ? sweep_solve<double2>(jobs, njobs, b, max_N, 1, info, s, launches, false)
-                                           : sweep_solve<float2>(jobs, njobs, b, max_N, 1, info, s, launches, fp32_sweep);
+  const cudaError_t e = fk == kFactorFP64 ? sweep_solve<double2>(jobs, njobs, b, max_N, 1, info, s, launches, false, nullptr)
+                                           : sweep_solve<float2>(jobs, njobs, b, max_N, 1, info, s, launches, fp32_sweep, fmap);
   if (e != cudaSuccess) return e;
   if (check) {
     converge_check_kernel<<<njobs, 256, 0, s>>>(jobs, kRefineTol);
@@ -750,10 +752,11 @@ cudaError_t launch_refine_end(const JobDev *jobs, int njobs, int ns, int kkrsz, 
 
 cudaError_t launch_solve_refine(FactorKind fk, const JobDev *jobs, int njobs, int max_n, int max_N, int b,
                                 int steps, int ns, int kkrsz, int *info, cudaStream_t s, long *launches,
-                                bool fp32_sweep) {
-  cudaError_t e = launch_refine_begin(fk, jobs, njobs, max_n, max_N, b, info, s, launches, fp32_sweep);
+                                bool fp32_sweep, const CUtensorMap *fmap) {
+  cudaError_t e = launch_refine_begin(fk, jobs, njobs, max_n, max_N, b, info, s, launches, fp32_sweep, fmap);
   for (int it = 0; it < steps && e == cudaSuccess; ++it)
-    e = launch_refine_round(fk, jobs, njobs, max_n, max_N, b, it + 1 < steps, info, s, launches, fp32_sweep);
+    e = launch_refine_round(fk, jobs, njobs, max_n, max_N, b, it + 1 < steps, info, s, launches, fp32_sweep,
+                            fmap);
   if (e != cudaSuccess) return e;
   return launch_refine_end(jobs, njobs, ns, kkrsz, s, launches);
 }

@@ -236,6 +236,7 @@ void fill_slot(b200tau_ctx *ctx, JobDev &J, int slot, int ld, const Plan &p) {
   J.ld = ld;
   J.conv = ctx->d_conv + slot;
   J.cnorm = ctx->d_cnorm + slot;
+  J.slot = slot;
 }
 
 // Clears the per-slot status of the first nw slots: singular-pivot info, converged flag, last
@@ -361,10 +362,16 @@ int encode_factor_map(b200tau_ctx *ctx, int ld, int slots) {
   const cuuint64_t strides[2] = {(cuuint64_t)2 * ld * sizeof(float), (cuuint64_t)ctx->f_bytes};
   const cuuint32_t box[3] = {128, 64, 1};
   const cuuint32_t estr[3] = {1, 1, 1};
-  const CUresult r = enc(&ctx->tc.tF, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, ctx->d_F, dims, strides, box, estr,
-                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
-                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  CUresult r = enc(&ctx->tc.tF, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, ctx->d_F, dims, strides, box, estr,
+                   CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(ctx, B200TAU_ERR_CUDA, "cuTensorMapEncodeTiled (F) failed (%d)", (int)r);
+  // the sweeps' operand units: 64 complex rows x 32 columns
+  const cuuint32_t ubox[3] = {128, 32, 1};
+  r = enc(&ctx->tc.tFu, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, ctx->d_F, dims, strides, ubox, estr,
+          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(ctx, B200TAU_ERR_CUDA, "cuTensorMapEncodeTiled (F units) failed (%d)", (int)r);
   return B200TAU_OK;
 }
 
@@ -429,10 +436,10 @@ int ensure_fallback(b200tau_ctx *ctx, int ld) {
 // from the launches after kCompactAfterRounds), tau00_l.  `h` are the wave's records as uploaded
 // to ctx->d_jobs.
 int run_refinement(b200tau_ctx *ctx, const std::vector<JobDev> &h, int nw, int maxn, int maxN, int b, int ns,
-                   int kkrsz, const Plan &p) {
+                   int kkrsz, const Plan &p, const CUtensorMap *fmap) {
   const bool fp32_sweep = p.fk == kFactorFP32 && ctx->mixed_sweep == B200TAU_SWEEP_FP32;
   CK(launch_refine_begin(p.fk, ctx->d_jobs, nw, maxn, maxN, b, ctx->d_info, ctx->stream, &ctx->launches,
-                         fp32_sweep));
+                         fp32_sweep, fmap));
   // The kernels skip converged jobs.  After kCompactAfterRounds rounds the host reads the converged
   // flags once (the only wait inside a wave; the rest of the wave is queued right after it) and
   // the remaining rounds run on the unconverged jobs alone, with launches sized for them.
@@ -467,10 +474,20 @@ int run_refinement(b200tau_ctx *ctx, const std::vector<JobDev> &h, int nw, int m
       }
     }
     CK(launch_refine_round(p.fk, cur, ncur, cmaxn, cmaxN, b, true, cur_info, ctx->stream, &ctx->launches,
-                           fp32_sweep));
+                           fp32_sweep, fmap));
   }
   CK(launch_refine_end(ctx->d_jobs, nw, ns, kkrsz, ctx->stream, &ctx->launches));
   if (p.fk != kFactorFP32 || !ctx->fallback_on || ncur == 0) return B200TAU_OK;
+  {
+    // the second (and last) wait of a wave: when every job converged, none of the re-solve's
+    // launches is queued
+    std::vector<int> conv(nw);
+    CK(cudaMemcpyAsync(conv.data(), ctx->d_conv, sizeof(int) * nw, cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    bool any = false;
+    for (int w = 0; w < nw; ++w) any = any || conv[w] != kConverged;
+    if (!any) return B200TAU_OK;
+  }
   // Jobs whose FP32-factor refinement did not converge (condition numbers beyond what FP32 block
   // factors can refine, e.g. energies next to the real axis) take the FP64 path instead: an FP64
   // copy of the unmodified M, FP64 block elimination, the FP64 refinement rounds, tau00 from X -
@@ -516,7 +533,7 @@ int run_pipeline(b200tau_ctx *ctx, const std::vector<JobDev> &h, int nw, int max
                       ctx->profiling ? &ctx->timer : nullptr, tc, ctx->d_err));
   if ((rc = phase_end(ctx, 1)) || (rc = phase_begin(ctx))) return rc;
   if (p.steps > 0) {
-    if ((rc = run_refinement(ctx, h, nw, maxn, maxN, b, ns, kkrsz, p))) return rc;
+    if ((rc = run_refinement(ctx, h, nw, maxn, maxN, b, ns, kkrsz, p, tc ? &tc->tFu : nullptr))) return rc;
   } else {
     CK(launch_finalize_direct(p.fk, ctx->d_jobs, nw, ns, kkrsz, ctx->d_info, ctx->stream, &ctx->launches));
   }

@@ -2,6 +2,7 @@
 // sweep_flow.cu).
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 namespace b200 {
@@ -90,12 +91,32 @@ __device__ __forceinline__ bool mbar_try_cluster(unsigned long long *b, unsigned
   return ok != 0;
 }
 
-// Grid (cs, njobs) of 256-thread CTAs in clusters of (cs, 1, 1): one cluster per job.
+// Local barrier: one arrival that also expects `bytes` of asynchronous (TMA) transfers.
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long *b, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(b)), "r"(bytes) : "memory");
+}
+// Orders this thread's earlier generic-proxy shared-memory accesses before its later async-proxy
+// (TMA) ones.
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+// Tiled TMA load of the box at (x, y, z) of a 3-D tensor map into shared memory, completing on
+// barrier `bar`.  x times the element size must be a multiple of 16 bytes.
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z,
+                                            unsigned long long *bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];" ::
+          "r"(smem_u32(dst)),
+      "l"(map), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+      : "memory");
+}
+
+// Grid (cs, njobs) of `threads`-thread CTAs in clusters of (cs, 1, 1): one cluster per job.
 template <typename Kern, typename... Args>
-cudaError_t launch_cluster(Kern kern, int cs, int njobs, int smem, cudaStream_t s, Args... args) {
+cudaError_t launch_cluster(Kern kern, int cs, int njobs, int threads, int smem, cudaStream_t s, Args... args) {
   cudaLaunchConfig_t cfg = {};
   cfg.gridDim = dim3(cs, njobs, 1);
-  cfg.blockDim = dim3(256, 1, 1);
+  cfg.blockDim = dim3(threads, 1, 1);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = s;
   cudaLaunchAttribute attr[1];

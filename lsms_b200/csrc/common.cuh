@@ -84,7 +84,8 @@ struct JobDev {
   int t0_ld;
   int out_mode;          // 0: tau00_l (tau00 - t0, rotated); 1: raw tau00
   int inactive;          // 1: every kernel skips this record (a converged job in the FP64 re-solve)
-  int pad_[2];
+  int slot;              // workspace slot of F (the z coordinate of the factor tensor maps)
+  int pad_[1];
   // adjoint (b200tau_solve_vjp) only
   double2 *V;            // N x N workspace for M^-1 (ld)
   const double2 *taubar; // b x b cotangent on tau00
@@ -121,7 +122,8 @@ struct KernelTimer {
 // Per wave slot: A pack 2 ld rows x 128 floats (hi and lo), B pack ld rows x 128 floats.
 struct TcMaps {
   CUtensorMap tA_hi, tA_lo, tB_hi, tB_lo;
-  CUtensorMap tF;  // the wave's FP32 factor slots as floats {2 ld, ld, slots}, box {128, 64, 1}
+  CUtensorMap tF;   // the wave's FP32 factor slots as floats {2 ld, ld, slots}, box {128, 64, 1}
+  CUtensorMap tFu;  // the same slots, box {128, 32, 1}: one 64-row x 32-column sweep unit
   float *a_hi = nullptr, *a_lo = nullptr, *b_hi = nullptr, *b_lo = nullptr;
   size_t a_slot = 0, b_slot = 0;  // floats per slot
 };
@@ -161,26 +163,29 @@ cudaError_t launch_finalize_direct(FactorKind fk, const JobDev *jobs, int njobs,
 // zcgesv does; the residual and X += Y stay FP64.
 cudaError_t launch_solve_refine(FactorKind fk, const JobDev *jobs, int njobs, int max_n, int max_N,
                                 int b, int steps, int ns, int kkrsz, int *info, cudaStream_t s,
-                                long *launches, bool fp32_sweep = false);
+                                long *launches, bool fp32_sweep = false, const CUtensorMap *fmap = nullptr);
 // The same in pieces, for a driver that drops converged jobs between rounds: the initial solve
 // X = F^-1 [0; t0], one refinement round (with the convergence check when `check`), and tau00_l.
 cudaError_t launch_refine_begin(FactorKind fk, const JobDev *jobs, int njobs, int max_n, int max_N, int b,
-                                int *info, cudaStream_t s, long *launches, bool fp32_sweep = false);
+                                int *info, cudaStream_t s, long *launches, bool fp32_sweep = false,
+                                const CUtensorMap *fmap = nullptr);
 cudaError_t launch_refine_round(FactorKind fk, const JobDev *jobs, int njobs, int max_n, int max_N, int b,
-                                bool check, int *info, cudaStream_t s, long *launches, bool fp32_sweep = false);
+                                bool check, int *info, cudaStream_t s, long *launches, bool fp32_sweep = false,
+                                const CUtensorMap *fmap = nullptr);
 cudaError_t launch_refine_end(const JobDev *jobs, int njobs, int ns, int kkrsz, cudaStream_t s, long *launches);
 // One block sweep of the correction solve for all jobs, one thread-block cluster per job
 // (sweep.cu): forward (R -> Y over the D_k, A21_k factors) or backward (Y over the W_k factors,
 // X (+)= Y).  `fp32_arith` selects FP32 arithmetic on FP32 factors.  max_N bounds the jobs' N.
 cudaError_t launch_sweep(FactorKind fk, const JobDev *jobs, int njobs, int b, int max_N, bool forward, int mode,
-                         bool fp32_arith, cudaStream_t s);
+                         bool fp32_arith, const CUtensorMap *fmap, cudaStream_t s);
 // Cluster size of the sweeps for a wave of njobs (sweep.cu).
 int sweep_cluster_size(int njobs);
-// The dataflow sweeps for FP32 factors in FP32 arithmetic with b <= 16 (sweep_flow.cu).  Sets
-// *launched when it took the launch; false (and cudaSuccess) when the shape does not fit its
+// The dataflow sweeps for FP32 factors in FP32 arithmetic with b <= 16 (sweep_flow.cu), operand
+// units loaded through `fmap` (TcMaps::tFu over the jobs' factor slots).  Sets *launched when it
+// took the launch; false (and cudaSuccess) without a map or when the shape does not fit its
 // shared-memory layout, and the caller runs launch_sweep's step-synchronous kernels instead.
 cudaError_t launch_flow_sweep(const JobDev *jobs, int njobs, int b, int max_N, bool forward, int mode,
-                              cudaStream_t s, bool *launched);
+                              const CUtensorMap *fmap, cudaStream_t s, bool *launched);
 // Adjoint (adjoint.cu), FP64 factors: V = M^-1 from the block factors in F, then per LIZ site the
 // tau00 cotangent pull-back and d ln det M / d t (needs G in M, X refined, V).
 cudaError_t launch_inverse(const JobDev *jobs, int njobs, int max_n, int max_N, cudaStream_t s, long *launches);

@@ -347,13 +347,13 @@ cudaError_t sweep_impl(const JobDev *jobs, int njobs, bool forward, int mode, cu
     if ((e = cudaFuncSetAttribute(forward_sweep_kernel<T, V, BC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                   smem)) != cudaSuccess)
       return e;
-    return launch_cluster(forward_sweep_kernel<T, V, BC>, cs, njobs, smem, s, jobs);
+    return launch_cluster(forward_sweep_kernel<T, V, BC>, cs, njobs, 256, smem, s, jobs);
   }
   const int smem = SweepSmem<T, V>::kBackward;
   if ((e = cudaFuncSetAttribute(backward_sweep_kernel<T, V, BC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 smem)) != cudaSuccess)
     return e;
-  return launch_cluster(backward_sweep_kernel<T, V, BC>, cs, njobs, smem, s, jobs, mode);
+  return launch_cluster(backward_sweep_kernel<T, V, BC>, cs, njobs, 256, smem, s, jobs, mode);
 }
 
 template <typename T, typename V>
@@ -373,13 +373,13 @@ int sweep_cluster_size(int njobs) {
 }
 
 cudaError_t launch_sweep(FactorKind fk, const JobDev *jobs, int njobs, int b, int max_N, bool forward, int mode,
-                         bool fp32_arith, cudaStream_t s) {
+                         bool fp32_arith, const CUtensorMap *fmap, cudaStream_t s) {
   if (njobs <= 0) return cudaSuccess;
   if (b < 1 || b > kMaxB || (forward && mode != 1)) return cudaErrorInvalidValue;
   if (fk == kFactorFP64) return sweep_b<double2, double2>(jobs, njobs, b, forward, mode, s);
   if (fp32_arith) {
     bool done = false;
-    const cudaError_t e = launch_flow_sweep(jobs, njobs, b, max_N, forward, mode, s, &done);
+    const cudaError_t e = launch_flow_sweep(jobs, njobs, b, max_N, forward, mode, fmap, s, &done);
     if (e != cudaSuccess || done) return e;
     return sweep_b<float2, float2>(jobs, njobs, b, forward, mode, s);
   }
