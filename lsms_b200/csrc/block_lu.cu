@@ -428,10 +428,16 @@ __host__ __device__ constexpr int residual_smem_bytes() {
   return kResStages * kResK * (residual_rows<BC>() + BC) * (int)sizeof(double2);
 }
 
+// Register tile of a residual thread: RPT rows (ROWS / RPT apart) x NCT columns, 10 shared-memory
+// loads per 16 complex FMAs.
+template <int BC> struct ResTile { static constexpr int RPT = 2, NCT = 8; };
+
 template <int BC>
 __global__ void __launch_bounds__(256, 2) residual_kernel(const JobDev *__restrict__ jobs) {
-  constexpr int NC = 16;                  // columns per thread
+  constexpr int RPT = ResTile<BC>::RPT, NCT = ResTile<BC>::NCT;
   constexpr int ROWS = residual_rows<BC>();  // rows per CTA
+  constexpr int RG = ROWS / RPT;             // row groups
+  static_assert(RG * (BC / NCT) == 256, "residual thread layout");
   const JobDev &J = jobs[blockIdx.y];
   if (converged(J) || J.inactive) return;
   const int N = J.N, ld = J.ld, b = J.b;
@@ -442,8 +448,7 @@ __global__ void __launch_bounds__(256, 2) residual_kernel(const JobDev *__restri
   double2(*Xs)[kResK][BC] =
       reinterpret_cast<double2(*)[kResK][BC]>(rsm + sizeof(double2) * kResStages * kResK * ROWS);
   const int tid = threadIdx.x;
-  const int r = tid % ROWS, cg = tid / ROWS;
-  const int gr = row0 + r;
+  const int rg = tid % RG, cg = tid / RG;
   const double2 *__restrict__ M = J.M;
   const double2 *__restrict__ X = J.X;
   const double2 zero = make_double2(0.0, 0.0);
@@ -464,9 +469,11 @@ __global__ void __launch_bounds__(256, 2) residual_kernel(const JobDev *__restri
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
   };
-  double2 acc[NC];
+  double2 acc[RPT][NCT];
 #pragma unroll
-  for (int j = 0; j < NC; ++j) acc[j] = zero;
+  for (int i = 0; i < RPT; ++i)
+#pragma unroll
+    for (int j = 0; j < NCT; ++j) acc[i][j] = zero;
   const int nst = (N + kResK - 1) / kResK;
 #pragma unroll
   for (int q = 0; q < kResStages - 1; ++q) {
@@ -482,19 +489,29 @@ __global__ void __launch_bounds__(256, 2) residual_kernel(const JobDev *__restri
     const int st = q % kResStages;
 #pragma unroll
     for (int kk = 0; kk < kResK; ++kk) {
-      const double2 a = Ms[st][kk][r];
+      double2 a[RPT];
 #pragma unroll
-      for (int j = 0; j < NC; ++j) acc[j] = cfma(a, Xs[st][kk][cg * NC + j], acc[j]);
+      for (int i = 0; i < RPT; ++i) a[i] = Ms[st][kk][rg + i * RG];
+#pragma unroll
+      for (int j = 0; j < NCT; ++j) {
+        const double2 x = Xs[st][kk][cg * NCT + j];
+#pragma unroll
+        for (int i = 0; i < RPT; ++i) acc[i][j] = cfma(a[i], x, acc[i][j]);
+      }
     }
   }
   asm volatile("cp.async.wait_group 0;" ::: "memory");
-  if (gr >= N) return;
 #pragma unroll
-  for (int j = 0; j < NC; ++j) {
-    const int c = cg * NC + j;
-    if (c >= b) continue;
-    const double2 bv = (gr >= J.n) ? J.t0[(gr - J.n) + (size_t)c * J.t0_ld] : zero;
-    J.R[(size_t)gr + (size_t)c * ld] = csub(bv, acc[j]);
+  for (int i = 0; i < RPT; ++i) {
+    const int gr = row0 + rg + i * RG;
+    if (gr >= N) continue;
+#pragma unroll
+    for (int j = 0; j < NCT; ++j) {
+      const int c = cg * NCT + j;
+      if (c >= b) continue;
+      const double2 bv = (gr >= J.n) ? J.t0[(gr - J.n) + (size_t)c * J.t0_ld] : zero;
+      J.R[(size_t)gr + (size_t)c * ld] = csub(bv, acc[i][j]);
+    }
   }
 }
 
