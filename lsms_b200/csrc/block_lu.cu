@@ -547,9 +547,52 @@ __global__ void __launch_bounds__(256) schur_solve_kernel(const JobDev *__restri
 // CTAs of the looping trailing-update grid (two per SM)
 constexpr int kSparseGrid = 2 * 148;
 
+// Step k: W = D A12 and the operand packs on s, then the panel tiles of the update; s2 waits for
+// them and inverts the next diagonal block while s updates the other tiles; s waits for that
+// inverse before step k + 1.  Only the diagonal inverse moves off s, so the packs of step k + 1 are
+// written after every tile of step k has read those of step k.
+template <typename T, typename S>
+cudaError_t eliminate_lookahead(const JobDev *jobs, int njobs, int max_n, int max_N, int *info, cudaStream_t s,
+                                long *launches, KernelTimer *timer, const TcMaps &tc, int *err, const Lookahead &la,
+                                int smem_diag, int smem_gemm) {
+  cudaError_t e;
+  const int free_sms = njobs < tc_num_sms() / 2 ? njobs : tc_num_sms() / 2;
+  diag_inverse_kernel<T><<<njobs, kDiagThreads, smem_diag, s>>>(jobs, 0, info);
+  if (launches) *launches += 1;
+  for (int k = 0; k < max_n; k += kNb) {
+    const int rest = max_N - k - 1;
+    const int tiles = (rest + kTile - 1) / kTile;
+    const bool next = k + kNb < max_n;
+    if (tiles > 0) {
+      zgemm_tile_kernel<S, kOverwrite><<<dim3(tiles, 1, njobs), 256, smem_gemm, s>>>(jobs, k, tiles, 1, njobs);
+      const bool timed = timer && timer->used + 2 <= timer->cap;
+      if (timed) cudaEventRecord(timer->ev[timer->used++], s);
+      if ((e = launch_tc_pack(tc, jobs, njobs, k, max_N, s)) != cudaSuccess) return e;
+      if ((e = launch_tc_update(tc, jobs, njobs, k, max_N, err, s, 1, 0)) != cudaSuccess) return e;
+      if (next) {
+        if ((e = cudaEventRecord(la.panel, s)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(la.s2, la.panel, 0)) != cudaSuccess) return e;
+        diag_inverse_kernel<T><<<njobs, kDiagThreads, smem_diag, la.s2>>>(jobs, k + kNb, info);
+        if ((e = cudaEventRecord(la.diag, la.s2)) != cudaSuccess) return e;
+      }
+      if ((e = launch_tc_update(tc, jobs, njobs, k, max_N, err, s, 2, next ? tc_num_sms() - free_sms : 0)) !=
+          cudaSuccess)
+        return e;
+      if (next && (e = cudaStreamWaitEvent(s, la.diag, 0)) != cudaSuccess) return e;
+      if (timed) cudaEventRecord(timer->ev[timer->used++], s);
+      if (launches) *launches += next ? 5 : 4;
+    } else if (next) {
+      diag_inverse_kernel<T><<<njobs, kDiagThreads, smem_diag, s>>>(jobs, k + kNb, info);
+      if (launches) *launches += 1;
+    }
+  }
+  return cudaGetLastError();
+}
+
 template <typename T, typename S>
 cudaError_t eliminate_impl(const JobDev *jobs, int njobs, int max_n, int max_N, int *info, cudaStream_t s,
-                           long *launches, KernelTimer *timer, const TcMaps *tc, int *err, bool sparse_jobs) {
+                           long *launches, KernelTimer *timer, const TcMaps *tc, int *err, bool sparse_jobs,
+                           const Lookahead *la) {
   const int smem_diag = kNb * (kNb + 1) * (int)sizeof(double2);
   const int smem_gemm = 4 * kKc * kTile * (int)sizeof(T);
   cudaError_t e;
@@ -562,6 +605,12 @@ cudaError_t eliminate_impl(const JobDev *jobs, int njobs, int max_n, int max_N, 
   if ((e = cudaFuncSetAttribute(zgemm_tile_kernel<S, kSubtract>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem_gemm)) != cudaSuccess)
     return e;
+  // Look-ahead (tensor-core path): the update of step k first covers the panel tiles, which hold the
+  // next step's diagonal block; the next diagonal inverse then runs on the second stream while the
+  // other tiles are updated on SMs left free for it (the inverses take one SM per job).
+  if (tc != nullptr && la != nullptr && la->s2 != nullptr && !sparse_jobs)
+    return eliminate_lookahead<T, S>(jobs, njobs, max_n, max_N, info, s, launches, timer, *tc, err, *la, smem_diag,
+                                     smem_gemm);
   for (int k = 0; k < max_n; k += kNb) {
     diag_inverse_kernel<T><<<njobs, kDiagThreads, smem_diag, s>>>(jobs, k, info);
     const int rest = max_N - k - 1;
@@ -702,15 +751,16 @@ cudaError_t launch_copy_to_factor(FactorKind fk, const double2 *M, void *F, int 
 
 cudaError_t launch_eliminate(FactorKind fk, const JobDev *jobs, int njobs, int max_n, int max_N, int *info,
                              cudaStream_t s, long *launches, KernelTimer *timer, const TcMaps *tc,
-                             int *err, bool sparse_jobs) {
+                             int *err, bool sparse_jobs, const Lookahead *la) {
   if (fk == kFactorFP64)
     return eliminate_impl<double2, double>(jobs, njobs, max_n, max_N, info, s, launches, timer, nullptr, err,
-                                           sparse_jobs);
+                                           sparse_jobs, nullptr);
   if (tc) {
     cudaError_t e = tc_prepare();
     if (e != cudaSuccess) return e;
   }
-  return eliminate_impl<float2, float>(jobs, njobs, max_n, max_N, info, s, launches, timer, tc, err, sparse_jobs);
+  return eliminate_impl<float2, float>(jobs, njobs, max_n, max_N, info, s, launches, timer, tc, err, sparse_jobs,
+                                       la);
 }
 
 cudaError_t launch_finalize_direct(FactorKind fk, const JobDev *jobs, int njobs, int ns, int kkrsz, int *info,

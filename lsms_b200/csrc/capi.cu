@@ -53,6 +53,7 @@ struct b200tau_ctx {
   int device = 0;
   int lmax = 3, ns = 1, npola = 1, kkrsz = 16, b = 16, blk = 1024;
   cudaStream_t stream = nullptr;
+  Lookahead la;  // second stream and events of the elimination's look-ahead
   std::string err;
   AngularTables *d_tables = nullptr;
   double2 *d_tmat = nullptr;
@@ -530,7 +531,7 @@ int run_pipeline(b200tau_ctx *ctx, const std::vector<JobDev> &h, int nw, int max
   int rc = phase_begin(ctx);
   if (rc) return rc;
   CK(launch_eliminate(p.fk, ctx->d_jobs, nw, maxn, maxN, ctx->d_info, ctx->stream, &ctx->launches,
-                      ctx->profiling ? &ctx->timer : nullptr, tc, ctx->d_err));
+                      ctx->profiling ? &ctx->timer : nullptr, tc, ctx->d_err, false, &ctx->la));
   if ((rc = phase_end(ctx, 1)) || (rc = phase_begin(ctx))) return rc;
   if (p.steps > 0) {
     if ((rc = run_refinement(ctx, h, nw, maxn, maxN, b, ns, kkrsz, p, tc ? &tc->tFu : nullptr))) return rc;
@@ -714,6 +715,9 @@ int b200tau_create(b200tau_ctx **out, int device, int lmax, int n_spin_cant, int
   ctx->blk = (2 * ctx->kkrsz) * (2 * ctx->kkrsz);
   cudaError_t e = cudaSetDevice(device);
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->la.s2, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->la.panel, cudaEventDisableTiming);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ctx->la.diag, cudaEventDisableTiming);
   AngularTables tab;
   if (build_angular_tables(lmax, &tab)) e = cudaErrorInvalidValue;
   if (e == cudaSuccess) e = cudaMalloc(&ctx->d_tables, sizeof(AngularTables));
@@ -733,6 +737,7 @@ void b200tau_destroy(b200tau_ctx *ctx) {
   if (!ctx) return;
   cudaSetDevice(ctx->device);
   if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+  if (ctx->la.s2) cudaStreamSynchronize(ctx->la.s2);
   for (auto &a : ctx->atoms) free_atom(a);
   cudaFree(ctx->d_tables);
   cudaFree(ctx->d_tmat);
@@ -756,6 +761,9 @@ void b200tau_destroy(b200tau_ctx *ctx) {
   cudaFree(ctx->d_fbcount);
   for (auto &e : ctx->events) cudaEventDestroy(e);
   for (auto &e : ctx->pev) cudaEventDestroy(e);
+  if (ctx->la.panel) cudaEventDestroy(ctx->la.panel);
+  if (ctx->la.diag) cudaEventDestroy(ctx->la.diag);
+  if (ctx->la.s2) cudaStreamDestroy(ctx->la.s2);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }

@@ -135,6 +135,17 @@ cudaError_t tc_prepare();
 // Pack + tensor-core update A22 -= A21 W for step k of every job in the wave (FP32 factors).
 cudaError_t launch_tc_step(const TcMaps &maps, const JobDev *jobs, int njobs, int k, int max_N, int *err,
                            cudaStream_t s);
+// The two halves: the hi/lo operand packs of step k, and the update of the tiles of `part` (0 all,
+// 1 the first tile row and column of the trailing block, 2 the others) on at most max_grid SMs
+// (0: all).
+cudaError_t launch_tc_pack(const TcMaps &maps, const JobDev *jobs, int njobs, int k, int max_N, cudaStream_t s);
+cudaError_t launch_tc_update(const TcMaps &maps, const JobDev *jobs, int njobs, int k, int max_N, int *err,
+                             cudaStream_t s, int part, int max_grid);
+// A second stream and two events for the elimination's look-ahead (all null: none).
+struct Lookahead {
+  cudaStream_t s2 = nullptr;
+  cudaEvent_t panel = nullptr, diag = nullptr;
+};
 
 // Launchers (return cudaGetLastError of the launches).  `launches` accumulates the number of
 // kernels enqueued.
@@ -146,7 +157,8 @@ cudaError_t launch_kkr_build(const JobDev *jobs, int njobs, int max_L, const Bui
 // small looping grid instead of one CTA per tile.
 cudaError_t launch_eliminate(FactorKind fk, const JobDev *jobs, int njobs, int max_n, int max_N,
                              int *info, cudaStream_t s, long *launches, KernelTimer *timer,
-                             const TcMaps *tc, int *err, bool sparse_jobs = false);
+                             const TcMaps *tc, int *err, bool sparse_jobs = false,
+                             const Lookahead *la = nullptr);
 // F = M (n x n, leading dimension ld) converted to the factor type.
 cudaError_t launch_copy_to_factor(FactorKind fk, const double2 *M, void *F, int n, int ld, cudaStream_t s);
 // FP64 re-solve of the mixed jobs whose refinement did not converge, on the device: out[w] is
