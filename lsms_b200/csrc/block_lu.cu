@@ -186,8 +186,23 @@ constexpr int kTile = 64;
 constexpr int kKc = 16;
 enum { kOverwrite = 0, kSubtract = 1 };
 
+// Optional second output of the W = D A12 tiles (FP32, tensor-core path): W's hi/lo TF32 split in
+// the K-major operand layout of the trailing update (column c of the trailing block at
+// b + z * slot + c * 2 kNb floats, (re, im) of row p at 2 p), job z = the launch's job index.
+struct PackB {
+  float *hi = nullptr, *lo = nullptr;
+  size_t slot = 0;
+};
+
+__device__ __forceinline__ float tf32_round(float x) {
+  unsigned r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
 template <typename S, int MODE>
-__device__ __forceinline__ void zgemm_tile_body(const JobDev &J, int k, int bx, int by) {
+__device__ __forceinline__ void zgemm_tile_body(const JobDev &J, int k, int bx, int by, const PackB &pk = PackB(),
+                                                int z = 0) {
   using T = typename Vec2<S>::t;
   const int N = J.N, ld = J.ld;
   if (k >= J.n || J.inactive) return;
@@ -285,6 +300,14 @@ __device__ __forceinline__ void zgemm_tile_body(const JobDev &J, int k, int bx, 
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
       const int r = tx + 16 * i;
+      if (MODE == kOverwrite && sizeof(S) == 4 && pk.hi != nullptr) {
+        // rows past kb pack as zero
+        const float wr = r < m ? (float)acc[i][j].x : 0.f, wi = r < m ? (float)acc[i][j].y : 0.f;
+        const float hr = tf32_round(wr), hi = tf32_round(wi);
+        const size_t o = (size_t)z * pk.slot + (size_t)(bx * kTile + c) * (2 * kNb);
+        reinterpret_cast<float2 *>(pk.hi + o)[r] = make_float2(hr, hi);
+        reinterpret_cast<float2 *>(pk.lo + o)[r] = make_float2(wr - hr, wi - hi);
+      }
       if (r >= m) continue;
       T *dst = Cb + (size_t)r + (size_t)c * ld;
       if (MODE == kOverwrite) {
@@ -304,9 +327,9 @@ __device__ __forceinline__ void zgemm_tile_body(const JobDev &J, int k, int bx, 
 // prologue and C read-modify-write latencies are hidden by the other CTA's FMAs.
 template <typename S, int MODE>
 __global__ void __launch_bounds__(256, 2) zgemm_tile_kernel(const JobDev *__restrict__ jobs, int k, int tx, int ty,
-                                                            int nj) {
+                                                            int nj, PackB pk) {
   if (gridDim.z == (unsigned)nj && gridDim.x == (unsigned)tx && gridDim.y == (unsigned)ty) {
-    zgemm_tile_body<S, MODE>(jobs[blockIdx.z], k, blockIdx.x, blockIdx.y);
+    zgemm_tile_body<S, MODE>(jobs[blockIdx.z], k, blockIdx.x, blockIdx.y, pk, blockIdx.z);
     return;
   }
   // looping grid: jobs one after another (an inactive job costs one check), its tiles spread
@@ -547,9 +570,9 @@ __global__ void __launch_bounds__(256) schur_solve_kernel(const JobDev *__restri
 // CTAs of the looping trailing-update grid (two per SM)
 constexpr int kSparseGrid = 2 * 148;
 
-// Step k: W = D A12 and the operand packs on s, then the panel tiles of the update; s2 waits for
-// them and inverts the next diagonal block while s updates the other tiles; s waits for that
-// inverse before step k + 1.  Only the diagonal inverse moves off s, so the packs of step k + 1 are
+// Step k: W = D A12 (with W's operand pack) and A21's pack on s, then the update of the tile holding
+// the next diagonal block; s2 waits for it and inverts that block while s updates the other tiles;
+// s waits for the inverse before step k + 1.  Only the diagonal inverse moves off s, so the packs of step k + 1 are
 // written after every tile of step k has read those of step k.
 template <typename T, typename S>
 cudaError_t eliminate_lookahead(const JobDev *jobs, int njobs, int max_n, int max_N, int *info, cudaStream_t s,
@@ -564,10 +587,14 @@ cudaError_t eliminate_lookahead(const JobDev *jobs, int njobs, int max_n, int ma
     const int tiles = (rest + kTile - 1) / kTile;
     const bool next = k + kNb < max_n;
     if (tiles > 0) {
-      zgemm_tile_kernel<S, kOverwrite><<<dim3(tiles, 1, njobs), 256, smem_gemm, s>>>(jobs, k, tiles, 1, njobs);
+      PackB pk;
+      pk.hi = tc.b_hi;
+      pk.lo = tc.b_lo;
+      pk.slot = tc.b_slot;
+      zgemm_tile_kernel<S, kOverwrite><<<dim3(tiles, 1, njobs), 256, smem_gemm, s>>>(jobs, k, tiles, 1, njobs, pk);
       const bool timed = timer && timer->used + 2 <= timer->cap;
       if (timed) cudaEventRecord(timer->ev[timer->used++], s);
-      if ((e = launch_tc_pack(tc, jobs, njobs, k, max_N, s)) != cudaSuccess) return e;
+      if ((e = launch_tc_pack(tc, jobs, njobs, k, max_N, s, false)) != cudaSuccess) return e;
       if ((e = launch_tc_update(tc, jobs, njobs, k, max_N, err, s, 1, 0)) != cudaSuccess) return e;
       if (next) {
         if ((e = cudaEventRecord(la.panel, s)) != cudaSuccess) return e;
@@ -605,9 +632,9 @@ cudaError_t eliminate_impl(const JobDev *jobs, int njobs, int max_n, int max_N, 
   if ((e = cudaFuncSetAttribute(zgemm_tile_kernel<S, kSubtract>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem_gemm)) != cudaSuccess)
     return e;
-  // Look-ahead (tensor-core path): the update of step k first covers the panel tiles, which hold the
-  // next step's diagonal block; the next diagonal inverse then runs on the second stream while the
-  // other tiles are updated on SMs left free for it (the inverses take one SM per job).
+  // Look-ahead (tensor-core path): the update of step k first covers the tile holding the next
+  // step's diagonal block; the next diagonal inverse then runs on the second stream while the other
+  // tiles are updated on SMs left free for it (the inverses take one SM per job).
   if (tc != nullptr && la != nullptr && la->s2 != nullptr && !sparse_jobs)
     return eliminate_lookahead<T, S>(jobs, njobs, max_n, max_N, info, s, launches, timer, *tc, err, *la, smem_diag,
                                      smem_gemm);
@@ -617,7 +644,8 @@ cudaError_t eliminate_impl(const JobDev *jobs, int njobs, int max_n, int max_N, 
     const int tiles = (rest + kTile - 1) / kTile;
     if (launches) *launches += 1;
     if (tiles > 0) {
-      zgemm_tile_kernel<S, kOverwrite><<<dim3(tiles, 1, njobs), 256, smem_gemm, s>>>(jobs, k, tiles, 1, njobs);
+      zgemm_tile_kernel<S, kOverwrite><<<dim3(tiles, 1, njobs), 256, smem_gemm, s>>>(jobs, k, tiles, 1, njobs,
+                                                                                   PackB());
       const bool timed = timer && timer->used + 2 <= timer->cap;
       if (timed) cudaEventRecord(timer->ev[timer->used++], s);
       if (tc != nullptr) {
@@ -626,10 +654,10 @@ cudaError_t eliminate_impl(const JobDev *jobs, int njobs, int max_n, int max_N, 
       } else {
         if (sparse_jobs)
           zgemm_tile_kernel<S, kSubtract><<<std::min(tiles * tiles * njobs, kSparseGrid), 256, smem_gemm, s>>>(
-              jobs, k, tiles, tiles, njobs);
+              jobs, k, tiles, tiles, njobs, PackB());
         else
           zgemm_tile_kernel<S, kSubtract><<<dim3(tiles, tiles, njobs), 256, smem_gemm, s>>>(jobs, k, tiles, tiles,
-                                                                                           njobs);
+                                                                                           njobs, PackB());
       }
       if (timed) cudaEventRecord(timer->ev[timer->used++], s);
       if (launches) *launches += 2;

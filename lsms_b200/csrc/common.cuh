@@ -135,10 +135,11 @@ cudaError_t tc_prepare();
 // Pack + tensor-core update A22 -= A21 W for step k of every job in the wave (FP32 factors).
 cudaError_t launch_tc_step(const TcMaps &maps, const JobDev *jobs, int njobs, int k, int max_N, int *err,
                            cudaStream_t s);
-// The two halves: the hi/lo operand packs of step k, and the update of the tiles of `part` (0 all,
-// 1 the first tile row and column of the trailing block, 2 the others) on at most max_grid SMs
-// (0: all).
-cudaError_t launch_tc_pack(const TcMaps &maps, const JobDev *jobs, int njobs, int k, int max_N, cudaStream_t s);
+// The two halves: the hi/lo operand packs of step k (A21, and W unless the W = D A12 tiles wrote
+// theirs), and the update of the tiles of `part` (0 all, 1 the tile holding the next diagonal
+// block, 2 the others) on at most max_grid SMs (0: all).
+cudaError_t launch_tc_pack(const TcMaps &maps, const JobDev *jobs, int njobs, int k, int max_N, cudaStream_t s,
+                           bool pack_b);
 cudaError_t launch_tc_update(const TcMaps &maps, const JobDev *jobs, int njobs, int k, int max_N, int *err,
                              cudaStream_t s, int part, int max_grid);
 // A second stream and two events for the elimination's look-ahead (all null: none).

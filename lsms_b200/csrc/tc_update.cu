@@ -132,9 +132,9 @@ __device__ __forceinline__ float tf32_hi(float x) {
 
 // Tiles of one launch, sized for the largest trailing block of the wave: per job, part 0 covers
 // every tile (tm, tn) in the order ((z * tiles_m) + tm) * tiles_n + tn (tn fastest, so consecutive
-// CTAs share the A row block); part 1 only the first tile row and the first tile column (the
-// "panel": the next step's diagonal block, row block and column block); part 2 the others.  Tiles
-// outside a job's own trailing block are skipped identically by every role.
+// CTAs share the A row block); part 1 only tile (0, 0), which holds the next step's diagonal
+// block; part 2 all the others, in the same order.  Tiles outside a job's own trailing block are
+// skipped identically by every role.
 struct TileSpace {
   int tiles_m, tiles_n, per_job, total, part;
 };
@@ -147,12 +147,11 @@ __device__ __forceinline__ bool tile_of(const JobDev *jobs, const TileSpace &ts,
     tm = i / ts.tiles_n;
     tn = i - tm * ts.tiles_n;
   } else if (ts.part == 1) {
-    tm = i < ts.tiles_n ? 0 : i - ts.tiles_n + 1;
-    tn = i < ts.tiles_n ? i : 0;
+    tm = 0;
+    tn = 0;
   } else {
-    const int w = ts.tiles_n - 1;
-    tm = 1 + i / w;
-    tn = 1 + i - (tm - 1) * w;
+    tm = (i + 1) / ts.tiles_n;
+    tn = i + 1 - tm * ts.tiles_n;
   }
   const JobDev &J = jobs[z];
   if (k >= J.n) return false;
@@ -414,10 +413,11 @@ int tc_num_sms() {
   return n;
 }
 
-cudaError_t launch_tc_pack(const TcMaps &maps, const JobDev *jobs, int njobs, int k, int max_N, cudaStream_t s) {
+cudaError_t launch_tc_pack(const TcMaps &maps, const JobDev *jobs, int njobs, int k, int max_N, cudaStream_t s,
+                           bool pack_b) {
   const int rest = max_N - k - 1;  // upper bound of the trailing size over the wave
   if (rest <= 0) return cudaSuccess;
-  const int nA = (rest + 3) / 4, nB = (rest + 3) / 4;
+  const int nA = (rest + 3) / 4, nB = pack_b ? (rest + 3) / 4 : 0;
   tc_pack_kernel<<<dim3(nA + nB, njobs), 256, 0, s>>>(jobs, k, nA, maps.a_hi, maps.a_lo, maps.b_hi, maps.b_lo,
                                                       maps.a_slot, maps.b_slot);
   return cudaGetLastError();
@@ -431,9 +431,7 @@ cudaError_t launch_tc_update(const TcMaps &maps, const JobDev *jobs, int njobs, 
   ts.tiles_n = (rest + kTN - 1) / kTN;
   ts.tiles_m = (2 * rest + kTM - 1) / kTM;
   ts.part = part;
-  ts.per_job = part == 0 ? ts.tiles_m * ts.tiles_n
-               : part == 1 ? ts.tiles_m + ts.tiles_n - 1
-                           : (ts.tiles_m - 1) * (ts.tiles_n - 1);
+  ts.per_job = part == 0 ? ts.tiles_m * ts.tiles_n : part == 1 ? 1 : ts.tiles_m * ts.tiles_n - 1;
   ts.total = ts.per_job * njobs;
   if (ts.total <= 0) return cudaSuccess;
   int grid = ts.total < tc_num_sms() ? ts.total : tc_num_sms();
@@ -445,7 +443,7 @@ cudaError_t launch_tc_update(const TcMaps &maps, const JobDev *jobs, int njobs, 
 
 cudaError_t launch_tc_step(const TcMaps &maps, const JobDev *jobs, int njobs, int k, int max_N, int *err,
                            cudaStream_t s) {
-  cudaError_t e = launch_tc_pack(maps, jobs, njobs, k, max_N, s);
+  cudaError_t e = launch_tc_pack(maps, jobs, njobs, k, max_N, s, true);
   if (e != cudaSuccess) return e;
   return launch_tc_update(maps, jobs, njobs, k, max_N, err, s, 0, 0);
 }
