@@ -53,13 +53,23 @@ def algorithmic_flops(N: int, b: int, L: int) -> float:
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running."""
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms while running.
+
+    Started before the warm-up (nvidia-smi's own start-up queries the driver); only the samples
+    taken between mark_start() and mark_stop() count."""
 
     def __init__(self, gpu: int):
         self.gpu = gpu
         self.samples = []
         self._stop = threading.Event()
         self._proc = None
+        self._window = [None, None]
+
+    def mark_start(self):
+        self._window[0] = time.perf_counter()
+
+    def mark_stop(self):
+        self._window[1] = time.perf_counter()
 
     def __enter__(self):
         q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
@@ -79,7 +89,7 @@ class ClockSampler:
         for line in self._proc.stdout:
             parts = [p.strip() for p in line.split(",")]
             if len(parts) >= 7:
-                self.samples.append(parts)
+                self.samples.append((time.perf_counter(), parts))
 
     def __exit__(self, *a):
         if self._proc:
@@ -90,14 +100,21 @@ class ClockSampler:
                 self._proc.kill()
 
     def summary(self):
-        if not self.samples:
+        t0, t1 = self._window
+        inside = [p for t, p in self.samples if (t0 is None or t >= t0) and (t1 is None or t <= t1 + 0.25)]
+        samples = inside or [p for _, p in self.samples[-2:]]
+        return self._summarize(samples)
+
+    @staticmethod
+    def _summarize(samples):
+        if not samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
-        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        sm = [float(s[0]) for s in samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in samples if s[1].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].lower() == "active"})
+        reasons = sorted({names[i] for s in samples for i in range(4) if s[3 + i].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.samples)}
+                "reasons": reasons, "samples": len(samples)}
 
 
 def dist_setup():
@@ -374,22 +391,26 @@ def main():
         return float(t.item())
 
     def timed(prec, steps, warmup, sampler=None):
-        for _ in range(warmup):
-            s.solve_jobs_device(jobs, out.data_ptr(), prec)
-        s.sync()
-        torch.cuda.synchronize()
-        barrier()
-        e0 = torch.cuda.Event(enable_timing=True)
-        e1 = torch.cuda.Event(enable_timing=True)
-        launches = 0
         cm = sampler if sampler is not None else _Null()
-        with cm:
+        with cm:  # the sampler starts before the warm-up, and counts the timed window only
+            for _ in range(warmup):
+                s.solve_jobs_device(jobs, out.data_ptr(), prec)
+            s.sync()
+            torch.cuda.synchronize()
+            barrier()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            launches = 0
+            if sampler is not None:
+                sampler.mark_start()
             e0.record(stream)
             for _ in range(steps):
                 s.solve_jobs_device(jobs, out.data_ptr(), prec)
                 launches += s.last_launch_count
             e1.record(stream)
             s.sync()
+            if sampler is not None:
+                sampler.mark_stop()
         torch.cuda.synchronize()
         barrier()
         ms = e0.elapsed_time(e1) / steps

@@ -605,8 +605,8 @@ cudaError_t eliminate_lookahead(const JobDev *jobs, int njobs, int max_n, int ma
       if ((e = launch_tc_update(tc, jobs, njobs, k, max_N, err, s, 2, next ? tc_num_sms() - free_sms : 0)) !=
           cudaSuccess)
         return e;
+      if (timed) cudaEventRecord(timer->ev[timer->used++], s);  // the update kernels only
       if (next && (e = cudaStreamWaitEvent(s, la.diag, 0)) != cudaSuccess) return e;
-      if (timed) cudaEventRecord(timer->ev[timer->used++], s);
       if (launches) *launches += next ? 5 : 4;
     } else if (next) {
       diag_inverse_kernel<T><<<njobs, kDiagThreads, smem_diag, s>>>(jobs, k + kNb, info);
