@@ -39,10 +39,11 @@ sys.path.insert(0, ROOT)
 
 METRIC = "tau00 solves/s at N=2160 c128: mixed vs plain FP64 at <=1e-10 rel err; %peak"
 N_ENERGIES = 31
-# DRAM bytes (read + write) per tc_update_kernel launch of this workload: the ncu capture of a
-# 4-job launch at k = 320 (profiles/tc_update_contour2160_e4.md) measured 13.45 B per trailing-block
+# DRAM bytes (read + write) of the trailing update per elimination step of this workload (the
+# update of the next diagonal tile plus the interior launch): the ncu capture of a 24-job interior
+# launch at k = 192 (profiles/tc_update_contour2160_e24.md) measured 17.4 B per trailing-block
 # entry; scaled to 31 jobs and the average trailing block over the 34 steps (1.476e6 entries).
-TRAFFIC_PER_LAUNCH = 615.3e6
+TRAFFIC_PER_LAUNCH = 796.1e6
 
 
 def algorithmic_flops(N: int, b: int, L: int) -> float:
@@ -487,7 +488,7 @@ def main():
                          "bound": "tensor",
                          "achieved": achieved, "unit": "TFLOP/s",
                          "peak": tf32_peak, "frac": (achieved / tf32_peak) if achieved else None,
-                         "traffic": TRAFFIC_PER_LAUNCH,
+                         "traffic": TRAFFIC_PER_LAUNCH, "traffic_unit": "bytes per elimination step",
                          "launches_timed": k_launches, "device_ms": k_ms, "algorithmic_flops": k_flops,
                          "flops_note": "algorithmic complex FLOPs 8 m n kb; the tensor pipe executes 3x "
                                        "that (hi*hi + hi*lo + lo*hi)",

@@ -442,9 +442,10 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
 constexpr int kResK = 8;       // K per stage
 constexpr int kResStages = 3;
 
+constexpr int kResThreads = 128;  // four CTAs per SM, so a round on a few jobs still spans the GPU
 template <int BC>
 __host__ __device__ constexpr int residual_rows() {
-  return 256 * 16 / BC;
+  return kResThreads * 16 / BC;
 }
 template <int BC>
 __host__ __device__ constexpr int residual_smem_bytes() {
@@ -456,11 +457,11 @@ __host__ __device__ constexpr int residual_smem_bytes() {
 template <int BC> struct ResTile { static constexpr int RPT = 2, NCT = 8; };
 
 template <int BC>
-__global__ void __launch_bounds__(256, 2) residual_kernel(const JobDev *__restrict__ jobs) {
+__global__ void __launch_bounds__(kResThreads, 4) residual_kernel(const JobDev *__restrict__ jobs) {
   constexpr int RPT = ResTile<BC>::RPT, NCT = ResTile<BC>::NCT;
   constexpr int ROWS = residual_rows<BC>();  // rows per CTA
   constexpr int RG = ROWS / RPT;             // row groups
-  static_assert(RG * (BC / NCT) == 256, "residual thread layout");
+  static_assert(RG * (BC / NCT) == kResThreads, "residual thread layout");
   const JobDev &J = jobs[blockIdx.y];
   if (converged(J) || J.inactive) return;
   const int N = J.N, ld = J.ld, b = J.b;
@@ -478,13 +479,13 @@ __global__ void __launch_bounds__(256, 2) residual_kernel(const JobDev *__restri
   // columns [k0, k0 + kResK) of M (rows of the CTA) and rows [k0, k0 + kResK) of X into stage st;
   // entries past N or b read as zero
   auto stage = [&](int k0, int st) {
-    for (int e = tid; e < kResK * ROWS; e += 256) {
+    for (int e = tid; e < kResK * ROWS; e += kResThreads) {
       const int kk = e / ROWS, rr = e - kk * ROWS;
       const int gk = k0 + kk, grr = row0 + rr;
       if (gk < N && grr < N) cp_async16(&Ms[st][kk][rr], M + (size_t)grr + (size_t)gk * ld);
       else Ms[st][kk][rr] = zero;
     }
-    for (int e = tid; e < kResK * BC; e += 256) {
+    for (int e = tid; e < kResK * BC; e += kResThreads) {
       const int kk = e % kResK, c = e / kResK;
       const int gk = k0 + kk;
       if (c < b && gk < N) cp_async16(&Xs[st][kk][c], X + (size_t)gk + (size_t)c * ld);
@@ -820,13 +821,15 @@ cudaError_t launch_refine_round(FactorKind fk, const JobDev *jobs, int njobs, in
     if ((e0 = cudaFuncSetAttribute(residual_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm16)) !=
         cudaSuccess)
       return e0;
-    residual_kernel<16><<<dim3((max_N + residual_rows<16>() - 1) / residual_rows<16>(), njobs), 256, sm16, s>>>(jobs);
+    residual_kernel<16><<<dim3((max_N + residual_rows<16>() - 1) / residual_rows<16>(), njobs), kResThreads, sm16,
+                          s>>>(jobs);
   } else {
     constexpr int sm32 = residual_smem_bytes<32>();
     if ((e0 = cudaFuncSetAttribute(residual_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm32)) !=
         cudaSuccess)
       return e0;
-    residual_kernel<32><<<dim3((max_N + residual_rows<32>() - 1) / residual_rows<32>(), njobs), 256, sm32, s>>>(jobs);
+    residual_kernel<32><<<dim3((max_N + residual_rows<32>() - 1) / residual_rows<32>(), njobs), kResThreads, sm32,
+                          s>>>(jobs);
   }
   if (launches) *launches += 1;
   const cudaError_t e = fk == kFactorFP64 ? sweep_solve<double2>(jobs, njobs, b, max_N, 1, info, s, launches, false, nullptr)
