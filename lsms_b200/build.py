@@ -28,7 +28,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
     os.makedirs(LIB_DIR, exist_ok=True)
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
     deps = srcs + [os.path.join(CSRC, "common.cuh"), os.path.join(CSRC, "cplx.cuh"), os.path.join(CSRC, "gj.cuh"),
-                   os.path.join(CSRC, "cluster.cuh"),
+                   os.path.join(CSRC, "cluster.cuh"), os.path.join(CSRC, "umma.cuh"),
                    os.path.join(HERE, "..", "include", "b200tau.h")]
     if (not force and os.path.exists(LIB_PATH)
             and all(os.path.getmtime(LIB_PATH) >= os.path.getmtime(d) for d in deps)):

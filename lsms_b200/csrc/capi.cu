@@ -367,10 +367,11 @@ int encode_factor_map(b200tau_ctx *ctx, int ld, int slots) {
                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(ctx, B200TAU_ERR_CUDA, "cuTensorMapEncodeTiled (F) failed (%d)", (int)r);
-  // the sweeps' operand units: 64 complex rows x 32 columns
-  const cuuint32_t ubox[3] = {128, 32, 1};
+  // the sweeps' operand units: 32 real rows x 32 columns per box, in the tensor core's MN-major
+  // TF32 layout (128-byte swizzle on 32-byte atoms)
+  const cuuint32_t ubox[3] = {32, 32, 1};
   r = enc(&ctx->tc.tFu, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, ctx->d_F, dims, strides, ubox, estr,
-          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(ctx, B200TAU_ERR_CUDA, "cuTensorMapEncodeTiled (F units) failed (%d)", (int)r);
   return B200TAU_OK;

@@ -62,6 +62,9 @@ __device__ __forceinline__ void st_remote(unsigned addr, float4 v) {
                "f"(v.w)
                : "memory");
 }
+__device__ __forceinline__ void st_remote_f32(unsigned addr, float v) {
+  asm volatile("st.shared::cluster.f32 [%0], %1;" ::"r"(addr), "f"(v) : "memory");
+}
 
 __device__ __forceinline__ void mbar_init(unsigned long long *b, unsigned count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(b)), "r"(count) : "memory");
@@ -85,6 +88,17 @@ __device__ __forceinline__ bool mbar_try_cluster(unsigned long long *b, unsigned
   unsigned ok;
   asm volatile(
       "{ .reg .pred p; mbarrier.try_wait.parity.acquire.cluster.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
+      : "=r"(ok)
+      : "r"(smem_u32(b)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// The same with acquire at CTA scope, for barriers that only this CTA's threads, TMA loads or
+// tensor-core commits complete.
+__device__ __forceinline__ bool mbar_try_cta(unsigned long long *b, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2; selp.u32 %0, 1, 0, p; }"
       : "=r"(ok)
       : "r"(smem_u32(b)), "r"(parity)
       : "memory");

@@ -123,7 +123,7 @@ struct KernelTimer {
 struct TcMaps {
   CUtensorMap tA_hi, tA_lo, tB_hi, tB_lo;
   CUtensorMap tF;   // the wave's FP32 factor slots as floats {2 ld, ld, slots}, box {128, 64, 1}
-  CUtensorMap tFu;  // the same slots, box {128, 32, 1}: one 64-row x 32-column sweep unit
+  CUtensorMap tFu;  // the same slots, box {32, 32, 1}, MN-major TF32 swizzle: a quarter of a sweep unit
   float *a_hi = nullptr, *a_lo = nullptr, *b_hi = nullptr, *b_lo = nullptr;
   size_t a_slot = 0, b_slot = 0;  // floats per slot
 };
