@@ -405,7 +405,8 @@ __device__ __forceinline__ void split_unit(float *a, float *lo, int ncol) {
     float4 h = make_float4(0.f, 0.f, 0.f, 0.f), l = h;
     if (live) {
       const float4 x = A4[f];
-      h = make_float4(um::tf32_round(x.x), um::tf32_round(x.y), um::tf32_round(x.z), um::tf32_round(x.w));
+      h = make_float4(um::tf32_round_int(x.x), um::tf32_round_int(x.y), um::tf32_round_int(x.z),
+                      um::tf32_round_int(x.w));
       l = make_float4(x.x - h.x, x.y - h.y, x.z - h.z, x.w - h.w);
     }
     A4[f] = h;
@@ -501,6 +502,37 @@ __device__ __forceinline__ void acc_read(const FlowSmem &S, uint32_t tmem, int a
   }
 }
 
+// R (or Y) tile update from accumulator `nt`: rows row0 + m / 2 in [lo, hi) of the resident
+// tile `tile` (FP32, column-major) minus the product.  False, for every compute thread, when the
+// wait for the accumulator ran out.
+__device__ __forceinline__ bool tile_update(const FlowSmem &S, uint32_t tmem, int nt, float *tile, int row0, int lo,
+                                            int hi, const int *conv) {
+  if (!cta_wait<false>(S.acc_full + (nt & 1), (nt >> 1) & 1, conv)) return false;
+  um::fence_after();
+  float v[8];
+  acc_read(S, tmem, nt & 1, v);
+  const int w = threadIdx.x >> 5, m = 32 * (w & 3) + (threadIdx.x & 31), c0 = 8 * ((w >> 2) & 1);
+  const int gr = row0 + (m >> 1);
+  if (gr >= lo && gr < hi) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) tile[(c0 + i) * 128 + m] -= v[i];
+  }
+  return true;
+}
+// A tile update left for later: it runs after the next tile's units are split, so the tile's MMAs
+// overlap that split instead of stalling the compute warps.  Tiles on the block chain (the next
+// block's tile, the D multiply) are never deferred.
+struct Deferred {
+  int nt, row0, lo, hi;
+  float *tile;
+  __device__ bool flush(const FlowSmem &S, uint32_t tmem, const int *conv) {
+    if (nt < 0) return true;
+    const bool ok = tile_update(S, tmem, nt, tile, row0, lo, hi, conv);
+    nt = -1;
+    return ok;
+  }
+};
+
 // Grid (cs, njobs), cluster (cs, 1, 1), 320 threads: 8 compute warps, the producer warp and the
 // MMA warp.
 // Refinement rounds only (the initial solve has B = 0 above the central block).  own_max:
@@ -544,10 +576,13 @@ __global__ void __launch_bounds__(kBlock, 1)
       issue_units(it, S, tmem, conv);
     __syncwarp();
   } else {
-    int u = 0, nt = 0;  // units consumed, tiles finished
+    int u = 0, nt = 0;  // units consumed, tiles started
     bool ok = true;
+    Deferred dq{-1};
     for (int j = -1; j < nsteps && ok; ++j) {
       if (j >= 0) {
+        ok = dq.flush(S, tmem, conv);  // its MMAs read the operand that this step overwrites
+        if (!ok) break;
         ok = cta_wait<true>(S.full + (j & nsm), (j >> lns) & 1, conv);  // Y_j is in slot j % ns
         if (!ok) break;
         if (!it.fin && it.j == j) build_b(S.bstep, S.slots + (j & nsm) * kTileElems, min(64, n - 64 * j));
@@ -560,7 +595,7 @@ __global__ void __launch_bounds__(kBlock, 1)
         const bool dk = it.d;
         float2 *Rt = S.tiles + (t >> lcs) * kTileElems;
         if (dk) {
-          compute_sync();  // tile j + 1 is updated
+          compute_sync();  // tile j + 1 is updated (its update is never deferred)
           build_b(S.bd, Rt, min(64, n - 64 * t));
         }
         bool last;
@@ -570,21 +605,23 @@ __global__ void __launch_bounds__(kBlock, 1)
           last = !it.same_tile(j, t, dk);
           unit_split(S, u++, ncol, conv);
         } while (!last);
-        ok = cta_wait<false>(S.acc_full + (nt & 1), (nt >> 1) & 1, conv);
-        if (!ok) break;
-        um::fence_after();
-        float v[8];
-        acc_read(S, tmem, nt & 1, v);
-        ++nt;
+        const int me = nt++;
         if (!dk) {
           // R[tile t] -= A21_j Y_j for the rows below the block
-          const int k = 64 * j, kb = min(64, n - k), gr = 64 * t + r;
-          if (gr >= k + kb && gr < N) {
-            float *Rf = reinterpret_cast<float *>(Rt);
-#pragma unroll
-            for (int i = 0; i < 8; ++i) Rf[(c0 + i) * 128 + m] -= v[i];
+          const int lo = 64 * j + min(64, n - 64 * j);
+          float *Rf = reinterpret_cast<float *>(Rt);
+          if (t != j + 1) {
+            ok = dq.flush(S, tmem, conv);
+            dq = Deferred{me, 64 * t, lo, N, Rf};
+          } else {
+            ok = tile_update(S, tmem, me, Rf, 64 * t, lo, N, conv);
           }
         } else {
+          ok = cta_wait<false>(S.acc_full + (me & 1), (me >> 1) & 1, conv);
+          if (!ok) break;
+          um::fence_after();
+          float v[8];
+          acc_read(S, tmem, me & 1, v);
           // Y_(j+1) = D_(j+1) R_(j+1): into J.Y and into slot (j + 1) % ns of every CTA
           const int jd = j + 1, kd = 64 * jd, kbd = min(64, n - kd), slot = jd & nsm;
           if (jd >= ns) ok = cta_wait<true>(S.empty + slot, ((jd >> lns) - 1) & 1, conv);
@@ -609,6 +646,7 @@ __global__ void __launch_bounds__(kBlock, 1)
         }
       }
     }
+    if (ok) ok = dq.flush(S, tmem, conv);
     if (ok) {
       compute_sync();  // every tile update is done
       // the central rows of R for the Schur solve
@@ -640,8 +678,7 @@ __global__ void __launch_bounds__(kBlock, 1)
   const FlowSmem S(aligned_smem(sm_raw), L);
   const int n = J.n, ld = J.ld, b = J.b, ns = L.ns, nsm = ns - 1, lns = __ffs(ns) - 1;
   int *conv = J.conv;
-  const int tid = threadIdx.x, warp = tid >> 5, m = 32 * (warp & 3) + (tid & 31), r = m >> 1;
-  const int c0 = 8 * ((warp >> 2) & 1);
+  const int tid = threadIdx.x;
   const int kstart = n > 0 ? ((n - 1) / 64) * 64 : 0;  // last block
   const int nsteps = n > 0 ? kstart / 64 + 2 : 1;       // central block + blocks kstart .. 0
   const int p0 = kstart / 64 + 1;
@@ -693,7 +730,10 @@ __global__ void __launch_bounds__(kBlock, 1)
   } else {
     int u = 0, nt = 0;
     bool ok = true;
+    Deferred dq{-1};
     for (int s = 0; s < nsteps && ok; ++s) {
+      ok = dq.flush(S, tmem, conv);  // its MMAs read the operand that this step overwrites
+      if (!ok) break;
       ok = cta_wait<true>(S.full + (s & nsm), (s >> lns) & 1, conv);  // block s is in slot s % ns
       if (!ok) break;
       const int ks = s == 0 ? n : kstart - 64 * (s - 1);
@@ -711,20 +751,16 @@ __global__ void __launch_bounds__(kBlock, 1)
           last = !it.same_tile(s, t);
           unit_split(S, u++, ncol, conv);
         } while (!last);
-        ok = cta_wait<false>(S.acc_full + (nt & 1), (nt >> 1) & 1, conv);
-        if (!ok) break;
-        um::fence_after();
-        float v[8];
-        acc_read(S, tmem, nt & 1, v);
-        ++nt;
+        const int me = nt++;
         // Y[tile t] -= W[tile t, block s] Y_s for the rows above the block
         float2 *Yt = S.tiles + (t >> lcs) * kTileElems;
-        if (64 * t + r < ks) {
-          float *Yf = reinterpret_cast<float *>(Yt);
-#pragma unroll
-          for (int i = 0; i < 8; ++i) Yf[(c0 + i) * 128 + m] -= v[i];
-        }
-        if (t == tnext) {
+        float *Yf = reinterpret_cast<float *>(Yt);
+        if (t != tnext) {
+          ok = dq.flush(S, tmem, conv);
+          dq = Deferred{me, 64 * t, 0, ks, Yf};
+        } else {
+          ok = tile_update(S, tmem, me, Yf, 64 * t, 0, ks, conv);
+          if (!ok) break;
           // the rows of block s + 1 are final: X (+)= Y there, and the block to every CTA
           const int kn = 64 * tnext, kbn = min(64, n - kn), slot = (s + 1) & nsm;
           if (s + 1 >= ns)
@@ -763,6 +799,7 @@ __global__ void __launch_bounds__(kBlock, 1)
         }
       }
     }
+    if (ok) ok = dq.flush(S, tmem, conv);
     if (!ok && tid == 0) job_abort(conv);
   }
   flow_teardown(S, tmem);

@@ -78,5 +78,11 @@ __device__ __forceinline__ float tf32_round(float x) {
   return __uint_as_float(r);
 }
 
+// The same value computed on the integer pipe, for finite inputs: half a TF32 unit in the last
+// place added to the magnitude bits, then the 13 bits below the TF32 mantissa cleared.
+__device__ __forceinline__ float tf32_round_int(float x) {
+  return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xffffe000u);
+}
+
 }  // namespace um
 }  // namespace b200
