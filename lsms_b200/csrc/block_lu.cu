@@ -456,16 +456,42 @@ __host__ __device__ constexpr int residual_smem_bytes() {
 // loads per 16 complex FMAs.
 template <int BC> struct ResTile { static constexpr int RPT = 2, NCT = 8; };
 
+// The jobs of a wave still refining: list[0] = their number, list[1..] their indices in order.
+// One warp.
+__global__ void active_list_kernel(const JobDev *__restrict__ jobs, int njobs, int *list) {
+  const int lane = threadIdx.x;
+  int count = 0;
+  for (int base = 0; base < njobs; base += 32) {
+    const int w = base + lane;
+    const bool a = w < njobs && !converged(jobs[w]) && !jobs[w].inactive;
+    const unsigned mask = __ballot_sync(0xffffffffu, a);
+    if (a) list[1 + count + __popc(mask & ((1u << lane) - 1u))] = w;
+    count += __popc(mask);
+  }
+  if (lane == 0) list[0] = count;
+}
+
+// Without a list: grid (jobs, row blocks), converged jobs leave at once.  With `active` (from
+// active_list_kernel): a 1-D grid whose first count x rowblocks CTAs take (active job i % count,
+// row block i / count), so the jobs still refining spread evenly over the SMs; the rest leave.
 template <int BC>
-__global__ void __launch_bounds__(kResThreads, 4) residual_kernel(const JobDev *__restrict__ jobs) {
+__global__ void __launch_bounds__(kResThreads, 4) residual_kernel(const JobDev *__restrict__ jobs,
+                                                                  const int *__restrict__ active, int rowblocks) {
   constexpr int RPT = ResTile<BC>::RPT, NCT = ResTile<BC>::NCT;
   constexpr int ROWS = residual_rows<BC>();  // rows per CTA
   constexpr int RG = ROWS / RPT;             // row groups
   static_assert(RG * (BC / NCT) == kResThreads, "residual thread layout");
-  const JobDev &J = jobs[blockIdx.y];
+  int jw = blockIdx.x, rb = blockIdx.y;
+  if (active != nullptr) {
+    const int cnt = active[0], i = blockIdx.x;
+    if (i >= cnt * rowblocks) return;
+    jw = active[1 + i % cnt];
+    rb = i / cnt;
+  }
+  const JobDev &J = jobs[jw];
   if (converged(J) || J.inactive) return;
   const int N = J.N, ld = J.ld, b = J.b;
-  const int row0 = blockIdx.x * ROWS;
+  const int row0 = rb * ROWS;
   if (row0 >= N) return;
   extern __shared__ __align__(16) unsigned char rsm[];
   double2(*Ms)[kResK][ROWS] = reinterpret_cast<double2(*)[kResK][ROWS]>(rsm);
@@ -669,16 +695,18 @@ cudaError_t eliminate_impl(const JobDev *jobs, int njobs, int max_n, int max_N, 
 
 template <typename T>
 cudaError_t sweep_solve(const JobDev *jobs, int njobs, int b, int max_N, int mode, int *info, cudaStream_t s,
-                        long *launches, bool fp32, const CUtensorMap *fmap) {
+                        long *launches, bool fp32, const CUtensorMap *fmap, int active_hint = 0) {
   const FactorKind fk = sizeof(T) == sizeof(double2) ? kFactorFP64 : kFactorFP32;
   cudaError_t e;
   // forward (skipped for the initial solve: B is zero above the central block)
   if (mode == 1) {
-    if ((e = launch_sweep(fk, jobs, njobs, b, max_N, true, mode, fp32, fmap, s)) != cudaSuccess) return e;
+    if ((e = launch_sweep(fk, jobs, njobs, b, max_N, true, mode, fp32, fmap, s, active_hint)) != cudaSuccess)
+      return e;
     if (launches) *launches += 1;
   }
   schur_solve_kernel<T><<<njobs, 256, 0, s>>>(jobs, mode, info);
-  if ((e = launch_sweep(fk, jobs, njobs, b, max_N, false, mode, fp32, fmap, s)) != cudaSuccess) return e;
+  if ((e = launch_sweep(fk, jobs, njobs, b, max_N, false, mode, fp32, fmap, s, active_hint)) != cudaSuccess)
+    return e;
   if (launches) *launches += 2;
   return cudaSuccess;
 }
@@ -748,6 +776,18 @@ __global__ void fallback_prepare_kernel(const JobDev *__restrict__ jobs, JobDev 
   out[w] = J;
 }
 
+// The re-solve gate of a mixed wave: the graph's conditional body (the FP64 re-solve) runs only
+// when some record has not converged.
+__global__ void fallback_gate_kernel(const JobDev *__restrict__ jobs, int njobs, cudaGraphConditionalHandle h) {
+  int any = 0;
+  for (int w = threadIdx.x; w < njobs; w += blockDim.x) {
+    const int *c = jobs[w].conv;
+    any |= (c == nullptr || *c != kConverged) ? 1 : 0;
+  }
+  any = __syncthreads_or(any);
+  if (threadIdx.x == 0) cudaGraphSetConditional(h, any ? 1u : 0u);
+}
+
 // F = M (FP64, N x N) for the active records; CTAs (blockIdx.x) stride over the columns of job
 // blockIdx.y
 __global__ void __launch_bounds__(256) copy_jobs_to_factor_kernel(const JobDev *__restrict__ jobs) {
@@ -767,6 +807,18 @@ cudaError_t launch_fallback_prepare(const JobDev *jobs, JobDev *out, int njobs, 
   copy_jobs_to_factor_kernel<<<dim3(std::min(max_N, 64), njobs), 256, 0, s>>>(out);
   if (launches) *launches += 2;
   return cudaGetLastError();
+}
+
+cudaError_t add_fallback_gate_node(cudaGraph_t g, cudaGraphNode_t *node, const JobDev *jobs, int njobs,
+                                   cudaGraphConditionalHandle h) {
+  cudaKernelNodeParams kp = {};
+  void *args[3] = {&jobs, &njobs, &h};
+  kp.func = reinterpret_cast<void *>(fallback_gate_kernel);
+  kp.gridDim = dim3(1);
+  kp.blockDim = dim3(256);
+  kp.sharedMemBytes = 0;
+  kp.kernelParams = args;
+  return cudaGraphAddKernelNode(node, g, nullptr, 0, &kp);
 }
 
 cudaError_t launch_copy_to_factor(FactorKind fk, const double2 *M, void *F, int n, int ld, cudaStream_t s) {
@@ -811,29 +863,32 @@ cudaError_t launch_refine_begin(FactorKind fk, const JobDev *jobs, int njobs, in
   return e != cudaSuccess ? e : cudaGetLastError();
 }
 
+template <int BC>
+cudaError_t launch_residual(const JobDev *jobs, int njobs, int max_N, int *active, cudaStream_t s) {
+  constexpr int sm = residual_smem_bytes<BC>();
+  const cudaError_t e = cudaFuncSetAttribute(residual_kernel<BC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (e != cudaSuccess) return e;
+  const int rowblocks = (max_N + residual_rows<BC>() - 1) / residual_rows<BC>();
+  if (active) {
+    active_list_kernel<<<1, 32, 0, s>>>(jobs, njobs, active);
+    residual_kernel<BC><<<njobs * rowblocks, kResThreads, sm, s>>>(jobs, active, rowblocks);
+  } else {
+    residual_kernel<BC><<<dim3(njobs, rowblocks), kResThreads, sm, s>>>(jobs, nullptr, rowblocks);
+  }
+  return cudaGetLastError();
+}
+
 cudaError_t launch_refine_round(FactorKind fk, const JobDev *jobs, int njobs, int max_n, int max_N, int b,
                                 bool check, int *info, cudaStream_t s, long *launches, bool fp32_sweep,
-                                const CUtensorMap *fmap) {
+                                const CUtensorMap *fmap, int active_hint, int *active) {
   (void)max_n;
-  cudaError_t e0;
-  if (b <= 16) {
-    constexpr int sm16 = residual_smem_bytes<16>();
-    if ((e0 = cudaFuncSetAttribute(residual_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm16)) !=
-        cudaSuccess)
-      return e0;
-    residual_kernel<16><<<dim3((max_N + residual_rows<16>() - 1) / residual_rows<16>(), njobs), kResThreads, sm16,
-                          s>>>(jobs);
-  } else {
-    constexpr int sm32 = residual_smem_bytes<32>();
-    if ((e0 = cudaFuncSetAttribute(residual_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm32)) !=
-        cudaSuccess)
-      return e0;
-    residual_kernel<32><<<dim3((max_N + residual_rows<32>() - 1) / residual_rows<32>(), njobs), kResThreads, sm32,
-                          s>>>(jobs);
-  }
-  if (launches) *launches += 1;
+  const cudaError_t e0 = b <= 16 ? launch_residual<16>(jobs, njobs, max_N, active, s)
+                                 : launch_residual<32>(jobs, njobs, max_N, active, s);
+  if (e0 != cudaSuccess) return e0;
+  if (launches) *launches += active ? 2 : 1;
   const cudaError_t e = fk == kFactorFP64 ? sweep_solve<double2>(jobs, njobs, b, max_N, 1, info, s, launches, false, nullptr)
-                                           : sweep_solve<float2>(jobs, njobs, b, max_N, 1, info, s, launches, fp32_sweep, fmap);
+                                           : sweep_solve<float2>(jobs, njobs, b, max_N, 1, info, s, launches, fp32_sweep, fmap,
+                                                                 active_hint);
   if (e != cudaSuccess) return e;
   if (check) {
     converge_check_kernel<<<njobs, 256, 0, s>>>(jobs, kRefineTol);

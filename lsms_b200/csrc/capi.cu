@@ -69,12 +69,11 @@ struct b200tau_ctx {
   int slots = 0;
   JobDev *d_jobs = nullptr;
   int jobs_cap = 0;
-  JobDev *d_jobs2 = nullptr;  // the jobs still refining after compaction (at most `slots`)
-  int jobs2_cap = 0;
-  JobDev *d_jobs3 = nullptr;  // their FP64 re-solve records
+  JobDev *d_jobs3 = nullptr;  // the FP64 re-solve records of a mixed wave
   int jobs3_cap = 0;
-  int *d_info = nullptr;   // 2 x slots: the wave's jobs, then the compacted list
+  int *d_info = nullptr;   // 2 x slots: the wave's jobs, then their FP64 re-solve records
   int *d_conv = nullptr;   // per slot: refinement converged
+  int *d_active = nullptr;  // slots + 1: the jobs still refining (residual launches)
   double *d_cnorm = nullptr;  // per slot: relative size of the last refinement correction
   int *d_err = nullptr;    // device error flags
   double2 *d_out = nullptr;
@@ -113,6 +112,17 @@ struct b200tau_ctx {
   TcMaps tc;
   float *d_pack = nullptr;
   int tc_ld = 0, tc_slots = 0;
+  // the mixed path's FP64 re-solve as a graph with a conditional body (ensure_fallback_graph)
+  cudaStream_t cap_stream = nullptr;
+  cudaGraph_t fb_graph = nullptr;
+  cudaGraphExec_t fb_exec = nullptr;
+  std::vector<long long> fb_key;
+  // converged flags after the first refinement rounds, copied back without a wait: the next
+  // call's estimate of how many jobs the later rounds' sweeps serve
+  int *h_hint = nullptr;
+  cudaEvent_t hint_ev = nullptr;
+  bool hint_pending = false;
+  int h_hint_cap = 0, hint_n = 0, active_hint = 0;
 };
 
 namespace {
@@ -171,12 +181,14 @@ int ensure_workspace(b200tau_ctx *ctx, int ld, int slots, const Plan &p) {
   cudaFree(ctx->d_vec);
   cudaFree(ctx->d_info);
   cudaFree(ctx->d_conv);
+  cudaFree(ctx->d_active);
   cudaFree(ctx->d_cnorm);
   ctx->d_M = nullptr;
   ctx->d_F = nullptr;
   ctx->d_vec = nullptr;
   ctx->d_info = nullptr;
   ctx->d_conv = nullptr;
+  ctx->d_active = nullptr;
   ctx->d_cnorm = nullptr;
   const size_t m_el = std::max(m_need, ctx->m_elems);
   const size_t f_b = std::max(f_need, ctx->f_bytes);
@@ -187,6 +199,7 @@ int ensure_workspace(b200tau_ctx *ctx, int ld, int slots, const Plan &p) {
   CK(cudaMalloc(&ctx->d_vec, v_el * sl * sizeof(double2)));
   CK(cudaMalloc(&ctx->d_info, sizeof(int) * 2 * sl));
   CK(cudaMalloc(&ctx->d_conv, sizeof(int) * sl));
+  CK(cudaMalloc(&ctx->d_active, sizeof(int) * (sl + 1)));
   CK(cudaMalloc(&ctx->d_cnorm, sizeof(double) * sl));
   ctx->m_elems = m_el;
   ctx->f_bytes = f_b;
@@ -405,17 +418,9 @@ double trailing_flops(const std::vector<JobDev> &h) {
 }
 
 
-int ensure_jobs2(b200tau_ctx *ctx, int n) {
-  if (n <= ctx->jobs2_cap) return B200TAU_OK;
-  cudaFree(ctx->d_jobs2);
-  ctx->d_jobs2 = nullptr;
-  CK(cudaMalloc(&ctx->d_jobs2, sizeof(JobDev) * n));
-  ctx->jobs2_cap = n;
-  return B200TAU_OK;
-}
-
-// Refinement rounds run on every job of the wave until this many are done.
-constexpr int kCompactAfterRounds = 2;
+// Refinement rounds after which the jobs still refining are copied back (without a wait) as the
+// next call's estimate of how many the later rounds' sweeps serve.
+constexpr int kHintAfterRounds = 2;
 
 // FP64 storage for re-solving any job of a mixed wave (one ld x ld block per slot) and the
 // device counter of re-solved jobs.
@@ -424,6 +429,13 @@ int ensure_fallback(b200tau_ctx *ctx, int ld) {
   if (!ctx->d_fbcount) {
     CK(cudaMalloc(&ctx->d_fbcount, sizeof(int)));
     CK(cudaMemsetAsync(ctx->d_fbcount, 0, sizeof(int), ctx->stream));
+  }
+  if (ctx->jobs3_cap < ctx->slots) {
+    CK(cudaStreamSynchronize(ctx->stream));
+    cudaFree(ctx->d_jobs3);
+    ctx->d_jobs3 = nullptr;
+    CK(cudaMalloc(&ctx->d_jobs3, sizeof(JobDev) * ctx->slots));
+    ctx->jobs3_cap = ctx->slots;
   }
   if (ctx->d_ffb && need <= ctx->ffb_elems) return B200TAU_OK;
   CK(cudaStreamSynchronize(ctx->stream));
@@ -434,84 +446,122 @@ int ensure_fallback(b200tau_ctx *ctx, int ld) {
   return B200TAU_OK;
 }
 
-// Initial solve, `p.steps` refinement rounds (converged jobs skip the later ones, and are dropped
-// from the launches after kCompactAfterRounds), tau00_l.  `h` are the wave's records as uploaded
-// to ctx->d_jobs.
+void drop_fallback_graph(b200tau_ctx *ctx) {
+  if (ctx->fb_exec) cudaGraphExecDestroy(ctx->fb_exec);
+  if (ctx->fb_graph) cudaGraphDestroy(ctx->fb_graph);
+  ctx->fb_exec = nullptr;
+  ctx->fb_graph = nullptr;
+  ctx->fb_key.clear();
+}
+
+// The FP64 re-solve of a mixed wave as one graph: a gate kernel, then a conditional node whose
+// body - the re-solve records (converged jobs inactive), FP64 block elimination, the FP64
+// refinement rounds and tau00 - runs only when some job did not converge.  So the host queues
+// the re-solve without waiting for the refinement's outcome, and a wave whose jobs all converged
+// pays one small launch for it.  Built on first use and again when the wave's shape or buffers
+// change (the records themselves are read from device memory when the graph runs).
+int ensure_fallback_graph(b200tau_ctx *ctx, int nw, int maxn, int maxN, int ld, int b, int ns, int kkrsz) {
+  const int steps = std::max(1, ctx->refine_steps[0]);
+  int *finfo = ctx->d_info + ctx->slots;
+  const std::vector<long long> key = {nw, maxn, maxN, ld, b, ns, kkrsz, steps, ctx->slots,
+                                      (long long)(uintptr_t)ctx->d_jobs, (long long)(uintptr_t)ctx->d_jobs3,
+                                      (long long)(uintptr_t)ctx->d_ffb, (long long)(uintptr_t)ctx->d_info,
+                                      (long long)(uintptr_t)ctx->d_fbcount, (long long)(uintptr_t)ctx->d_err};
+  if (ctx->fb_exec && key == ctx->fb_key) return B200TAU_OK;
+  drop_fallback_graph(ctx);
+  if (!ctx->cap_stream) CK(cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking));
+  cudaGraph_t g = nullptr;
+  CK(cudaGraphCreate(&g, 0));
+  ctx->fb_graph = g;
+  cudaGraphConditionalHandle h;
+  CK(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+  cudaGraphNode_t gate = nullptr, cond = nullptr;
+  CK(add_fallback_gate_node(g, &gate, ctx->d_jobs, nw, h));
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeIf;
+  cp.conditional.size = 1;
+  CK(cudaGraphAddNode(&cond, g, &gate, 1, &cp));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  CK(cudaStreamBeginCaptureToGraph(ctx->cap_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+  cudaError_t e = launch_fallback_prepare(ctx->d_jobs, ctx->d_jobs3, nw, ctx->d_ffb, (size_t)ld * ld, maxN,
+                                          ctx->d_fbcount, ctx->cap_stream, nullptr);
+  if (e == cudaSuccess)
+    e = launch_eliminate(kFactorFP64, ctx->d_jobs3, nw, maxn, maxN, finfo, ctx->cap_stream, nullptr, nullptr,
+                         nullptr, ctx->d_err, true);
+  if (e == cudaSuccess)
+    e = launch_solve_refine(kFactorFP64, ctx->d_jobs3, nw, maxn, maxN, b, steps, ns, kkrsz, finfo,
+                            ctx->cap_stream, nullptr);
+  cudaGraph_t captured = nullptr;
+  const cudaError_t ec = cudaStreamEndCapture(ctx->cap_stream, &captured);
+  if (e == cudaSuccess) e = ec;
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    drop_fallback_graph(ctx);
+    return fail(ctx, B200TAU_ERR_CUDA, "capturing the FP64 re-solve: %s", cudaGetErrorString(e));
+  }
+  CK(cudaGraphInstantiate(&ctx->fb_exec, g, 0));
+  ctx->fb_key = key;
+  return B200TAU_OK;
+}
+
+// The previous call's count of jobs still refining after kHintAfterRounds rounds, once its copy
+// has landed (never waits for it).
+void refresh_active_hint(b200tau_ctx *ctx) {
+  if (!ctx->hint_pending) return;
+  const cudaError_t q = cudaEventQuery(ctx->hint_ev);
+  if (q == cudaErrorNotReady) {
+    if (cudaPeekAtLastError() == cudaErrorNotReady) cudaGetLastError();
+    return;
+  }
+  ctx->hint_pending = false;
+  if (q != cudaSuccess) return;
+  int active = 0;
+  for (int w = 0; w < ctx->hint_n; ++w) active += ctx->h_hint[w] == 0;
+  ctx->active_hint = active;
+}
+
+// Initial solve, `p.steps` refinement rounds (converged jobs skip the later ones: every launch
+// covers the wave and the kernels leave converged jobs at once), tau00_l, and the FP64 re-solve of
+// jobs that did not converge.  The host never waits inside the wave.  `h` are the wave's records
+// as uploaded to ctx->d_jobs.
 int run_refinement(b200tau_ctx *ctx, const std::vector<JobDev> &h, int nw, int maxn, int maxN, int b, int ns,
                    int kkrsz, const Plan &p, const CUtensorMap *fmap) {
   const bool fp32_sweep = p.fk == kFactorFP32 && ctx->mixed_sweep == B200TAU_SWEEP_FP32;
+  refresh_active_hint(ctx);
   CK(launch_refine_begin(p.fk, ctx->d_jobs, nw, maxn, maxN, b, ctx->d_info, ctx->stream, &ctx->launches,
                          fp32_sweep, fmap));
-  // The kernels skip converged jobs.  After kCompactAfterRounds rounds the host reads the converged
-  // flags once (the only wait inside a wave; the rest of the wave is queued right after it) and
-  // the remaining rounds run on the unconverged jobs alone, with launches sized for them.
-  const JobDev *cur = ctx->d_jobs;
-  int ncur = nw, cmaxn = maxn, cmaxN = maxN;
-  int *cur_info = ctx->d_info;
   for (int it = 0; it < p.steps; ++it) {
-    if (it == kCompactAfterRounds) {
-      std::vector<int> conv(nw);
-      CK(cudaMemcpyAsync(conv.data(), ctx->d_conv, sizeof(int) * nw, cudaMemcpyDeviceToHost, ctx->stream));
-      CK(cudaStreamSynchronize(ctx->stream));
-      std::vector<JobDev> keep;
-      cmaxn = cmaxN = 0;
-      for (int w = 0; w < nw; ++w)
-        if (!conv[w]) {
-          keep.push_back(h[w]);
-          cmaxn = std::max(cmaxn, h[w].n);
-          cmaxN = std::max(cmaxN, h[w].N);
-        }
-      if (keep.empty()) {  // every job converged: nothing left to refine or to re-solve
-        ncur = 0;
-        break;
+    const int hint = it >= kHintAfterRounds ? ctx->active_hint : 0;
+    CK(launch_refine_round(p.fk, ctx->d_jobs, nw, maxn, maxN, b, true, ctx->d_info, ctx->stream, &ctx->launches,
+                           fp32_sweep, fmap, hint, ctx->d_active));
+    if (it + 1 == kHintAfterRounds && p.steps > kHintAfterRounds && !ctx->hint_pending) {
+      if (ctx->h_hint_cap < nw) {  // (no copy into the old buffer is pending)
+        if (ctx->h_hint) cudaFreeHost(ctx->h_hint);
+        ctx->h_hint = nullptr;
+        ctx->h_hint_cap = 0;
+        CK(cudaMallocHost(&ctx->h_hint, sizeof(int) * nw));
+        ctx->h_hint_cap = nw;
       }
-      if ((int)keep.size() < nw) {
-        int rc = ensure_jobs2(ctx, ctx->slots);
-        if (rc) return rc;
-        CK(cudaMemcpyAsync(ctx->d_jobs2, keep.data(), sizeof(JobDev) * keep.size(), cudaMemcpyHostToDevice,
-                           ctx->stream));
-        cur = ctx->d_jobs2;
-        ncur = (int)keep.size();
-        cur_info = ctx->d_info + ctx->slots;  // the compacted list's own pivot flags
-      }
+      if (!ctx->hint_ev) CK(cudaEventCreateWithFlags(&ctx->hint_ev, cudaEventDisableTiming));
+      ctx->hint_n = nw;
+      CK(cudaMemcpyAsync(ctx->h_hint, ctx->d_conv, sizeof(int) * ctx->hint_n, cudaMemcpyDeviceToHost,
+                         ctx->stream));
+      CK(cudaEventRecord(ctx->hint_ev, ctx->stream));
+      ctx->hint_pending = true;
     }
-    CK(launch_refine_round(p.fk, cur, ncur, cmaxn, cmaxN, b, true, cur_info, ctx->stream, &ctx->launches,
-                           fp32_sweep, fmap));
   }
   CK(launch_refine_end(ctx->d_jobs, nw, ns, kkrsz, ctx->stream, &ctx->launches));
-  if (p.fk != kFactorFP32 || !ctx->fallback_on || ncur == 0) return B200TAU_OK;
-  {
-    // the second (and last) wait of a wave: when every job converged, none of the re-solve's
-    // launches is queued
-    std::vector<int> conv(nw);
-    CK(cudaMemcpyAsync(conv.data(), ctx->d_conv, sizeof(int) * nw, cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-    bool any = false;
-    for (int w = 0; w < nw; ++w) any = any || conv[w] != kConverged;
-    if (!any) return B200TAU_OK;
-  }
+  if (p.fk != kFactorFP32 || !ctx->fallback_on) return B200TAU_OK;
   // Jobs whose FP32-factor refinement did not converge (condition numbers beyond what FP32 block
   // factors can refine, e.g. energies next to the real axis) take the FP64 path instead: an FP64
   // copy of the unmodified M, FP64 block elimination, the FP64 refinement rounds, tau00 from X -
-  // the same kernels and arithmetic as a PREC_FP64 solve of the job.  The selection happens on the
-  // device (converged jobs become inactive records), so the host never waits inside a wave.
-  // (only the jobs still refining after the compaction can need it)
-  const int ld = h[0].ld;
-  int rc = ensure_fallback(ctx, ld);
-  if (rc || (rc = ensure_jobs2(ctx, ctx->slots))) return rc;
-  if (ctx->jobs3_cap < ctx->slots) {
-    cudaFree(ctx->d_jobs3);
-    ctx->d_jobs3 = nullptr;
-    CK(cudaMalloc(&ctx->d_jobs3, sizeof(JobDev) * ctx->slots));
-    ctx->jobs3_cap = ctx->slots;
-  }
-  int *finfo = ctx->d_info + ctx->slots;
-  CK(launch_fallback_prepare(cur, ctx->d_jobs3, ncur, ctx->d_ffb, (size_t)ld * ld, cmaxN, ctx->d_fbcount,
-                             ctx->stream, &ctx->launches));
-  CK(launch_eliminate(kFactorFP64, ctx->d_jobs3, ncur, cmaxn, cmaxN, finfo, ctx->stream, &ctx->launches, nullptr,
-                      nullptr, ctx->d_err, true));
-  CK(launch_solve_refine(kFactorFP64, ctx->d_jobs3, ncur, cmaxn, cmaxN, b, std::max(1, ctx->refine_steps[0]), ns,
-                         kkrsz, finfo, ctx->stream, &ctx->launches));
+  // the same kernels and arithmetic as a PREC_FP64 solve of the job.
+  int rc = ensure_fallback(ctx, h[0].ld);
+  if (rc || (rc = ensure_fallback_graph(ctx, nw, maxn, maxN, h[0].ld, b, ns, kkrsz))) return rc;
+  CK(cudaGraphLaunch(ctx->fb_exec, ctx->stream));
+  ctx->launches += 1;
   return B200TAU_OK;
 }
 
@@ -746,10 +796,10 @@ void b200tau_destroy(b200tau_ctx *ctx) {
   cudaFree(ctx->d_F);
   cudaFree(ctx->d_vec);
   cudaFree(ctx->d_jobs);
-  cudaFree(ctx->d_jobs2);
   cudaFree(ctx->d_jobs3);
   cudaFree(ctx->d_info);
   cudaFree(ctx->d_conv);
+  cudaFree(ctx->d_active);
   cudaFree(ctx->d_cnorm);
   cudaFree(ctx->d_err);
   cudaFree(ctx->d_out);
@@ -765,6 +815,10 @@ void b200tau_destroy(b200tau_ctx *ctx) {
   if (ctx->la.panel) cudaEventDestroy(ctx->la.panel);
   if (ctx->la.diag) cudaEventDestroy(ctx->la.diag);
   if (ctx->la.s2) cudaStreamDestroy(ctx->la.s2);
+  drop_fallback_graph(ctx);
+  if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
+  if (ctx->hint_ev) cudaEventDestroy(ctx->hint_ev);
+  if (ctx->h_hint) cudaFreeHost(ctx->h_hint);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }

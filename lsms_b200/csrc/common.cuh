@@ -182,15 +182,19 @@ cudaError_t launch_solve_refine(FactorKind fk, const JobDev *jobs, int njobs, in
 cudaError_t launch_refine_begin(FactorKind fk, const JobDev *jobs, int njobs, int max_n, int max_N, int b,
                                 int *info, cudaStream_t s, long *launches, bool fp32_sweep = false,
                                 const CUtensorMap *fmap = nullptr);
+// `active_hint` (> 0): about how many of the jobs are still refining, which sizes the dataflow
+// sweeps' clusters; the launches still cover all njobs, so any value is correct.  `active`
+// (njobs + 1 ints of device scratch, optional): the residual first lists the jobs still refining
+// there and spreads its CTAs over them alone.
 cudaError_t launch_refine_round(FactorKind fk, const JobDev *jobs, int njobs, int max_n, int max_N, int b,
                                 bool check, int *info, cudaStream_t s, long *launches, bool fp32_sweep = false,
-                                const CUtensorMap *fmap = nullptr);
+                                const CUtensorMap *fmap = nullptr, int active_hint = 0, int *active = nullptr);
 cudaError_t launch_refine_end(const JobDev *jobs, int njobs, int ns, int kkrsz, cudaStream_t s, long *launches);
 // One block sweep of the correction solve for all jobs, one thread-block cluster per job
 // (sweep.cu): forward (R -> Y over the D_k, A21_k factors) or backward (Y over the W_k factors,
 // X (+)= Y).  `fp32_arith` selects FP32 arithmetic on FP32 factors.  max_N bounds the jobs' N.
 cudaError_t launch_sweep(FactorKind fk, const JobDev *jobs, int njobs, int b, int max_N, bool forward, int mode,
-                         bool fp32_arith, const CUtensorMap *fmap, cudaStream_t s);
+                         bool fp32_arith, const CUtensorMap *fmap, cudaStream_t s, int active_hint = 0);
 // Cluster size of the sweeps for a wave of njobs (sweep.cu).
 int sweep_cluster_size(int njobs);
 // The dataflow sweeps for FP32 factors in FP32 arithmetic with b <= 16 (sweep_flow.cu), operand
@@ -198,7 +202,11 @@ int sweep_cluster_size(int njobs);
 // took the launch; false (and cudaSuccess) without a map or when the shape does not fit its
 // shared-memory layout, and the caller runs launch_sweep's step-synchronous kernels instead.
 cudaError_t launch_flow_sweep(const JobDev *jobs, int njobs, int b, int max_N, bool forward, int mode,
-                              const CUtensorMap *fmap, cudaStream_t s, bool *launched);
+                              const CUtensorMap *fmap, cudaStream_t s, bool *launched, int active_hint = 0);
+// Graph node of the mixed path's FP64 re-solve gate: sets `h` to 1 when any of the njobs records
+// has not converged (its conv word is not kConverged), else 0.
+cudaError_t add_fallback_gate_node(cudaGraph_t g, cudaGraphNode_t *node, const JobDev *jobs, int njobs,
+                                   cudaGraphConditionalHandle h);
 // Adjoint (adjoint.cu), FP64 factors: V = M^-1 from the block factors in F, then per LIZ site the
 // tau00 cotangent pull-back and d ln det M / d t (needs G in M, X refined, V).
 cudaError_t launch_inverse(const JobDev *jobs, int njobs, int max_n, int max_N, cudaStream_t s, long *launches);

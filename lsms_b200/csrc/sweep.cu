@@ -373,13 +373,13 @@ int sweep_cluster_size(int njobs) {
 }
 
 cudaError_t launch_sweep(FactorKind fk, const JobDev *jobs, int njobs, int b, int max_N, bool forward, int mode,
-                         bool fp32_arith, const CUtensorMap *fmap, cudaStream_t s) {
+                         bool fp32_arith, const CUtensorMap *fmap, cudaStream_t s, int active_hint) {
   if (njobs <= 0) return cudaSuccess;
   if (b < 1 || b > kMaxB || (forward && mode != 1)) return cudaErrorInvalidValue;
   if (fk == kFactorFP64) return sweep_b<double2, double2>(jobs, njobs, b, forward, mode, s);
   if (fp32_arith) {
     bool done = false;
-    const cudaError_t e = launch_flow_sweep(jobs, njobs, b, max_N, forward, mode, fmap, s, &done);
+    const cudaError_t e = launch_flow_sweep(jobs, njobs, b, max_N, forward, mode, fmap, s, &done, active_hint);
     if (e != cudaSuccess || done) return e;
     return sweep_b<float2, float2>(jobs, njobs, b, forward, mode, s);
   }

@@ -839,16 +839,19 @@ int active_clusters(const void *kern, int cs, int smem) {
 
 }  // namespace
 
-// Cluster size: the largest of 8, 4, 2, 1 whose layout fits and whose clusters for all jobs are
-// resident at once; else the smallest that fits (the jobs then run in waves).  Not launched
-// (*launched false) when no cluster size up to 8 holds the tiles in shared memory.
+// Cluster size: the largest of 8, 4, 2, 1 whose layout fits and whose clusters for all active jobs
+// (active_hint of them when given, else njobs) are resident at once; else the smallest that fits
+// (the jobs then run in waves).  Clusters of converged jobs leave at once, so the grid always
+// covers all njobs.  Not launched (*launched false) when no cluster size up to 8 holds the tiles in
+// shared memory.
 cudaError_t launch_flow_sweep(const JobDev *jobs, int njobs, int b, int max_N, bool forward, int mode,
-                              const CUtensorMap *fmap, cudaStream_t s, bool *launched) {
+                              const CUtensorMap *fmap, cudaStream_t s, bool *launched, int active_hint) {
   *launched = false;
   if (njobs <= 0 || b > kCols || max_N <= 0 || fmap == nullptr) return cudaSuccess;
   const int T = (max_N + 63) / 64;
   const void *kern = forward ? reinterpret_cast<const void *>(forward_flow_kernel)
                              : reinterpret_cast<const void *>(backward_flow_kernel);
+  const int want = active_hint > 0 && active_hint < njobs ? active_hint : njobs;
   int cs = 0, fallback = 0;
   for (int c = 8; c >= 1; c >>= 1) {
     const FlowLayout L = flow_layout(c, (T + c - 1) / c, forward);
@@ -856,7 +859,7 @@ cudaError_t launch_flow_sweep(const JobDev *jobs, int njobs, int b, int max_N, b
     fallback = c;
     const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L.total);
     if (e != cudaSuccess) return e;
-    if (active_clusters(kern, c, L.total) >= njobs) {
+    if (active_clusters(kern, c, L.total) >= want) {
       cs = c;
       break;
     }

@@ -129,6 +129,30 @@ def test_n2160_full_contour_mixed_vs_fp64(solver_factory, sweep):
     assert max(errs) <= TOL_MIXED, errs
 
 
+def test_mixed_resolves_unconverged_jobs_in_fp64(solver_factory):
+    """A mixed wave whose refinement stops before the convergence test can pass (one round) hands
+    every job to the FP64 re-solve, which the host queues without waiting for the outcome; its
+    results are the FP64 path's.  The next wave, with the full refinement, converges and re-solves
+    nothing."""
+    prob = W.config_n2160()
+    s = _solver(solver_factory, prob)
+    idx = [0, 7, 15, 30]
+    jobs = T.make_jobs([(0, i, 0, prob.energies[i]) for i in idx])
+    fp64 = s.solve_jobs(jobs, T.PREC_FP64)
+    s.set_refinement(T.PREC_MIXED, 1)
+    try:
+        forced = s.solve_jobs(jobs, T.PREC_MIXED)
+        assert s.last_fallback_count == len(idx)
+    finally:
+        s.set_refinement(T.PREC_MIXED, 6)
+    errs = [tau_err(prob, i, 0, forced[k], fp64[k]) for k, i in enumerate(idx)]
+    assert max(errs) <= TOL_FP64, errs
+    mixed = s.solve_jobs(jobs, T.PREC_MIXED)
+    assert s.last_fallback_count == 0
+    errs = [tau_err(prob, i, 0, mixed[k], fp64[k]) for k, i in enumerate(idx)]
+    assert max(errs) <= TOL_MIXED, errs
+
+
 def test_batched_equals_one_at_a_time(solver_factory):
     prob = W.make_problem("fcc", 6.82, 4, 3, W.semicircle_contour(-0.3, 0.7, 6), 21, n_species=2)
     s = _solver(solver_factory, prob)
