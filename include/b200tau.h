@@ -123,8 +123,12 @@ int b200tau_solve(b200tau_ctx *ctx, const b200tau_job *jobs, int njobs,
 
 /* As b200tau_solve, but tau00_l_dev is device memory and the call returns
  * once the work is enqueued on the context's stream (inputs already resident
- * from upload_tmat / set_atom).  Errors detected on the device are reported by
- * the next b200tau_sync. */
+ * from upload_tmat / set_atom).  When the jobs fit one wave (the slots the
+ * workspace holds) the call does not wait for the device, the FP64 re-solve of
+ * unconverged MIXED jobs included, so several calls can be queued ahead; it
+ * waits between waves when there are more jobs, and when a call first needs
+ * (or outgrows) a workspace buffer, which it then allocates.  Errors detected on the device are reported
+ * by the next b200tau_sync. */
 int b200tau_solve_device(b200tau_ctx *ctx, const b200tau_job *jobs, int njobs,
                          int prec, double *tau00_l_dev);
 int b200tau_sync(b200tau_ctx *ctx);
