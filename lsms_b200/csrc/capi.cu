@@ -49,6 +49,13 @@ struct Plan {
 
 }  // namespace
 
+// One FP64 re-solve graph of a context (capi.cu, fallback_graph).
+struct FallbackGraph {
+  std::vector<long long> key;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
 struct b200tau_ctx {
   int device = 0;
   int lmax = 3, ns = 1, npola = 1, kkrsz = 16, b = 16, blk = 1024;
@@ -112,11 +119,9 @@ struct b200tau_ctx {
   TcMaps tc;
   float *d_pack = nullptr;
   int tc_ld = 0, tc_slots = 0;
-  // the mixed path's FP64 re-solve as a graph with a conditional body (ensure_fallback_graph)
+  // the mixed path's FP64 re-solve as graphs with a conditional body (fallback_graph)
   cudaStream_t cap_stream = nullptr;
-  cudaGraph_t fb_graph = nullptr;
-  cudaGraphExec_t fb_exec = nullptr;
-  std::vector<long long> fb_key;
+  std::vector<FallbackGraph> fb;  // most recently used last
   // converged flags after the first refinement rounds, copied back without a wait: the next
   // call's estimate of how many jobs the later rounds' sweeps serve
   int *h_hint = nullptr;
@@ -446,63 +451,88 @@ int ensure_fallback(b200tau_ctx *ctx, int ld) {
   return B200TAU_OK;
 }
 
-void drop_fallback_graph(b200tau_ctx *ctx) {
-  if (ctx->fb_exec) cudaGraphExecDestroy(ctx->fb_exec);
-  if (ctx->fb_graph) cudaGraphDestroy(ctx->fb_graph);
-  ctx->fb_exec = nullptr;
-  ctx->fb_graph = nullptr;
-  ctx->fb_key.clear();
+void destroy_fallback_graph(FallbackGraph &f) {
+  if (f.exec) cudaGraphExecDestroy(f.exec);  // (a launch still in flight completes first)
+  if (f.graph) cudaGraphDestroy(f.graph);
+  f.exec = nullptr;
+  f.graph = nullptr;
 }
+
+void drop_fallback_graphs(b200tau_ctx *ctx) {
+  for (auto &f : ctx->fb) destroy_fallback_graph(f);
+  ctx->fb.clear();
+}
+
+// Graph shapes kept per context: the waves of a call are full but for the last one.
+constexpr size_t kFallbackGraphs = 4;
 
 // The FP64 re-solve of a mixed wave as one graph: a gate kernel, then a conditional node whose
 // body - the re-solve records (converged jobs inactive), FP64 block elimination, the FP64
 // refinement rounds and tau00 - runs only when some job did not converge.  So the host queues
 // the re-solve without waiting for the refinement's outcome, and a wave whose jobs all converged
-// pays one small launch for it.  Built on first use and again when the wave's shape or buffers
-// change (the records themselves are read from device memory when the graph runs).
-int ensure_fallback_graph(b200tau_ctx *ctx, int nw, int maxn, int maxN, int ld, int b, int ns, int kkrsz) {
+// pays one small launch for it.  The body is captured for the call's bounds (N <= ld, n <= ld - b;
+// its kernels skip the steps and rows beyond each job's own), so every wave of nw jobs shares one
+// graph; a graph is built on first use of its (nw, buffers) and kept (the records themselves are
+// read from device memory when the graph runs).
+int fallback_graph(b200tau_ctx *ctx, int nw, int ld, int b, int ns, int kkrsz, cudaGraphExec_t *out) {
   const int steps = std::max(1, ctx->refine_steps[0]);
+  const int maxN = ld, maxn = ld - b;
   int *finfo = ctx->d_info + ctx->slots;
-  const std::vector<long long> key = {nw, maxn, maxN, ld, b, ns, kkrsz, steps, ctx->slots,
+  const std::vector<long long> key = {nw, ld, b, ns, kkrsz, steps, ctx->slots,
                                       (long long)(uintptr_t)ctx->d_jobs, (long long)(uintptr_t)ctx->d_jobs3,
                                       (long long)(uintptr_t)ctx->d_ffb, (long long)(uintptr_t)ctx->d_info,
                                       (long long)(uintptr_t)ctx->d_fbcount, (long long)(uintptr_t)ctx->d_err};
-  if (ctx->fb_exec && key == ctx->fb_key) return B200TAU_OK;
-  drop_fallback_graph(ctx);
+  for (size_t i = 0; i < ctx->fb.size(); ++i)
+    if (ctx->fb[i].key == key) {
+      const FallbackGraph f = ctx->fb[i];  // most recently used last
+      ctx->fb.erase(ctx->fb.begin() + (long)i);
+      ctx->fb.push_back(f);
+      *out = f.exec;
+      return B200TAU_OK;
+    }
   if (!ctx->cap_stream) CK(cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking));
-  cudaGraph_t g = nullptr;
-  CK(cudaGraphCreate(&g, 0));
-  ctx->fb_graph = g;
+  FallbackGraph f;
+  f.key = key;
+  cudaError_t e = cudaGraphCreate(&f.graph, 0);
   cudaGraphConditionalHandle h;
-  CK(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+  if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h, f.graph, 0, cudaGraphCondAssignDefault);
   cudaGraphNode_t gate = nullptr, cond = nullptr;
-  CK(add_fallback_gate_node(g, &gate, ctx->d_jobs, nw, h));
+  if (e == cudaSuccess) e = add_fallback_gate_node(f.graph, &gate, ctx->d_jobs, nw, h);
   cudaGraphNodeParams cp = {};
   cp.type = cudaGraphNodeTypeConditional;
   cp.conditional.handle = h;
   cp.conditional.type = cudaGraphCondTypeIf;
   cp.conditional.size = 1;
-  CK(cudaGraphAddNode(&cond, g, &gate, 1, &cp));
-  cudaGraph_t body = cp.conditional.phGraph_out[0];
-  CK(cudaStreamBeginCaptureToGraph(ctx->cap_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-  cudaError_t e = launch_fallback_prepare(ctx->d_jobs, ctx->d_jobs3, nw, ctx->d_ffb, (size_t)ld * ld, maxN,
-                                          ctx->d_fbcount, ctx->cap_stream, nullptr);
-  if (e == cudaSuccess)
-    e = launch_eliminate(kFactorFP64, ctx->d_jobs3, nw, maxn, maxN, finfo, ctx->cap_stream, nullptr, nullptr,
-                         nullptr, ctx->d_err, true);
-  if (e == cudaSuccess)
-    e = launch_solve_refine(kFactorFP64, ctx->d_jobs3, nw, maxn, maxN, b, steps, ns, kkrsz, finfo,
-                            ctx->cap_stream, nullptr);
-  cudaGraph_t captured = nullptr;
-  const cudaError_t ec = cudaStreamEndCapture(ctx->cap_stream, &captured);
-  if (e == cudaSuccess) e = ec;
+  if (e == cudaSuccess) e = cudaGraphAddNode(&cond, f.graph, &gate, 1, &cp);
+  if (e == cudaSuccess) {
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    e = cudaStreamBeginCaptureToGraph(ctx->cap_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+      e = launch_fallback_prepare(ctx->d_jobs, ctx->d_jobs3, nw, ctx->d_ffb, (size_t)ld * ld, maxN, ctx->d_fbcount,
+                                  ctx->cap_stream, nullptr);
+      if (e == cudaSuccess)
+        e = launch_eliminate(kFactorFP64, ctx->d_jobs3, nw, maxn, maxN, finfo, ctx->cap_stream, nullptr, nullptr,
+                             nullptr, ctx->d_err, true);
+      if (e == cudaSuccess)
+        e = launch_solve_refine(kFactorFP64, ctx->d_jobs3, nw, maxn, maxN, b, steps, ns, kkrsz, finfo,
+                                ctx->cap_stream, nullptr);
+      cudaGraph_t captured = nullptr;
+      const cudaError_t ec = cudaStreamEndCapture(ctx->cap_stream, &captured);
+      if (e == cudaSuccess) e = ec;
+    }
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&f.exec, f.graph, 0);
   if (e != cudaSuccess) {
     cudaGetLastError();
-    drop_fallback_graph(ctx);
-    return fail(ctx, B200TAU_ERR_CUDA, "capturing the FP64 re-solve: %s", cudaGetErrorString(e));
+    destroy_fallback_graph(f);
+    return fail(ctx, B200TAU_ERR_CUDA, "building the FP64 re-solve graph: %s", cudaGetErrorString(e));
   }
-  CK(cudaGraphInstantiate(&ctx->fb_exec, g, 0));
-  ctx->fb_key = key;
+  if (ctx->fb.size() >= kFallbackGraphs) {
+    destroy_fallback_graph(ctx->fb.front());
+    ctx->fb.erase(ctx->fb.begin());
+  }
+  ctx->fb.push_back(f);
+  *out = f.exec;
   return B200TAU_OK;
 }
 
@@ -558,9 +588,10 @@ int run_refinement(b200tau_ctx *ctx, const std::vector<JobDev> &h, int nw, int m
   // factors can refine, e.g. energies next to the real axis) take the FP64 path instead: an FP64
   // copy of the unmodified M, FP64 block elimination, the FP64 refinement rounds, tau00 from X -
   // the same kernels and arithmetic as a PREC_FP64 solve of the job.
+  cudaGraphExec_t fb = nullptr;
   int rc = ensure_fallback(ctx, h[0].ld);
-  if (rc || (rc = ensure_fallback_graph(ctx, nw, maxn, maxN, h[0].ld, b, ns, kkrsz))) return rc;
-  CK(cudaGraphLaunch(ctx->fb_exec, ctx->stream));
+  if (rc || (rc = fallback_graph(ctx, nw, h[0].ld, b, ns, kkrsz, &fb))) return rc;
+  CK(cudaGraphLaunch(fb, ctx->stream));
   ctx->launches += 1;
   return B200TAU_OK;
 }
@@ -815,7 +846,7 @@ void b200tau_destroy(b200tau_ctx *ctx) {
   if (ctx->la.panel) cudaEventDestroy(ctx->la.panel);
   if (ctx->la.diag) cudaEventDestroy(ctx->la.diag);
   if (ctx->la.s2) cudaStreamDestroy(ctx->la.s2);
-  drop_fallback_graph(ctx);
+  drop_fallback_graphs(ctx);
   if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
   if (ctx->hint_ev) cudaEventDestroy(ctx->hint_ev);
   if (ctx->h_hint) cudaFreeHost(ctx->h_hint);
