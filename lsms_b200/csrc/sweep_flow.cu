@@ -415,12 +415,14 @@ __device__ __forceinline__ void split_unit(float *a, float *lo, int ncol) {
 }
 
 // One unit on the compute side: wait for its load and for its lo buffer, split it, and arrive
-// (per warp) on the unit's split barrier.  A thread whose wait ran out marks the job aborted and
-// skips the rest, so the accumulator never fills and the tile's vote fails everywhere.
+// (per warp) on the unit's split barrier.  A warp in which a wait ran out marks the job aborted
+// and skips the rest (all its lanes alike, so the warp-wide sync below is reached by all or none),
+// so the accumulator never fills and the tile's vote fails everywhere.
 __device__ __forceinline__ void unit_split(const FlowSmem &S, int u, int ncol, int *conv) {
   const int st = u % kStages;
   bool okt = wait_local(S.ring_full + st, (u / kStages) & 1, conv);
   if (okt && u >= 2) okt = wait_local(S.lo_free + (u & 1), ((u >> 1) - 1) & 1, conv);
+  okt = __all_sync(0xffffffffu, okt);
   if (!okt) {
     job_abort(conv);
     return;
