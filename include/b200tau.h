@@ -52,6 +52,10 @@ extern "C" {
 #define B200TAU_SWEEP_FP64 0 /* mixed path: correction solve in FP64 arithmetic on FP32 factors */
 #define B200TAU_SWEEP_FP32 1 /* mixed path: correction solve in FP32, as zcgesv (default) */
 
+#define B200TAU_PIVOT_AUTO 0  /* PANEL from N = 3000 up, else BLOCK (default) */
+#define B200TAU_PIVOT_BLOCK 1 /* pivots inside each 64 x 64 diagonal block */
+#define B200TAU_PIVOT_PANEL 2 /* pivots from the whole remaining column of each 64-column panel */
+
 typedef struct b200tau_ctx b200tau_ctx;
 
 /* One solve: what calculateTauMatrix receives besides the shared state
@@ -123,12 +127,12 @@ int b200tau_solve(b200tau_ctx *ctx, const b200tau_job *jobs, int njobs,
 
 /* As b200tau_solve, but tau00_l_dev is device memory and the call returns
  * once the work is enqueued on the context's stream (inputs already resident
- * from upload_tmat / set_atom).  When the jobs fit one wave (the slots the
- * workspace holds) the call does not wait for the device, the FP64 re-solve of
- * unconverged MIXED jobs included, so several calls can be queued ahead; it
- * waits between waves when there are more jobs, and when a call first needs
- * (or outgrows) a workspace buffer, which it then allocates.  Errors detected on the device are reported
- * by the next b200tau_sync. */
+ * from upload_tmat / set_atom).  The call does not wait for the device, not
+ * between waves and not for the FP64 re-solve of unconverged MIXED jobs, so
+ * several calls can be queued ahead.  It waits only when a call first needs (or
+ * outgrows) a workspace buffer, which it then allocates.  Errors detected on
+ * the device (a singular pivot of any job of the last call, a bounded wait that
+ * ran out) are reported by the next b200tau_sync. */
 int b200tau_solve_device(b200tau_ctx *ctx, const b200tau_job *jobs, int njobs,
                          int prec, double *tau00_l_dev);
 int b200tau_sync(b200tau_ctx *ctx);
@@ -211,6 +215,27 @@ long b200tau_last_fallback_count(const b200tau_ctx *ctx);
 /* Turn that FP64 re-solve off (0) or on (1, the default).  Off, an unconverged MIXED job
  * returns its last refinement iterate. */
 int b200tau_set_mixed_fallback(b200tau_ctx *ctx, int enable);
+
+/* Row pivoting of the block elimination (B200TAU_PIVOT_*), both precisions.  BLOCK pivots inside
+ * each 64 x 64 diagonal block, as the reference's GPU solver inverts its diagonal blocks
+ * (zblock_lu_cuda_c.cu:218-259).  PANEL picks each 64-column step's rows from every remaining
+ * row of the panel by a tournament of partial-pivoting eliminations, then moves them into place
+ * in every column: the quality of LAPACK's zgetrf over the column (the reference's CPU path pivots
+ * with zgetrf inside blocks of ~N/3 rows, zblock_lu_cpp.cpp:58, linearSolvers_CPU.cpp:270), at
+ * the cost of the tournament and the row moves; ill-conditioned matrices need it for the MIXED
+ * refinement to converge.  Pivots never come from the central site's rows, so FP64 with 0
+ * refinement steps still reads tau00 from the Schur complement.  b200tau_solve_vjp always
+ * uses BLOCK. */
+int b200tau_set_pivoting(b200tau_ctx *ctx, int mode);
+
+/* Bound, in polls, of the first wait of every KKR-build CTA on the copy of the angular tables
+ * into its shared memory (default 1 << 24; 0 makes that wait give up at once).  A CTA whose wait
+ * runs out records it, still waits (with a far longer bound) for its copy to land before it
+ * exits, and leaves its block column of M unbuilt; the call then returns B200TAU_ERR_TIMEOUT
+ * (outputs are written but meaningless).  It exists to exercise that reporting: every bounded
+ * device wait of the library reports the same way.  No counterpart in the reference, which has
+ * no bounded waits (it aborts, src/Accelerator/zblock_lu_cuda_c.cu:30-52). */
+int b200tau_set_build_wait(b200tau_ctx *ctx, long polls);
 
 #ifdef __cplusplus
 }

@@ -5,6 +5,7 @@
 
 from __future__ import annotations
 
+import concurrent.futures
 import os
 import shutil
 import subprocess
@@ -13,7 +14,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB_DIR = os.path.join(HERE, "_lib")
 LIB_PATH = os.path.join(LIB_DIR, "libb200tau.so")
-SOURCES = ["capi.cu", "kkr_build.cu", "block_lu.cu", "tc_update.cu", "sweep.cu", "sweep_flow.cu", "adjoint.cu", "noalloc.cu", "angular.cpp"]
+SOURCES = ["capi.cu", "kkr_build.cu", "block_lu.cu", "tc_update.cu", "sweep.cu", "sweep_flow.cu", "adjoint.cu",
+           "noalloc.cu", "pivot.cu", "runtime.cu", "angular.cpp"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -33,15 +35,27 @@ def build(verbose: bool = False, force: bool = False) -> str:
     if (not force and os.path.exists(LIB_PATH)
             and all(os.path.getmtime(LIB_PATH) >= os.path.getmtime(d) for d in deps)):
         return LIB_PATH
-    cmd = [nvcc(), "-shared", "-Xcompiler", "-fPIC", "-O3", "-lineinfo", "-std=c++17", *ARCH,
-           "-o", LIB_PATH, *srcs]
+    # one object per source, compiled in parallel, then one link
+    obj_dir = os.path.join(LIB_DIR, "obj")
+    os.makedirs(obj_dir, exist_ok=True)
+    flags = ["-Xcompiler", "-fPIC", "-O3", "-lineinfo", "-std=c++17", *ARCH]
     if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-    res = subprocess.run(cmd, capture_output=True, text=True)
+        flags.insert(0, "-Xptxas=-v")
+    objs = [os.path.join(obj_dir, os.path.basename(src) + ".o") for src in srcs]
+
+    def compile_one(k):
+        return subprocess.run([nvcc(), "-c", *flags, "-o", objs[k], srcs[k]], capture_output=True, text=True)
+
+    with concurrent.futures.ThreadPoolExecutor(max_workers=min(len(srcs), os.cpu_count() or 1)) as ex:
+        results = list(ex.map(compile_one, range(len(srcs))))
+    for src, res in zip(srcs, results):
+        if res.returncode != 0:
+            raise RuntimeError(f"nvcc failed on {os.path.basename(src)}:\n" + res.stderr[-4000:])
+        if verbose:
+            print(os.path.basename(src), res.stderr)
+    res = subprocess.run([nvcc(), "-shared", *ARCH, "-o", LIB_PATH, *objs], capture_output=True, text=True)
     if res.returncode != 0:
-        raise RuntimeError("nvcc failed:\n" + res.stderr[-4000:])
-    if verbose:
-        print(res.stderr)
+        raise RuntimeError("nvcc link failed:\n" + res.stderr[-4000:])
     return LIB_PATH
 
 

@@ -348,7 +348,7 @@ cudaError_t launch_inverse(const JobDev *jobs, int njobs, int max_n, int max_N, 
 cudaError_t launch_vjp_assemble(const JobDev *jobs, int njobs, int max_L, int kkrsz, int ns, cudaStream_t s,
                                 long *launches) {
   if (njobs <= 0) return cudaSuccess;
-  cudaError_t e = cudaFuncSetAttribute(vjp_assemble_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kVjpSmem);
+  cudaError_t e = ensure_smem(vjp_assemble_kernel, kVjpSmem);
   if (e != cudaSuccess) return e;
   vjp_assemble_kernel<<<dim3(max_L, njobs), 256, kVjpSmem, s>>>(jobs, kkrsz, ns);
   if (launches) *launches += 1;

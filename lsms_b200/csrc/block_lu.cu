@@ -412,6 +412,9 @@ __global__ void __launch_bounds__(256) finalize_from_x_kernel(const JobDev *__re
                                                               int kkrsz) {
   const JobDev &J = jobs[blockIdx.x];
   if (J.inactive) return;
+  // a dataflow sweep whose bounded wait ran out aborted this job: report it in the error word
+  if (threadIdx.x == 0 && J.conv != nullptr && J.err != nullptr && *J.conv == kAborted)
+    atomicOr(J.err, kErrSweepWait);
   const int b = J.b;
   __shared__ double2 A[kMaxB][2 * kMaxB + 1];
   for (int e = threadIdx.x; e < b * b; e += blockDim.x) {
@@ -551,16 +554,19 @@ __global__ void __launch_bounds__(kResThreads, 4) residual_kernel(const JobDev *
     }
   }
   asm volatile("cp.async.wait_group 0;" ::: "memory");
+  // with panel pivoting the factors are those of P M: row gr of R goes to its physical row
+  const int *__restrict__ rowpos = J.piv != nullptr ? J.piv + ld : nullptr;
 #pragma unroll
   for (int i = 0; i < RPT; ++i) {
     const int gr = row0 + rg + i * RG;
     if (gr >= N) continue;
+    const int dst = rowpos != nullptr ? rowpos[gr] : gr;
 #pragma unroll
     for (int j = 0; j < NCT; ++j) {
       const int c = cg * NCT + j;
       if (c >= b) continue;
       const double2 bv = (gr >= J.n) ? J.t0[(gr - J.n) + (size_t)c * J.t0_ld] : zero;
-      J.R[(size_t)gr + (size_t)c * ld] = csub(bv, acc[i][j]);
+      J.R[(size_t)dst + (size_t)c * ld] = csub(bv, acc[i][j]);
     }
   }
 }
@@ -601,12 +607,22 @@ constexpr int kSparseGrid = 2 * 148;
 // the next diagonal block; s2 waits for it and inverts that block while s updates the other tiles;
 // s waits for the inverse before step k + 1.  Only the diagonal inverse moves off s, so the packs of step k + 1 are
 // written after every tile of step k has read those of step k.
+// With panel pivoting the first update covers the whole first tile column (the next step's panel,
+// every row), the second stream also runs the next step's tournament and applies its row moves to
+// the columns left of the other tiles, and the main stream applies them to the other columns once
+// their update is done.
 template <typename T, typename S>
 cudaError_t eliminate_lookahead(const JobDev *jobs, int njobs, int max_n, int max_N, int *info, cudaStream_t s,
                                 long *launches, KernelTimer *timer, const TcMaps &tc, int *err, const Lookahead &la,
-                                int smem_diag, int smem_gemm) {
+                                int smem_diag, int smem_gemm, bool panel) {
   cudaError_t e;
+  const FactorKind fk = sizeof(T) == sizeof(double2) ? kFactorFP64 : kFactorFP32;
   const int free_sms = njobs < tc_num_sms() / 2 ? njobs : tc_num_sms() / 2;
+  if (panel) {
+    if ((e = launch_pivot_init(jobs, njobs, s, launches)) != cudaSuccess) return e;
+    if ((e = launch_panel_select(fk, jobs, njobs, 0, max_n, s, launches)) != cudaSuccess) return e;
+    if ((e = launch_row_moves(fk, jobs, njobs, 0, 0, max_N, max_N, s, launches)) != cudaSuccess) return e;
+  }
   diag_inverse_kernel<T><<<njobs, kDiagThreads, smem_diag, s>>>(jobs, 0, info);
   if (launches) *launches += 1;
   for (int k = 0; k < max_n; k += kNb) {
@@ -622,36 +638,51 @@ cudaError_t eliminate_lookahead(const JobDev *jobs, int njobs, int max_n, int ma
       const bool timed = timer && timer->used + 2 <= timer->cap;
       if (timed) cudaEventRecord(timer->ev[timer->used++], s);
       if ((e = launch_tc_pack(tc, jobs, njobs, k, max_N, s, false)) != cudaSuccess) return e;
-      if ((e = launch_tc_update(tc, jobs, njobs, k, max_N, err, s, 1, 0)) != cudaSuccess) return e;
+      if ((e = launch_tc_update(tc, jobs, njobs, k, max_N, err, s, panel ? 3 : 1, 0)) != cudaSuccess) return e;
+      // the next step's columns left of the tiles still being updated: [0, k + 64 + one tile)
+      const int split = k + kNb + kTcTileCols;
       if (next) {
         if ((e = cudaEventRecord(la.panel, s)) != cudaSuccess) return e;
         if ((e = cudaStreamWaitEvent(la.s2, la.panel, 0)) != cudaSuccess) return e;
+        if (panel) {
+          if ((e = launch_panel_select(fk, jobs, njobs, k + kNb, max_n, la.s2, launches)) != cudaSuccess) return e;
+          if ((e = launch_row_moves(fk, jobs, njobs, k + kNb, 0, split, max_N, la.s2, launches)) != cudaSuccess)
+            return e;
+        }
         diag_inverse_kernel<T><<<njobs, kDiagThreads, smem_diag, la.s2>>>(jobs, k + kNb, info);
         if ((e = cudaEventRecord(la.diag, la.s2)) != cudaSuccess) return e;
       }
-      if ((e = launch_tc_update(tc, jobs, njobs, k, max_N, err, s, 2, next ? tc_num_sms() - free_sms : 0)) !=
-          cudaSuccess)
+      if ((e = launch_tc_update(tc, jobs, njobs, k, max_N, err, s, panel ? 4 : 2,
+                                next ? tc_num_sms() - free_sms : 0)) != cudaSuccess)
         return e;
       if (timed) cudaEventRecord(timer->ev[timer->used++], s);  // the update kernels only
       if (next && (e = cudaStreamWaitEvent(s, la.diag, 0)) != cudaSuccess) return e;
+      if (next && panel && (e = launch_row_moves(fk, jobs, njobs, k + kNb, split, max_N, max_N, s, launches)) !=
+                               cudaSuccess)
+        return e;
       if (launches) *launches += next ? 5 : 4;
     } else if (next) {
+      if (panel) {
+        if ((e = launch_panel_select(fk, jobs, njobs, k + kNb, max_n, s, launches)) != cudaSuccess) return e;
+        if ((e = launch_row_moves(fk, jobs, njobs, k + kNb, 0, max_N, max_N, s, launches)) != cudaSuccess) return e;
+      }
       diag_inverse_kernel<T><<<njobs, kDiagThreads, smem_diag, s>>>(jobs, k + kNb, info);
       if (launches) *launches += 1;
     }
   }
+  if (panel && (e = launch_pivot_finish(jobs, njobs, s, launches)) != cudaSuccess) return e;
   return cudaGetLastError();
 }
 
 template <typename T, typename S>
 cudaError_t eliminate_impl(const JobDev *jobs, int njobs, int max_n, int max_N, int *info, cudaStream_t s,
                            long *launches, KernelTimer *timer, const TcMaps *tc, int *err, bool sparse_jobs,
-                           const Lookahead *la) {
+                           const Lookahead *la, bool panel) {
+  const FactorKind fk = sizeof(T) == sizeof(double2) ? kFactorFP64 : kFactorFP32;
   const int smem_diag = kNb * (kNb + 1) * (int)sizeof(double2);
   const int smem_gemm = 4 * kKc * kTile * (int)sizeof(T);
   cudaError_t e;
-  if ((e = cudaFuncSetAttribute(diag_inverse_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                smem_diag)) != cudaSuccess)
+  if ((e = ensure_smem(diag_inverse_kernel<T>, smem_diag)) != cudaSuccess)
     return e;
   if ((e = cudaFuncSetAttribute(zgemm_tile_kernel<S, kOverwrite>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem_gemm)) != cudaSuccess)
@@ -664,8 +695,13 @@ cudaError_t eliminate_impl(const JobDev *jobs, int njobs, int max_n, int max_N, 
   // tiles are updated on SMs left free for it (the inverses take one SM per job).
   if (tc != nullptr && la != nullptr && la->s2 != nullptr && !sparse_jobs)
     return eliminate_lookahead<T, S>(jobs, njobs, max_n, max_N, info, s, launches, timer, *tc, err, *la, smem_diag,
-                                     smem_gemm);
+                                     smem_gemm, panel);
+  if (panel && (e = launch_pivot_init(jobs, njobs, s, launches)) != cudaSuccess) return e;
   for (int k = 0; k < max_n; k += kNb) {
+    if (panel) {
+      if ((e = launch_panel_select(fk, jobs, njobs, k, max_n, s, launches)) != cudaSuccess) return e;
+      if ((e = launch_row_moves(fk, jobs, njobs, k, 0, max_N, max_N, s, launches)) != cudaSuccess) return e;
+    }
     diag_inverse_kernel<T><<<njobs, kDiagThreads, smem_diag, s>>>(jobs, k, info);
     const int rest = max_N - k - 1;
     const int tiles = (rest + kTile - 1) / kTile;
@@ -690,6 +726,7 @@ cudaError_t eliminate_impl(const JobDev *jobs, int njobs, int max_n, int max_N, 
       if (launches) *launches += 2;
     }
   }
+  if (panel && (e = launch_pivot_finish(jobs, njobs, s, launches)) != cudaSuccess) return e;
   return cudaGetLastError();
 }
 
@@ -832,16 +869,16 @@ cudaError_t launch_copy_to_factor(FactorKind fk, const double2 *M, void *F, int 
 
 cudaError_t launch_eliminate(FactorKind fk, const JobDev *jobs, int njobs, int max_n, int max_N, int *info,
                              cudaStream_t s, long *launches, KernelTimer *timer, const TcMaps *tc,
-                             int *err, bool sparse_jobs, const Lookahead *la) {
+                             int *err, bool sparse_jobs, const Lookahead *la, bool panel) {
   if (fk == kFactorFP64)
     return eliminate_impl<double2, double>(jobs, njobs, max_n, max_N, info, s, launches, timer, nullptr, err,
-                                           sparse_jobs, nullptr);
+                                           sparse_jobs, nullptr, panel);
   if (tc) {
     cudaError_t e = tc_prepare();
     if (e != cudaSuccess) return e;
   }
   return eliminate_impl<float2, float>(jobs, njobs, max_n, max_N, info, s, launches, timer, tc, err, sparse_jobs,
-                                       la);
+                                       la, panel);
 }
 
 cudaError_t launch_finalize_direct(FactorKind fk, const JobDev *jobs, int njobs, int ns, int kkrsz, int *info,
@@ -866,7 +903,7 @@ cudaError_t launch_refine_begin(FactorKind fk, const JobDev *jobs, int njobs, in
 template <int BC>
 cudaError_t launch_residual(const JobDev *jobs, int njobs, int max_N, int *active, cudaStream_t s) {
   constexpr int sm = residual_smem_bytes<BC>();
-  const cudaError_t e = cudaFuncSetAttribute(residual_kernel<BC>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  const cudaError_t e = ensure_smem(residual_kernel<BC>, sm);
   if (e != cudaSuccess) return e;
   const int rowblocks = (max_N + residual_rows<BC>() - 1) / residual_rows<BC>();
   if (active) {

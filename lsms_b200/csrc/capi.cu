@@ -29,6 +29,8 @@ struct AtomDev {
   int L = 0;
   int N = 0;       // n_spin_cant * nrmat
   int b = 0;       // kkrsz_ns of the central site
+  unsigned char *dev = nullptr;  // one device buffer holding the five arrays below
+  int cap_L = 0;                 // sites it has room for (re-registering a LIZ that fits reuses it)
   double *pos = nullptr;   // device, 3 x L
   int *lmax = nullptr;     // device, L
   int *store = nullptr;    // device, L
@@ -39,6 +41,10 @@ struct AtomDev {
   double2 ubr[4], ubrd[4];
   bool valid = false;
 };
+
+// Bytes of an atom's device record for L sites: pos (3 L doubles), then lmax, store, perm (L ints
+// each) and off (L + 1 ints).
+size_t atom_bytes(int L) { return sizeof(double) * 3 * (size_t)L + sizeof(int) * (4 * (size_t)L + 1); }
 
 // How a precision runs: factor type, refinement steps (0: direct from the Schur block).
 struct Plan {
@@ -93,6 +99,18 @@ struct b200tau_ctx {
   double2 *d_adj = nullptr;
   size_t adj_cap = 0;
   unsigned char *d_tdiag = nullptr;  // per (store, energy, spin) t block: exactly diagonal
+  size_t tmat_cap = 0, tdiag_cap = 0;  // elements / flags the two buffers hold
+  // per-job singular-pivot status of the last solve call, copied back wave by wave without a wait,
+  // and the device error word read back with the outputs
+  int *h_info = nullptr;
+  int h_info_cap = 0, info_jobs = 0;
+  std::vector<int> info_order;  // caller's job index of each entry of h_info
+  int *h_err = nullptr;
+  long table_polls = kTablePolls;  // first wait of the KKR build's table copy (b200tau_set_build_wait)
+  int pivoting = B200TAU_PIVOT_AUTO;  // b200tau_set_pivoting
+  int *d_piv = nullptr;               // panel pivoting's per-slot buffers (pivot_ints(ld) each)
+  size_t piv_ints = 0;
+  int piv_slots = 0;
   long launches = 0;
   bool fallback_on = true;
   double2 *d_ffb = nullptr;  // FP64 factor storage of those re-solves, one per slot
@@ -153,15 +171,31 @@ int fail(b200tau_ctx *c, int code, const char *fmt, ...) {
   } while (0)
 
 void free_atom(AtomDev &a) {
-  cudaFree(a.pos);
-  cudaFree(a.lmax);
-  cudaFree(a.store);
-  cudaFree(a.perm);
-  cudaFree(a.off);
+  cudaFree(a.dev);
   a = AtomDev();
 }
 
 inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
+
+// B200TAU_PIVOT_AUTO takes panel pivoting from this N up: the tournament's latency per step is then
+// small beside the trailing update, and these (non-collinear, N = 4320) matrices need it.
+constexpr int kPanelAutoN = 3000;
+
+bool use_panel(const b200tau_ctx *ctx, int maxN) {
+  return ctx->pivoting == B200TAU_PIVOT_PANEL || (ctx->pivoting == B200TAU_PIVOT_AUTO && maxN >= kPanelAutoN);
+}
+
+int ensure_piv(b200tau_ctx *ctx, int ld, int slots) {
+  const size_t per = (size_t)pivot_ints(ld);
+  if (ctx->d_piv && per <= ctx->piv_ints && slots <= ctx->piv_slots) return B200TAU_OK;
+  CK(cudaStreamSynchronize(ctx->stream));  // (work still queued may use the old buffers)
+  cudaFree(ctx->d_piv);
+  ctx->d_piv = nullptr;
+  ctx->piv_ints = std::max(per, ctx->piv_ints);
+  ctx->piv_slots = std::max(slots, ctx->piv_slots);
+  CK(cudaMalloc(&ctx->d_piv, sizeof(int) * ctx->piv_ints * ctx->piv_slots));
+  return B200TAU_OK;
+}
 
 Plan plan_for(const b200tau_ctx *ctx, int prec) {
   Plan p;
@@ -256,7 +290,12 @@ void fill_slot(b200tau_ctx *ctx, JobDev &J, int slot, int ld, const Plan &p) {
   J.conv = ctx->d_conv + slot;
   J.cnorm = ctx->d_cnorm + slot;
   J.slot = slot;
+  J.err = ctx->d_err;
+  J.piv = nullptr;
 }
+
+// The slot's panel-pivoting buffer (ensure_piv has sized it for the call).
+int *slot_piv(const b200tau_ctx *ctx, int slot) { return ctx->d_piv + (size_t)slot * ctx->piv_ints; }
 
 // Clears the per-slot status of the first nw slots: singular-pivot info, converged flag, last
 // correction size.
@@ -281,6 +320,7 @@ BuildParams build_params(const b200tau_ctx *ctx, const Plan &p) {
   bp.tdiag = ctx->d_tdiag;
   bp.group = ctx->group_size;
   bp.g_mode = 0;
+  bp.table_polls = ctx->table_polls;
   return bp;
 }
 
@@ -474,11 +514,11 @@ constexpr size_t kFallbackGraphs = 4;
 // its kernels skip the steps and rows beyond each job's own), so every wave of nw jobs shares one
 // graph; a graph is built on first use of its (nw, buffers) and kept (the records themselves are
 // read from device memory when the graph runs).
-int fallback_graph(b200tau_ctx *ctx, int nw, int ld, int b, int ns, int kkrsz, cudaGraphExec_t *out) {
+int fallback_graph(b200tau_ctx *ctx, int nw, int ld, int b, int ns, int kkrsz, bool panel, cudaGraphExec_t *out) {
   const int steps = std::max(1, ctx->refine_steps[0]);
   const int maxN = ld, maxn = ld - b;
   int *finfo = ctx->d_info + ctx->slots;
-  const std::vector<long long> key = {nw, ld, b, ns, kkrsz, steps, ctx->slots,
+  const std::vector<long long> key = {nw, ld, b, ns, kkrsz, steps, ctx->slots, panel ? 1 : 0,
                                       (long long)(uintptr_t)ctx->d_jobs, (long long)(uintptr_t)ctx->d_jobs3,
                                       (long long)(uintptr_t)ctx->d_ffb, (long long)(uintptr_t)ctx->d_info,
                                       (long long)(uintptr_t)ctx->d_fbcount, (long long)(uintptr_t)ctx->d_err};
@@ -512,7 +552,7 @@ int fallback_graph(b200tau_ctx *ctx, int nw, int ld, int b, int ns, int kkrsz, c
                                   ctx->cap_stream, nullptr);
       if (e == cudaSuccess)
         e = launch_eliminate(kFactorFP64, ctx->d_jobs3, nw, maxn, maxN, finfo, ctx->cap_stream, nullptr, nullptr,
-                             nullptr, ctx->d_err, true);
+                             nullptr, ctx->d_err, true, nullptr, panel);
       if (e == cudaSuccess)
         e = launch_solve_refine(kFactorFP64, ctx->d_jobs3, nw, maxn, maxN, b, steps, ns, kkrsz, finfo,
                                 ctx->cap_stream, nullptr);
@@ -557,7 +597,7 @@ void refresh_active_hint(b200tau_ctx *ctx) {
 // jobs that did not converge.  The host never waits inside the wave.  `h` are the wave's records
 // as uploaded to ctx->d_jobs.
 int run_refinement(b200tau_ctx *ctx, const std::vector<JobDev> &h, int nw, int maxn, int maxN, int b, int ns,
-                   int kkrsz, const Plan &p, const CUtensorMap *fmap) {
+                   int kkrsz, const Plan &p, const CUtensorMap *fmap, bool panel) {
   const bool fp32_sweep = p.fk == kFactorFP32 && ctx->mixed_sweep == B200TAU_SWEEP_FP32;
   refresh_active_hint(ctx);
   CK(launch_refine_begin(p.fk, ctx->d_jobs, nw, maxn, maxN, b, ctx->d_info, ctx->stream, &ctx->launches,
@@ -590,14 +630,14 @@ int run_refinement(b200tau_ctx *ctx, const std::vector<JobDev> &h, int nw, int m
   // the same kernels and arithmetic as a PREC_FP64 solve of the job.
   cudaGraphExec_t fb = nullptr;
   int rc = ensure_fallback(ctx, h[0].ld);
-  if (rc || (rc = fallback_graph(ctx, nw, h[0].ld, b, ns, kkrsz, &fb))) return rc;
+  if (rc || (rc = fallback_graph(ctx, nw, h[0].ld, b, ns, kkrsz, panel, &fb))) return rc;
   CK(cudaGraphLaunch(fb, ctx->stream));
   ctx->launches += 1;
   return B200TAU_OK;
 }
 
 int run_pipeline(b200tau_ctx *ctx, const std::vector<JobDev> &h, int nw, int maxn, int maxN, int ld, int ns,
-                 int kkrsz, int b, const Plan &p) {
+                 int kkrsz, int b, const Plan &p, bool panel) {
   if (ctx->profiling && ctx->timer.used + 4 * (maxn / kNb + 2) > ctx->timer.cap) {
     int rc = drain_timer(ctx);
     if (rc) return rc;
@@ -613,10 +653,10 @@ int run_pipeline(b200tau_ctx *ctx, const std::vector<JobDev> &h, int nw, int max
   int rc = phase_begin(ctx);
   if (rc) return rc;
   CK(launch_eliminate(p.fk, ctx->d_jobs, nw, maxn, maxN, ctx->d_info, ctx->stream, &ctx->launches,
-                      ctx->profiling ? &ctx->timer : nullptr, tc, ctx->d_err, false, &ctx->la));
+                      ctx->profiling ? &ctx->timer : nullptr, tc, ctx->d_err, false, &ctx->la, panel));
   if ((rc = phase_end(ctx, 1)) || (rc = phase_begin(ctx))) return rc;
   if (p.steps > 0) {
-    if ((rc = run_refinement(ctx, h, nw, maxn, maxN, b, ns, kkrsz, p, tc ? &tc->tFu : nullptr))) return rc;
+    if ((rc = run_refinement(ctx, h, nw, maxn, maxN, b, ns, kkrsz, p, tc ? &tc->tFu : nullptr, panel))) return rc;
   } else {
     CK(launch_finalize_direct(p.fk, ctx->d_jobs, nw, ns, kkrsz, ctx->d_info, ctx->stream, &ctx->launches));
   }
@@ -635,6 +675,9 @@ int run_wave(b200tau_ctx *ctx, const b200tau_job *jobs, const int *idx, int nw, 
              double2 *out_base, const AdjointBufs *adj = nullptr) {
   std::vector<JobDev> h(nw);
   int maxL = 0, maxN = 0, maxn = 0;
+  for (int w = 0; w < nw; ++w) maxN = std::max(maxN, ctx->atoms[jobs[idx[w]].atom].N);
+  // the adjoint forms M^-1 from block factors without row moves
+  const bool panel = adj == nullptr && use_panel(ctx, maxN);
   for (int w = 0; w < nw; ++w) {
     const b200tau_job &jb = jobs[idx[w]];
     const AtomDev &a = ctx->atoms[jb.atom];
@@ -648,6 +691,7 @@ int run_wave(b200tau_ctx *ctx, const b200tau_job *jobs, const int *idx, int nw, 
     J.perm = a.perm;
     J.off = a.off;
     fill_slot(ctx, J, w, ld, p);
+    if (panel) J.piv = slot_piv(ctx, w);
     J.L = a.L;
     J.N = a.N;
     J.b = a.b;
@@ -682,7 +726,7 @@ int run_wave(b200tau_ctx *ctx, const b200tau_job *jobs, const int *idx, int nw, 
   CK(launch_kkr_build(ctx->d_jobs, nw, maxL, build_params(ctx, p), ctx->d_err, ctx->stream, &ctx->launches));
   if ((rc = phase_end(ctx, 0))) return rc;
   if (ctx->profiling) ctx->prof_flops += trailing_flops(h);
-  if ((rc = run_pipeline(ctx, h, nw, maxn, maxN, ld, ctx->ns, ctx->kkrsz, ctx->b, p))) return rc;
+  if ((rc = run_pipeline(ctx, h, nw, maxn, maxN, ld, ctx->ns, ctx->kkrsz, ctx->b, p, panel))) return rc;
   if (!adj) return B200TAU_OK;
   // adjoint: G into M's storage (M is no longer needed once X is refined), M^-1 from the factors,
   // then the per-site contractions
@@ -695,7 +739,7 @@ int run_wave(b200tau_ctx *ctx, const b200tau_job *jobs, const int *idx, int nw, 
   return B200TAU_OK;
 }
 
-int check_info(b200tau_ctx *ctx, const std::vector<int> &info, const int *idx, int nw) {
+int check_info(b200tau_ctx *ctx, const int *info, const int *idx, int nw) {
   for (int w = 0; w < nw; ++w)
     if (info[w] != 0)
       return fail(ctx, B200TAU_ERR_SINGULAR,
@@ -703,6 +747,25 @@ int check_info(b200tau_ctx *ctx, const std::vector<int> &info, const int *idx, i
                               : "job %d: 1 - Delta is singular",
                   idx[w], info[w] > 0 ? info[w] - 1 : 0);
   return B200TAU_OK;
+}
+
+// Page-locked host room for the per-job status of a call of n jobs.
+int ensure_host_info(b200tau_ctx *ctx, int n) {
+  if (n <= ctx->h_info_cap) return B200TAU_OK;
+  CK(cudaStreamSynchronize(ctx->stream));  // no copy into the old buffer is pending
+  if (ctx->h_info) cudaFreeHost(ctx->h_info);
+  ctx->h_info = nullptr;
+  ctx->h_info_cap = 0;
+  CK(cudaMallocHost(&ctx->h_info, sizeof(int) * (size_t)n));
+  ctx->h_info_cap = n;
+  return B200TAU_OK;
+}
+
+// The status of the last solve call's jobs, once the stream has been synchronised.
+int check_host_info(b200tau_ctx *ctx) {
+  const int n = ctx->info_jobs;
+  ctx->info_jobs = 0;
+  return n > 0 ? check_info(ctx, ctx->h_info, ctx->info_order.data(), n) : B200TAU_OK;
 }
 
 int validate_jobs(b200tau_ctx *ctx, const b200tau_job *jobs, int njobs) {
@@ -727,8 +790,11 @@ int validate_jobs(b200tau_ctx *ctx, const b200tau_job *jobs, int njobs) {
   return B200TAU_OK;
 }
 
-int solve_impl(b200tau_ctx *ctx, const b200tau_job *jobs, int njobs, int prec, double2 *dev_out,
-               bool sync_and_check) {
+// Enqueues every wave of the call; the host does not wait.  Each wave's singular-pivot status is
+// copied into ctx->h_info (caller order in ctx->info_order) behind the wave, for check_host_info
+// after the caller's synchronisation.
+int solve_impl(b200tau_ctx *ctx, const b200tau_job *jobs, int njobs, int prec, double2 *dev_out) {
+  ctx->info_jobs = 0;
   if (njobs == 0) return B200TAU_OK;
   int rc = validate_jobs(ctx, jobs, njobs);
   if (rc) return rc;
@@ -745,30 +811,37 @@ int solve_impl(b200tau_ctx *ctx, const b200tau_job *jobs, int njobs, int prec, d
   const int slots = choose_slots(ctx, ld, njobs, p, extra);
   if ((rc = ensure_workspace(ctx, ld, slots, p))) return rc;
   if ((rc = ensure_jobs(ctx, slots))) return rc;
+  if ((rc = ensure_host_info(ctx, njobs))) return rc;
+  if (use_panel(ctx, maxN) && (rc = ensure_piv(ctx, ld, slots))) return rc;
   ctx->launches = 0;
   if (ctx->d_fbcount) CK(cudaMemsetAsync(ctx->d_fbcount, 0, sizeof(int), ctx->stream));
-  std::vector<int> info(slots);
   for (int w0 = 0; w0 < njobs; w0 += slots) {
     const int nw = std::min(slots, njobs - w0);
     if ((rc = run_wave(ctx, jobs, &order[w0], nw, ld, p, dev_out))) return rc;
-    if (sync_and_check || w0 + nw < njobs) {
-      CK(cudaMemcpyAsync(info.data(), ctx->d_info, sizeof(int) * nw, cudaMemcpyDeviceToHost,
-                         ctx->stream));
-      CK(cudaStreamSynchronize(ctx->stream));
-      if ((rc = check_info(ctx, info, &order[w0], nw))) return rc;
-    }
+    CK(cudaMemcpyAsync(ctx->h_info + w0, ctx->d_info, sizeof(int) * nw, cudaMemcpyDeviceToHost, ctx->stream));
+  }
+  ctx->info_order = order;
+  ctx->info_jobs = njobs;
+  return B200TAU_OK;
+}
+
+// The device error word as copied to ctx->h_err by the caller's last enqueued read (the stream
+// has been synchronised since); a set word is cleared on the device and reported.
+int check_host_err(b200tau_ctx *ctx) {
+  const int flags = *ctx->h_err;
+  if (flags) {
+    *ctx->h_err = 0;
+    CK(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return fail(ctx, B200TAU_ERR_TIMEOUT, "a device-side wait exceeded its bound (flags %d)", flags);
   }
   return B200TAU_OK;
 }
 
 int check_err_flags(b200tau_ctx *ctx) {
-  int flags = 0;
-  CK(cudaMemcpy(&flags, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
-  if (flags) {
-    cudaMemset(ctx->d_err, 0, sizeof(int));
-    return fail(ctx, B200TAU_ERR_TIMEOUT, "a device-side wait exceeded its bound (flags %d)", flags);
-  }
-  return B200TAU_OK;
+  CK(cudaMemcpyAsync(ctx->h_err, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  return check_host_err(ctx);
 }
 
 int check_prec(b200tau_ctx *ctx, int prec) {
@@ -806,6 +879,8 @@ int b200tau_create(b200tau_ctx **out, int device, int lmax, int n_spin_cant, int
   if (e == cudaSuccess) e = cudaMemcpy(ctx->d_tables, &tab, sizeof(tab), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMalloc(&ctx->d_err, sizeof(int));
   if (e == cudaSuccess) e = cudaMemset(ctx->d_err, 0, sizeof(int));
+  if (e == cudaSuccess) e = cudaMallocHost(&ctx->h_err, sizeof(int));
+  if (e == cudaSuccess) *ctx->h_err = 0;
   if (e != cudaSuccess) {
     int code = e == cudaErrorMemoryAllocation ? B200TAU_ERR_OOM : B200TAU_ERR_CUDA;
     b200tau_destroy(ctx);
@@ -841,6 +916,7 @@ void b200tau_destroy(b200tau_ctx *ctx) {
   cudaFree(ctx->d_adj);
   cudaFree(ctx->d_ffb);
   cudaFree(ctx->d_fbcount);
+  cudaFree(ctx->d_piv);
   for (auto &e : ctx->events) cudaEventDestroy(e);
   for (auto &e : ctx->pev) cudaEventDestroy(e);
   if (ctx->la.panel) cudaEventDestroy(ctx->la.panel);
@@ -850,6 +926,8 @@ void b200tau_destroy(b200tau_ctx *ctx) {
   if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
   if (ctx->hint_ev) cudaEventDestroy(ctx->hint_ev);
   if (ctx->h_hint) cudaFreeHost(ctx->h_hint);
+  if (ctx->h_info) cudaFreeHost(ctx->h_info);
+  if (ctx->h_err) cudaFreeHost(ctx->h_err);
   if (ctx->stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
 }
@@ -925,6 +1003,21 @@ int b200tau_set_mixed_engine(b200tau_ctx *ctx, int engine) {
   return B200TAU_OK;
 }
 
+int b200tau_set_pivoting(b200tau_ctx *ctx, int mode) {
+  if (!ctx) return B200TAU_ERR_ARG;
+  if (mode != B200TAU_PIVOT_AUTO && mode != B200TAU_PIVOT_BLOCK && mode != B200TAU_PIVOT_PANEL)
+    return fail(ctx, B200TAU_ERR_ARG, "unknown pivoting mode %d", mode);
+  ctx->pivoting = mode;
+  return B200TAU_OK;
+}
+
+int b200tau_set_build_wait(b200tau_ctx *ctx, long polls) {
+  if (!ctx) return B200TAU_ERR_ARG;
+  if (polls < 0) return fail(ctx, B200TAU_ERR_ARG, "build wait polls %ld < 0", polls);
+  ctx->table_polls = polls;
+  return B200TAU_OK;
+}
+
 int b200tau_set_mixed_fallback(b200tau_ctx *ctx, int enable) {
   if (!ctx) return B200TAU_ERR_ARG;
   ctx->fallback_on = enable != 0;
@@ -954,38 +1047,43 @@ int b200tau_upload_tmat(b200tau_ctx *ctx, const double *tmat_store, long ld, int
     return fail(ctx, B200TAU_ERR_ARG, "upload_tmat: bad arguments (ld %ld, nstore %d, blk %d, expected blk %d)",
                 ld, nstore, blk_size, ctx->blk);
   CK(cudaSetDevice(ctx->device));
-  const size_t bytes = sizeof(double2) * (size_t)ld * nstore;
-  if (!ctx->d_tmat || (size_t)ctx->tmat_ld * ctx->nstore < (size_t)ld * nstore) {
-    CK(cudaStreamSynchronize(ctx->stream));
-    cudaFree(ctx->d_tmat);
-    ctx->d_tmat = nullptr;
-    CK(cudaMalloc(&ctx->d_tmat, bytes));
-  }
-  CK(cudaMemcpyAsync(ctx->d_tmat, tmat_store, bytes, cudaMemcpyHostToDevice, ctx->stream));
-  // Which t blocks are exactly diagonal (no spin-orbit or non-spherical coupling): the KKR build
-  // then forms the block row t_i G_ij from the diagonal alone.  One flag per (store, energy, spin).
+  const size_t elems = (size_t)ld * nstore;
   const int group = (int)(ld / blk_size);
-  const bool colpol = ctx->npola != ctx->ns;
-  const int b = ctx->b, kk = ctx->kkrsz;
-  std::vector<unsigned char> flags((size_t)nstore * group * 2, 0);
-  for (int s = 0; s < nstore; ++s)
-    for (int ie = 0; ie < group; ++ie)
-      for (int sp = 0; sp < (colpol ? 2 : 1); ++sp) {
-        const double *t = tmat_store + 2 * ((size_t)s * ld + (size_t)ie * blk_size + (colpol ? kk * kk * sp : 0));
-        bool diag = true;
-        for (int c = 0; c < b && diag; ++c)
-          for (int r = 0; r < b; ++r)
-            if (r != c && (t[2 * (r + (size_t)c * b)] != 0.0 || t[2 * (r + (size_t)c * b) + 1] != 0.0)) {
-              diag = false;
-              break;
-            }
-        flags[((size_t)s * group + ie) * 2 + sp] = diag ? 1 : 0;
-      }
-  CK(cudaStreamSynchronize(ctx->stream));
-  cudaFree(ctx->d_tdiag);
-  ctx->d_tdiag = nullptr;
-  CK(cudaMalloc(&ctx->d_tdiag, flags.size()));
-  CK(cudaMemcpy(ctx->d_tdiag, flags.data(), flags.size(), cudaMemcpyHostToDevice));
+  const size_t nflags = (size_t)nstore * group * 2;
+  if (elems > ctx->tmat_cap || nflags > ctx->tdiag_cap) {
+    CK(cudaStreamSynchronize(ctx->stream));  // solves still queued read the old buffers
+    if (elems > ctx->tmat_cap) {
+      cudaFree(ctx->d_tmat);
+      ctx->d_tmat = nullptr;
+      ctx->tmat_cap = 0;
+      CK(cudaMalloc(&ctx->d_tmat, sizeof(double2) * elems));
+      ctx->tmat_cap = elems;
+    }
+    if (nflags > ctx->tdiag_cap) {
+      cudaFree(ctx->d_tdiag);
+      ctx->d_tdiag = nullptr;
+      ctx->tdiag_cap = 0;
+      CK(cudaMalloc(&ctx->d_tdiag, nflags));
+      ctx->tdiag_cap = nflags;
+    }
+  }
+  // stream-ordered behind any solve still queued on the context
+  CK(cudaMemcpyAsync(ctx->d_tmat, tmat_store, sizeof(double2) * elems, cudaMemcpyHostToDevice, ctx->stream));
+  // Which t blocks are exactly diagonal (no spin-orbit or non-spherical coupling): the KKR build
+  // then forms the block row t_i G_ij from the diagonal alone.  One flag per (store, energy, spin),
+  // found on the device.
+  CK(launch_tdiag_flags(ctx->d_tmat, ld, nstore, group, ctx->b, ctx->kkrsz, ctx->npola != ctx->ns,
+                        ctx->d_tdiag, ctx->stream));
+  // A copy from page-locked memory reads the caller's buffer after cudaMemcpyAsync returns (one
+  // from pageable memory is staged before it returns): wait for it, so that the buffer is free
+  // when this call returns.
+  cudaPointerAttributes pa;
+  if (cudaPointerGetAttributes(&pa, tmat_store) == cudaSuccess) {
+    if (pa.type == cudaMemoryTypeHost) CK(cudaStreamSynchronize(ctx->stream));
+  } else {
+    cudaGetLastError();
+    CK(cudaStreamSynchronize(ctx->stream));
+  }
   ctx->tmat_ld = ld;
   ctx->nstore = nstore;
   ctx->group_size = group;
@@ -1009,9 +1107,16 @@ int b200tau_set_atom(b200tau_ctx *ctx, int atom, int num_liz, const double *liz_
   CK(cudaSetDevice(ctx->device));
   if ((int)ctx->atoms.size() <= atom) ctx->atoms.resize(atom + 1);
   AtomDev &a = ctx->atoms[atom];
-  CK(cudaStreamSynchronize(ctx->stream));
-  free_atom(a);
   const int L = num_liz;
+  if (L > a.cap_L) {  // a larger LIZ than this record holds: a new device buffer
+    CK(cudaStreamSynchronize(ctx->stream));  // solves still queued read the old one
+    cudaFree(a.dev);
+    a.dev = nullptr;
+    a.cap_L = 0;
+    CK(cudaMalloc(&a.dev, atom_bytes(L)));
+    a.cap_L = L;
+  }
+  a.valid = false;
   // central site last (see JobDev)
   std::vector<int> perm(L), off(L + 1);
   for (int p = 0; p < L - 1; ++p) perm[p] = p + 1;
@@ -1030,16 +1135,25 @@ int b200tau_set_atom(b200tau_ctx *ctx, int atom, int num_liz, const double *liz_
     a.ubr[k] = ubr ? make_double2(ubr[2 * k], ubr[2 * k + 1]) : make_double2(0, 0);
     a.ubrd[k] = ubrd ? make_double2(ubrd[2 * k], ubrd[2 * k + 1]) : make_double2(0, 0);
   }
-  CK(cudaMalloc(&a.pos, sizeof(double) * 3 * L));
-  CK(cudaMalloc(&a.lmax, sizeof(int) * L));
-  CK(cudaMalloc(&a.store, sizeof(int) * L));
-  CK(cudaMalloc(&a.perm, sizeof(int) * L));
-  CK(cudaMalloc(&a.off, sizeof(int) * (L + 1)));
-  CK(cudaMemcpy(a.pos, liz_pos, sizeof(double) * 3 * L, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(a.lmax, liz_lmax, sizeof(int) * L, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(a.store, liz_store_idx, sizeof(int) * L, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(a.perm, perm.data(), sizeof(int) * L, cudaMemcpyHostToDevice));
-  CK(cudaMemcpy(a.off, off.data(), sizeof(int) * (L + 1), cudaMemcpyHostToDevice));
+  // one host image of the record, one stream-ordered copy (from pageable memory the copy is
+  // staged before cudaMemcpyAsync returns, so the image may go out of scope)
+  std::vector<unsigned char> img(atom_bytes(L));
+  unsigned char *q = img.data();
+  std::memcpy(q, liz_pos, sizeof(double) * 3 * L);
+  q += sizeof(double) * 3 * L;
+  std::memcpy(q, liz_lmax, sizeof(int) * L);
+  q += sizeof(int) * L;
+  std::memcpy(q, liz_store_idx, sizeof(int) * L);
+  q += sizeof(int) * L;
+  std::memcpy(q, perm.data(), sizeof(int) * L);
+  q += sizeof(int) * L;
+  std::memcpy(q, off.data(), sizeof(int) * (L + 1));
+  a.pos = reinterpret_cast<double *>(a.dev);
+  a.lmax = reinterpret_cast<int *>(a.dev + sizeof(double) * 3 * L);
+  a.store = a.lmax + L;
+  a.perm = a.store + L;
+  a.off = a.perm + L;
+  CK(cudaMemcpyAsync(a.dev, img.data(), img.size(), cudaMemcpyHostToDevice, ctx->stream));
   a.valid = true;
   return B200TAU_OK;
 }
@@ -1054,10 +1168,16 @@ int b200tau_solve(b200tau_ctx *ctx, const b200tau_job *jobs, int njobs, int prec
   CK(cudaSetDevice(ctx->device));
   const size_t outn = (size_t)njobs * ctx->b * ctx->b;
   if ((rc = ensure_out(ctx, outn))) return rc;
-  if ((rc = solve_impl(ctx, jobs, njobs, prec, ctx->d_out, true))) return rc;
+  if ((rc = solve_impl(ctx, jobs, njobs, prec, ctx->d_out))) return rc;
+  // outputs, status words and error word behind the waves; one wait
+  CK(cudaMemcpyAsync(ctx->h_err, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaMemcpyAsync(tau00_l, ctx->d_out, sizeof(double2) * outn, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
-  return check_err_flags(ctx);
+  if ((rc = check_host_err(ctx))) {  // the wait that ran out, not what followed from it
+    ctx->info_jobs = 0;
+    return rc;
+  }
+  return check_host_info(ctx);
 }
 
 int b200tau_solve_device(b200tau_ctx *ctx, const b200tau_job *jobs, int njobs, int prec,
@@ -1068,22 +1188,20 @@ int b200tau_solve_device(b200tau_ctx *ctx, const b200tau_job *jobs, int njobs, i
   int rc = check_prec(ctx, prec);
   if (rc) return rc;
   CK(cudaSetDevice(ctx->device));
-  return solve_impl(ctx, jobs, njobs, prec, reinterpret_cast<double2 *>(tau00_l_dev), false);
+  return solve_impl(ctx, jobs, njobs, prec, reinterpret_cast<double2 *>(tau00_l_dev));
 }
 
 int b200tau_sync(b200tau_ctx *ctx) {
   if (!ctx) return B200TAU_ERR_ARG;
+  CK(cudaSetDevice(ctx->device));
+  CK(cudaMemcpyAsync(ctx->h_err, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
-  if (ctx->d_info && ctx->slots > 0) {
-    std::vector<int> info(ctx->slots);
-    CK(cudaMemcpy(info.data(), ctx->d_info, sizeof(int) * ctx->slots, cudaMemcpyDeviceToHost));
-    for (int w = 0; w < ctx->slots; ++w)
-      if (info[w] != 0) {
-        cudaMemset(ctx->d_info, 0, sizeof(int) * ctx->slots);
-        return fail(ctx, B200TAU_ERR_SINGULAR, "a job of the last wave hit a singular pivot");
-      }
+  int rc = check_host_err(ctx);
+  if (rc) {
+    ctx->info_jobs = 0;
+    return rc;
   }
-  return check_err_flags(ctx);
+  return check_host_info(ctx);
 }
 
 int b200tau_solve_dense(b200tau_ctx *ctx, const double *m, int n, int ldm, const double *t0, int b,
@@ -1127,10 +1245,15 @@ int b200tau_solve_dense(b200tau_ctx *ctx, const double *m, int n, int ldm, const
   J.t0_ld = b;
   J.out = ctx->d_out;
   J.out_mode = 1;
+  const bool panel = use_panel(ctx, n);
+  if (panel) {
+    if ((rc = ensure_piv(ctx, ld, 1))) return rc;
+    J.piv = slot_piv(ctx, 0);
+  }
   CK(cudaMemcpyAsync(ctx->d_jobs, &J, sizeof(J), cudaMemcpyHostToDevice, ctx->stream));
   if ((rc = reset_slot_status(ctx, 1))) return rc;
   ctx->launches = 0;
-  if ((rc = run_pipeline(ctx, std::vector<JobDev>{J}, 1, r, n, ld, 1, b, b, p))) return rc;
+  if ((rc = run_pipeline(ctx, std::vector<JobDev>{J}, 1, r, n, ld, 1, b, b, p, panel))) return rc;
   int info = 0;
   CK(cudaMemcpyAsync(&info, ctx->d_info, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaMemcpyAsync(tau00, ctx->d_out, es * b * b, cudaMemcpyDeviceToHost, ctx->stream));
@@ -1197,7 +1320,7 @@ int b200tau_solve_vjp(b200tau_ctx *ctx, const b200tau_job *jobs, int njobs, cons
     if ((rc = run_wave(ctx, jobs, &order[w0], nw, ld, p, ctx->d_out, &adj))) return rc;
     CK(cudaMemcpyAsync(info.data(), ctx->d_info, sizeof(int) * nw, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
-    if ((rc = check_info(ctx, info, &order[w0], nw))) return rc;
+    if ((rc = check_info(ctx, info.data(), &order[w0], nw))) return rc;
   }
   if (tau00)
     CK(cudaMemcpyAsync(tau00, ctx->d_out, sizeof(double2) * bb * njobs, cudaMemcpyDeviceToHost, ctx->stream));

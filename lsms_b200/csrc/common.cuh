@@ -17,12 +17,39 @@ constexpr int kNdlm = (kMaxLend + 1) * (kMaxLend + 2) / 2;       // 28 P_lm valu
 constexpr int kNdlj = (kMaxLend + 1) * (kMaxLend + 1);           // 49 D_lm values
 constexpr int kMaxTerms = kMaxLmax + 1;                          // Gaunt terms per G element
 constexpr int kNb = 64;                                         // elimination block width
+// Panel pivoting (pivot.cu): candidate rows per tournament leaf, and nodes merged per level.
+constexpr int kPivLeafRows = 256;
+constexpr int kPivFanIn = 4;
+// Per-job pivot buffer of panel pivoting (ints), for leading dimension ld:
+//   [0, ld)                  perm: the original row at each physical row position
+//   [ld, 2 ld)               rowpos: the physical position of each original row (after elimination)
+//   [2 ld, 2 ld + 1 + 4 kNb) the step's row moves: count, kNb*2 destinations, kNb*2 sources
+//   then two areas of pivot_sets(ld) x kNb candidate rows (tournament levels, alternating)
+__host__ __device__ constexpr int pivot_sets(int ld) { return (ld + kPivLeafRows - 1) / kPivLeafRows; }
+__host__ __device__ constexpr int pivot_moves_offset(int ld) { return 2 * ld; }
+__host__ __device__ constexpr int pivot_sets_offset(int ld, int which) {
+  return 2 * ld + 1 + 4 * kNb + which * pivot_sets(ld) * kNb;
+}
+__host__ __device__ constexpr int pivot_ints(int ld) { return pivot_sets_offset(ld, 2); }
+// Columns of one tile of the tensor-core trailing update (tc_update.cu).
+constexpr int kTcTileCols = 256;
 // A refining job stops once its estimated remaining error on tau00 is below this fraction of
 // max|tau00|: 100x below the mixed path's 1e-10 accuracy target.
 constexpr double kRefineTol = 1e-12;
 // JobDev::conv values (0: still refining)
 constexpr int kConverged = 1;
-constexpr int kDiverged = 2;
+constexpr int kDiverged = 2;  // the corrections stopped shrinking (numerical)
+constexpr int kAborted = 3;   // a bounded wait of a dataflow sweep ran out on this job
+// Bits of the context's device error word: a bounded wait ran out in the KKR build's table copy,
+// in the tensor-core trailing update, or in a dataflow sweep of the refinement.
+constexpr int kErrBuildWait = 1;
+constexpr int kErrUpdateWait = 2;
+constexpr int kErrSweepWait = 8;
+// Polls of a bounded wait: the default bound of the first wait on the KKR build's table copy, and
+// the far longer bound of a wait that only drains copies or tensor-core work still in flight
+// after an earlier wait gave up (a CTA never exits with such work outstanding).
+constexpr long kTablePolls = 1L << 24;
+constexpr long kDrainPolls = 1L << 26;
 
 // Angular-momentum tables for G_ij (makegij_c.f:79-128, buildKKRMatrix_CPU.cpp:144-176),
 // laid out as a gather list: G(lm2, lm1) = pi4 * i^rot * sum_q coef[q] * D[didx[q]]
@@ -91,6 +118,9 @@ struct JobDev {
   const double2 *taubar; // b x b cotangent on tau00
   double2 *tbar;         // L blocks of b x b, LIZ site order: d<taubar, tau00>/d t_site
   double2 *dlogdet;      // L blocks of b x b: d ln det M / d t_site (may be null)
+  int *err;              // the context's device error word (kErr* bits), or null
+  int *piv;              // panel pivoting's buffer (pivot_ints(ld) ints), null: pivots inside the
+                         // 64 x 64 diagonal blocks only
 };
 
 struct BuildParams {
@@ -106,6 +136,7 @@ struct BuildParams {
   int group;                    // energies in the uploaded tmatStore group
   int g_mode;                   // 1: write the structure constants G (no t factor, zero diagonal
                                 // blocks) into M instead of M = 1 - t G (adjoint)
+  long table_polls;             // bound of the first wait on the table copy (kTablePolls)
 };
 
 enum FactorKind { kFactorFP64 = 0, kFactorFP32 = 1 };
@@ -137,7 +168,8 @@ cudaError_t launch_tc_step(const TcMaps &maps, const JobDev *jobs, int njobs, in
                            cudaStream_t s);
 // The two halves: the hi/lo operand packs of step k (A21, and W unless the W = D A12 tiles wrote
 // theirs), and the update of the tiles of `part` (0 all, 1 the tile holding the next diagonal
-// block, 2 the others) on at most max_grid SMs (0: all).
+// block, 2 the others; 3 the first tile column, which holds the next step's whole panel, 4 the
+// other tile columns) on at most max_grid SMs (0: all).
 cudaError_t launch_tc_pack(const TcMaps &maps, const JobDev *jobs, int njobs, int k, int max_N, cudaStream_t s,
                            bool pack_b);
 cudaError_t launch_tc_update(const TcMaps &maps, const JobDev *jobs, int njobs, int k, int max_N, int *err,
@@ -148,18 +180,42 @@ struct Lookahead {
   cudaEvent_t panel = nullptr, diag = nullptr;
 };
 
+// cudaFuncSetAttribute(fn, MaxDynamicSharedMemorySize, bytes) on the current device, skipped when
+// an earlier call on this device already allowed at least `bytes` (a per-launch host call costs
+// more than the launch itself).
+cudaError_t ensure_smem_attr(const void *fn, int bytes);
+template <typename K>
+inline cudaError_t ensure_smem(K *kernel, int bytes) {
+  return ensure_smem_attr(reinterpret_cast<const void *>(kernel), bytes);
+}
+
 // Launchers (return cudaGetLastError of the launches).  `launches` accumulates the number of
 // kernels enqueued.
 cudaError_t launch_kkr_build(const JobDev *jobs, int njobs, int max_L, const BuildParams &p,
                              int *err_flags, cudaStream_t s, long *launches);
+// flags[(store * group + iie) * 2 + ispin] = 1 when that b x b t block of the device tmatStore
+// (column-major, leading dimension ld per store column) has no non-zero off-diagonal element;
+// spin 1 is written as 0 unless the store is collinear spin-polarised (`colpol`).
+cudaError_t launch_tdiag_flags(const double2 *tmat, long ld, int nstore, int group, int b, int kkrsz, bool colpol,
+                               unsigned char *flags, cudaStream_t s);
 // Block elimination of F over the first n columns (all jobs of the wave).
 // With FP32 factors and `tc` non-null the trailing update runs on the tensor cores (tc_update.cu).
 // `sparse_jobs`: most records are inactive (the FP64 re-solve), so the trailing update runs on a
-// small looping grid instead of one CTA per tile.
+// small looping grid instead of one CTA per tile.  `panel`: the records carry pivot buffers and
+// every step picks its rows by panel pivoting (pivot.cu).
 cudaError_t launch_eliminate(FactorKind fk, const JobDev *jobs, int njobs, int max_n, int max_N,
                              int *info, cudaStream_t s, long *launches, KernelTimer *timer,
                              const TcMaps *tc, int *err, bool sparse_jobs = false,
-                             const Lookahead *la = nullptr);
+                             const Lookahead *la = nullptr, bool panel = false);
+// Panel pivoting (pivot.cu), for the records with a pivot buffer: the identity permutation; the
+// tournament that picks step k's kb rows from [k, n) and writes the step's row moves; those moves
+// applied to columns [c0, c1) of F; and the final row positions for the residual.
+cudaError_t launch_pivot_init(const JobDev *jobs, int njobs, cudaStream_t s, long *launches);
+cudaError_t launch_panel_select(FactorKind fk, const JobDev *jobs, int njobs, int k, int max_n, cudaStream_t s,
+                                long *launches);
+cudaError_t launch_row_moves(FactorKind fk, const JobDev *jobs, int njobs, int k, int c0, int c1, int max_N,
+                             cudaStream_t s, long *launches);
+cudaError_t launch_pivot_finish(const JobDev *jobs, int njobs, cudaStream_t s, long *launches);
 // F = M (n x n, leading dimension ld) converted to the factor type.
 cudaError_t launch_copy_to_factor(FactorKind fk, const double2 *M, void *F, int n, int ld, cudaStream_t s);
 // FP64 re-solve of the mixed jobs whose refinement did not converge, on the device: out[w] is

@@ -79,10 +79,21 @@ __device__ __forceinline__ int div_kk(int e, int kk) {
   }
 }
 
+__device__ __forceinline__ bool table_copy_done(unsigned bar) {
+  unsigned done;
+  asm volatile(
+      "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
+      : "=r"(done)
+      : "r"(bar)
+      : "memory");
+  return done != 0;
+}
+
 // Stage the angular tables with one bulk copy (cp.async.bulk, completion on an mbarrier).
-// The wait is bounded; on expiry the CTA records an error and keeps waiting (bounded again)
-// so that it never exits with a copy into its shared memory still in flight.
-__device__ bool stage_tables(BuildSmem &sm, const AngularTables *src, int *err) {
+// The wait is bounded by `polls` (BuildParams::table_polls); the outcome is made uniform over the
+// CTA, and on expiry the CTA records an error and keeps waiting (bounded again, far longer) so
+// that it never exits with a copy into its shared memory still in flight.
+__device__ bool stage_tables(BuildSmem &sm, const AngularTables *src, int *err, long polls) {
   const unsigned bar = smem_u32(&sm.bar);
   if (threadIdx.x == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
@@ -98,29 +109,16 @@ __device__ bool stage_tables(BuildSmem &sm, const AngularTables *src, int *err) 
   }
   __syncthreads();
   bool ok = false;
-  for (long it = 0; it < (1L << 24); ++it) {
-    unsigned done;
-    asm volatile(
-        "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
-        : "=r"(done)
-        : "r"(bar)
-        : "memory");
-    if (done) {
+  for (long it = 0; it < polls; ++it)
+    if (table_copy_done(bar)) {
       ok = true;
       break;
     }
-  }
+  ok = __syncthreads_and(ok) != 0;
   if (!ok) {
-    if (threadIdx.x == 0) atomicExch(err, 1);
-    for (long it = 0; it < (1L << 26); ++it) {
-      unsigned done;
-      asm volatile(
-          "{ .reg .pred p; mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0; selp.u32 %0, 1, 0, p; }"
-          : "=r"(done)
-          : "r"(bar)
-          : "memory");
-      if (done) break;
-    }
+    if (threadIdx.x == 0) atomicOr(err, kErrBuildWait);
+    for (long it = 0; it < kDrainPolls; ++it)
+      if (table_copy_done(bar)) break;
   }
   return ok;
 }
@@ -133,7 +131,7 @@ __global__ void __launch_bounds__(kThreads)
   const JobDev &J = jobs[blockIdx.y];
   const int pc = blockIdx.x;
   if (pc >= J.L) return;
-  if (!stage_tables(sm, p.tables, err)) return;
+  if (!stage_tables(sm, p.tables, err, p.table_polls)) return;
   const AngularTables &T = sm.tab;
   {
     const int it = threadIdx.x >> 5, L = threadIdx.x & 31;
@@ -413,7 +411,38 @@ __global__ void __launch_bounds__(kThreads)
   }
 }
 
+// One warp per (store, energy, spin) t block: is every off-diagonal element exactly zero?
+__global__ void tdiag_flags_kernel(const double2 *__restrict__ tmat, long ld, int nstore, int group, int b,
+                                   int kkrsz, int colpol, unsigned char *__restrict__ flags) {
+  const int f = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int lane = threadIdx.x & 31;
+  if (f >= nstore * group * 2) return;
+  const int sp = f & 1, ie = (f >> 1) % group, st = (f >> 1) / group;
+  if (sp == 1 && !colpol) {
+    if (lane == 0) flags[f] = 0;
+    return;
+  }
+  const long blk = (long)(2 * kkrsz) * (2 * kkrsz);
+  const double2 *t = tmat + (long)st * ld + (long)ie * blk + (colpol ? (long)kkrsz * kkrsz * sp : 0);
+  bool off = false;
+  for (int e = lane; e < b * b; e += 32) {
+    const int c = e / b, r = e - c * b;
+    const double2 v = t[e];
+    off |= r != c && (v.x != 0.0 || v.y != 0.0);
+  }
+  off = __any_sync(0xffffffffu, off);
+  if (lane == 0) flags[f] = off ? 0 : 1;
+}
+
 }  // namespace
+
+cudaError_t launch_tdiag_flags(const double2 *tmat, long ld, int nstore, int group, int b, int kkrsz, bool colpol,
+                               unsigned char *flags, cudaStream_t s) {
+  const int n = nstore * group * 2;
+  if (n <= 0) return cudaSuccess;
+  tdiag_flags_kernel<<<(n + 7) / 8, 256, 0, s>>>(tmat, ld, nstore, group, b, kkrsz, colpol ? 1 : 0, flags);
+  return cudaGetLastError();
+}
 
 cudaError_t launch_kkr_build(const JobDev *jobs, int njobs, int max_L, const BuildParams &p,
                              int *err_flags, cudaStream_t s, long *launches) {
@@ -421,7 +450,7 @@ cudaError_t launch_kkr_build(const JobDev *jobs, int njobs, int max_L, const Bui
   if (p.f_kind < 0 || p.f_kind > 2) return cudaErrorInvalidValue;
   void (*kern)(const JobDev *, BuildParams, int *) =
       p.f_kind == 0 ? kkr_build_kernel<0> : p.f_kind == 1 ? kkr_build_kernel<1> : kkr_build_kernel<2>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaError_t e = ensure_smem(kern, smem);
   if (e != cudaSuccess) return e;
   dim3 grid(max_L, njobs);
   kern<<<grid, kThreads, smem, s>>>(jobs, p, err_flags);

@@ -22,7 +22,6 @@
 
 #include <cuda_runtime.h>
 
-#include <cstdio>
 #include <cstring>
 #include <mutex>
 
@@ -76,10 +75,7 @@ extern "C" int b200tau_solve_dense_noalloc(const double *m, int n, int ldm, cons
                                            double *tau00, void *stream) {
   if (!m || !t0 || !tau00) return B200TAU_ERR_ARG;
   if (n < 1 || b < 1 || b > n || b > kMaxB || ldm < n) return B200TAU_ERR_ARG;
-  if (n > kNoAllocMaxN) {
-    fprintf(stderr, "b200tau_solve_dense_noalloc: n = %d exceeds the fixed scratch limit %d\n", n, kNoAllocMaxN);
-    return B200TAU_ERR_ARG;
-  }
+  if (n > kNoAllocMaxN) return B200TAU_ERR_ARG;  // beyond the fixed scratch array
   cudaStream_t s = static_cast<cudaStream_t>(stream);
   unsigned char *base = nullptr;
   if (scratch_address(&base) != cudaSuccess) return B200TAU_ERR_CUDA;
@@ -120,6 +116,7 @@ extern "C" int b200tau_solve_dense_noalloc(const double *m, int n, int ldm, cons
   J.t0_ld = b;
   J.out = reinterpret_cast<double2 *>(tau00);  // b x b, written by the last kernel
   J.out_mode = 1;
+  J.err = flags + 2;
   // the JobDev record is copied from a pageable host object; the runtime stages pageable
   // host-to-device copies before the call returns, so the stack object may go out of scope
   if (e == cudaSuccess) e = cudaMemcpyAsync(dJ, &J, sizeof(J), cudaMemcpyHostToDevice, s);

@@ -34,8 +34,9 @@
 //    lane m of TMEM is real row m, and a shuffle between lanes 2r and 2r + 1 forms
 //    Re = Ar Yr - Ai Yi and Im = Ar Yi + Ai Yr.
 //
-// Every barrier wait is bounded.  A wait that runs out marks the job diverged (JobDev::conv),
-// which also ends the other CTAs' waits, and the refinement re-solves that job in FP64.
+// Every barrier wait is bounded.  A wait that runs out marks the job aborted (JobDev::conv =
+// kAborted), which also ends the other CTAs' waits; the job's tau00_l step reports it in the
+// context's error word, and the refinement re-solves that job in FP64.
 
 #include <cuda_runtime.h>
 
@@ -95,10 +96,10 @@ __host__ __device__ inline FlowLayout flow_layout(int cs, int own, bool forward)
 
 // The job's abort word: JobDev::conv (null for an initial solve without refinement state).
 __device__ __forceinline__ bool job_aborted(const int *conv) {
-  return conv != nullptr && *reinterpret_cast<volatile const int *>(conv) == kDiverged;
+  return conv != nullptr && *reinterpret_cast<volatile const int *>(conv) == kAborted;
 }
 __device__ __forceinline__ void job_abort(int *conv) {
-  if (conv != nullptr) atomicExch(conv, kDiverged);
+  if (conv != nullptr) atomicExch(conv, kAborted);
 }
 // Barrier 1 over the 256 compute threads (the producer warp runs on its own).
 __device__ __forceinline__ void compute_sync() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
@@ -859,7 +860,7 @@ cudaError_t launch_flow_sweep(const JobDev *jobs, int njobs, int b, int max_N, b
     const FlowLayout L = flow_layout(c, (T + c - 1) / c, forward);
     if (L.total > kMaxSmem) break;
     fallback = c;
-    const cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L.total);
+    const cudaError_t e = ensure_smem(kern, L.total);
     if (e != cudaSuccess) return e;
     if (active_clusters(kern, c, L.total) >= want) {
       cs = c;
@@ -869,7 +870,7 @@ cudaError_t launch_flow_sweep(const JobDev *jobs, int njobs, int b, int max_N, b
   if (cs == 0) cs = fallback;
   if (cs == 0) return cudaSuccess;
   const FlowLayout L = flow_layout(cs, (T + cs - 1) / cs, forward);
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, L.total);
+  cudaError_t e = ensure_smem(kern, L.total);
   if (e != cudaSuccess) return e;
   if (forward)
     e = launch_cluster(forward_flow_kernel, cs, njobs, kBlock, L.total, s, jobs, L.own, *fmap);

@@ -34,7 +34,7 @@ namespace b200 {
 namespace {
 
 constexpr int kTM = 128;          // real rows per tile (64 complex rows)
-constexpr int kTN = 256;          // columns per tile
+constexpr int kTN = kTcTileCols;  // columns per tile
 constexpr int kTK = kTcChunk;     // floats per K chunk (64 bytes: one 64-byte swizzle span)
 constexpr int kKReal = 2 * kNb;   // 128 real K per step
 constexpr int kChunks = kKReal / kTK;
@@ -84,6 +84,11 @@ __device__ __forceinline__ bool mbar_wait(unsigned long long *b, unsigned parity
   for (long i = 0; i < kWaitBound; ++i)
     if (mbar_try(b, parity)) return true;
   return false;
+}
+// The wait for work already in flight after a wait ran out: the far longer drain bound.
+__device__ __forceinline__ void mbar_drain(unsigned long long *b, unsigned parity) {
+  for (long i = 0; i < kDrainPolls; ++i)
+    if (mbar_try(b, parity)) return;
 }
 
 __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z,
@@ -149,9 +154,15 @@ __device__ __forceinline__ bool tile_of(const JobDev *jobs, const TileSpace &ts,
   } else if (ts.part == 1) {
     tm = 0;
     tn = 0;
-  } else {
+  } else if (ts.part == 2) {
     tm = (i + 1) / ts.tiles_n;
     tn = i + 1 - tm * ts.tiles_n;
+  } else if (ts.part == 3) {
+    tm = i;
+    tn = 0;
+  } else {
+    tm = i / (ts.tiles_n - 1);
+    tn = 1 + i - tm * (ts.tiles_n - 1);
   }
   const JobDev &J = jobs[z];
   if (k >= J.n) return false;
@@ -215,7 +226,7 @@ __global__ void __launch_bounds__(192, 1)
         for (int c = 0; c < kChunks; ++c, ++g) {
           const int s = (int)(g % kStages);
           if (g >= kStages && !mbar_wait(&sm.empty[s], (unsigned)(((g / kStages) - 1) & 1))) {
-            atomicExch(err, 2);
+            atomicOr(err, kErrUpdateWait);
             sm.abort = 1;
             break;
           }
@@ -226,9 +237,14 @@ __global__ void __launch_bounds__(192, 1)
           tma_load_3d(sm.b_lo[s], &tB_lo, c * kTK, col0, z, &sm.full[s]);
         }
       }
-      // every issued load has landed before the CTA can exit (bounded; normally already true)
+      // every issued load has landed before the CTA can exit (normally already true); a wait that
+      // runs out is recorded and the wait goes on, far longer, so that no load can still be
+      // writing into this CTA's shared memory when it exits
       for (long q = g > kStages ? g - kStages : 0; q < g; ++q)
-        mbar_wait(&sm.full[q % kStages], (unsigned)((q / kStages) & 1));
+        if (!mbar_wait(&sm.full[q % kStages], (unsigned)((q / kStages) & 1))) {
+          atomicOr(err, kErrUpdateWait);
+          mbar_drain(&sm.full[q % kStages], (unsigned)((q / kStages) & 1));
+        }
     }
   } else if (warp == 1) {
     if (lane == 0) {
@@ -239,7 +255,7 @@ __global__ void __launch_bounds__(192, 1)
         if (!tile_of(jobs, ts, k, t, z, row0, col0, kb)) continue;
         const int a = li & 1;
         if (li >= 2 && !mbar_wait(&sm.acc_empty[a], (unsigned)(((li >> 1) - 1) & 1))) {
-          atomicExch(err, 5);
+          atomicOr(err, kErrUpdateWait);
           sm.abort = 1;
           break;
         }
@@ -249,7 +265,7 @@ __global__ void __launch_bounds__(192, 1)
         for (int c = 0; c < kChunks; ++c, ++g) {
           const int s = (int)(g % kStages);
           if (!mbar_wait(&sm.full[s], (unsigned)((g / kStages) & 1))) {
-            atomicExch(err, 3);
+            atomicOr(err, kErrUpdateWait);
             sm.abort = 1;
             ok = false;
             break;
@@ -271,9 +287,12 @@ __global__ void __launch_bounds__(192, 1)
         umma_commit(&sm.acc_full[a]);
         ++li;
       }
-      // the MMAs issued are complete before TMEM is released (bounded)
+      // the MMAs issued are complete before TMEM is released (the same keep-waiting rule)
       umma_commit(&sm.drain);
-      mbar_wait(&sm.drain, 0);
+      if (!mbar_wait(&sm.drain, 0)) {
+        atomicOr(err, kErrUpdateWait);
+        mbar_drain(&sm.drain, 0);
+      }
     }
   } else {
     // Epilogue, warps 2..5 -> TMEM lane quarter (warp % 4), 32 real rows each.  Each 64-column
@@ -297,7 +316,7 @@ __global__ void __launch_bounds__(192, 1)
         const bool ok = mbar_wait(&sm.acc_full[a], (unsigned)((li >> 1) & 1));
         sm.ep_ok = ok ? 1 : 0;
         if (!ok) {
-          atomicExch(err, 4);
+          atomicOr(err, kErrUpdateWait);
           sm.abort = 1;
         }
       }
@@ -431,7 +450,11 @@ cudaError_t launch_tc_update(const TcMaps &maps, const JobDev *jobs, int njobs, 
   ts.tiles_n = (rest + kTN - 1) / kTN;
   ts.tiles_m = (2 * rest + kTM - 1) / kTM;
   ts.part = part;
-  ts.per_job = part == 0 ? ts.tiles_m * ts.tiles_n : part == 1 ? 1 : ts.tiles_m * ts.tiles_n - 1;
+  ts.per_job = part == 0   ? ts.tiles_m * ts.tiles_n
+               : part == 1 ? 1
+               : part == 2 ? ts.tiles_m * ts.tiles_n - 1
+               : part == 3 ? ts.tiles_m
+                           : ts.tiles_m * (ts.tiles_n - 1);
   ts.total = ts.per_job * njobs;
   if (ts.total <= 0) return cudaSuccess;
   int grid = ts.total < tc_num_sms() ? ts.total : tc_num_sms();
@@ -449,7 +472,7 @@ cudaError_t launch_tc_step(const TcMaps &maps, const JobDev *jobs, int njobs, in
 }
 
 cudaError_t tc_prepare() {
-  return cudaFuncSetAttribute(tc_update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)tc_smem_bytes());
+  return ensure_smem(tc_update_kernel, (int)tc_smem_bytes());
 }
 
 }  // namespace b200

@@ -40,6 +40,9 @@ ENGINE_TENSOR = 0
 ENGINE_SIMT = 1
 SWEEP_FP64 = 0
 SWEEP_FP32 = 1
+PIVOT_AUTO = 0
+PIVOT_BLOCK = 1
+PIVOT_PANEL = 2
 
 # Symbols declared in include/b200tau.h.
 EXPORTS = (
@@ -49,7 +52,8 @@ EXPORTS = (
     "b200tau_gaunt_numbers", "b200tau_set_refinement", "b200tau_set_profiling",
     "b200tau_profile_read", "b200tau_set_mixed_engine", "b200tau_solve_dense_noalloc",
     "b200tau_profile_phases", "b200tau_set_mixed_sweep", "b200tau_solve_vjp",
-    "b200tau_last_fallback_count", "b200tau_set_mixed_fallback",
+    "b200tau_last_fallback_count", "b200tau_set_mixed_fallback", "b200tau_set_build_wait",
+    "b200tau_set_pivoting",
 )
 
 
@@ -105,6 +109,8 @@ def load_library():
     lib.b200tau_last_fallback_count.argtypes = [P]
     lib.b200tau_last_fallback_count.restype = L
     lib.b200tau_set_mixed_fallback.argtypes = [P, I]
+    lib.b200tau_set_build_wait.argtypes = [P, L]
+    lib.b200tau_set_pivoting.argtypes = [P, I]
     _lib = lib
     return lib
 
@@ -190,6 +196,15 @@ class TauSolver:
     def set_mixed_fallback(self, enable: bool):
         """Re-solve unconverged mixed-precision jobs by FP64 block LU (default on)."""
         self._check(self.lib.b200tau_set_mixed_fallback(self.ctx, int(bool(enable))))
+
+    def set_pivoting(self, mode: int):
+        """Row pivoting of the elimination: PIVOT_AUTO (default), PIVOT_BLOCK or PIVOT_PANEL."""
+        self._check(self.lib.b200tau_set_pivoting(self.ctx, mode))
+
+    def set_build_wait(self, polls: int):
+        """Bound of the KKR build's first wait on its table copy (0: give up at once); a wait
+        that runs out makes the call return ERR_TIMEOUT (see b200tau_set_build_wait)."""
+        self._check(self.lib.b200tau_set_build_wait(self.ctx, int(polls)))
 
     def set_mixed_sweep(self, sweep: int):
         """Arithmetic of the mixed path's correction solve: SWEEP_FP32 (default) or SWEEP_FP64."""

@@ -99,11 +99,14 @@ def test_fp64_without_refinement_is_the_block_lu(solver_factory):
 
 
 def test_n2160_contour_points_match_reference(solver_factory, ref):
+    """Every point of the 31-point contour at N = 2160 (the benchmark's workload), FP64 and MIXED
+    against the reference's own calculateTauMatrix."""
     prob = W.config_n2160()
     s = _solver(solver_factory, prob)
-    picks = [0, 15, 30]
+    picks = list(range(len(prob.energies)))
     out = s.solve_jobs(T.make_jobs([(0, i, 0, prob.energies[i]) for i in picks]), T.PREC_FP64)
     mixed = s.solve_jobs(T.make_jobs([(0, i, 0, prob.energies[i]) for i in picks]), T.PREC_MIXED)
+    assert s.last_fallback_count == 0
     for k, i in enumerate(picks):
         want = ref.calculate_tau(prob, i, 0, ref.ZBLOCKLU_CPP)
         assert tau_err(prob, i, 0, out[k], want) <= TOL_FP64, (i, tau_err(prob, i, 0, out[k], want))
@@ -294,41 +297,40 @@ def test_batched_alloy_with_vacancies_matches_reference(solver_factory, ref):
         assert tau_err(prob, iie, 0, mixed[k], want) <= TOL_MIXED, (a, iie)
 
 
-def cond1(m: np.ndarray) -> float:
-    """1-norm condition number."""
-    return float(np.abs(m).sum(0).max() * np.abs(np.linalg.inv(m)).sum(0).max())
-
-
 def test_noncollinear_n4320_matches_reference(solver_factory, ref):
     """Non-collinear kkrsz_ns = 32 over the 135-site fcc LIZ (N = 4320), spin-dependent phase
-    shifts with a random moment per site, two energies:
-    * FP64 agreement within 1e-12 or kappa_1(M) x 1e-16, whichever is larger, both for the
-      solver alone on the reference's own M and for the full path (device-built M): these
-      matrices have kappa_1 ~ 1e5..1e7, and two FP64 block-LU solves that differ only in their
-      blocking or in the rounding of sin/cos/exp in the build differ by about kappa x eps;
-    * the mixed path stays within 1e-10 of the FP64 path (refinement, or the FP64 re-solve of
-      jobs it cannot refine)."""
+    shifts with a random moment per site (condition numbers 1e5..1e7), five (atom, energy) jobs.
+    The reference's own two solvers disagree on these matrices by `spread` = |zgesv (0x2001) -
+    zblock_lu (0x2005)| (up to ~4e-11); the FP64 path (panel pivoting, the default at this size)
+    must agree with zgesv within max(1e-12, spread) and with zblock_lu within max(1e-12,
+    2 spread), on the full path (device-built M) and solver-only on the reference's own M; the
+    MIXED path within 1e-10 of FP64 without re-solving any job in FP64."""
     wl = W.config_noncollinear_batch(n_atoms=2)
     s = solver_factory(3, 2, 2)
     s.upload_tmat(wl.tmat_store)
     for a, at in enumerate(wl.atoms):
         s.set_atom(a, at.liz_pos, at.liz_lmax, at.liz_store_idx, at.ubr, at.ubrd)
-    picks = [(0, 2), (1, 9)]
+    picks = [(0, 2), (1, 9), (0, 0), (1, 5), (0, 15)]
     specs = [(a, iie, 0, wl.energies[iie]) for a, iie in picks]
     fp64 = s.solve_jobs(T.make_jobs(specs), T.PREC_FP64)
     mixed = s.solve_jobs(T.make_jobs(specs), T.PREC_MIXED)
+    assert s.last_fallback_count == 0
     for k, (a, iie) in enumerate(picks):
         prob = wl.problem(a)
         assert prob.nrmat_ns == 4320
-        m = ref.build_kkr(prob, iie)
-        t0 = prob.t_block(int(prob.liz_store_idx[0]), iie)
-        want_raw = ref.calculate_tau(prob, iie, 0, ref.ZBLOCKLU_CPP)
-        dense = s.solve_tau00_dense(m, t0)
-        raw_ref = port_tau00_raw(prob, iie, want_raw)
-        tol = max(TOL_FP64, cond1(m) * 1e-16)
-        assert relerr(dense, raw_ref) <= tol, (a, iie, relerr(dense, raw_ref), tol)
-        assert tau_err(prob, iie, 0, fp64[k], want_raw) <= tol, (a, iie, tau_err(prob, iie, 0, fp64[k], want_raw), tol)
+        blocklu = ref.calculate_tau(prob, iie, 0, ref.ZBLOCKLU_CPP)
+        zgesv = ref.calculate_tau(prob, iie, 0, ref.ZGESV)
+        spread = tau_err(prob, iie, 0, zgesv, blocklu)
+        tol_z, tol_b = max(TOL_FP64, spread), max(TOL_FP64, 2 * spread)
+        assert tau_err(prob, iie, 0, fp64[k], zgesv) <= tol_z, (a, iie, tau_err(prob, iie, 0, fp64[k], zgesv), spread)
+        assert tau_err(prob, iie, 0, fp64[k], blocklu) <= tol_b, (a, iie, tau_err(prob, iie, 0, fp64[k], blocklu), spread)
         assert tau_err(prob, iie, 0, mixed[k], fp64[k]) <= TOL_MIXED, (a, iie, tau_err(prob, iie, 0, mixed[k], fp64[k]))
+        if k < 2:  # solver-only on the reference's own matrix
+            m = ref.build_kkr(prob, iie)
+            t0 = prob.t_block(int(prob.liz_store_idx[0]), iie)
+            dense = s.solve_tau00_dense(m, t0)
+            assert relerr(dense, port_tau00_raw(prob, iie, zgesv)) <= tol_z
+            assert relerr(dense, port_tau00_raw(prob, iie, blocklu)) <= tol_b
 
 
 def port_tau00_raw(prob, iie, tau00_l):

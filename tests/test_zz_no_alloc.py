@@ -4,8 +4,10 @@ acceptable on their path).  The entry works on device buffers the caller owns an
 in a fixed file-scope device array, so it allocates nothing.
 
 Checked here through the C ABI: two calls in a row on different matrices give the same tau00 as
-the allocating entry b200tau_solve_dense (FP64 tolerance 1e-12), so nothing left in the shared
-scratch array by the first call leaks into the second; sizes above the limit are refused.
+the allocating entry b200tau_solve_dense and as the oracle (the reference's own calculateTauMatrix
+on the same matrix), both at the FP64 tolerance 1e-12, so nothing left in the shared scratch array
+by the first call leaks into the second; the device's free memory is the same before and after
+each call (nothing was allocated); sizes above the limit are refused.
 This file is collected last so that a stop-at-first-failure run has run everything else first."""
 
 import ctypes
@@ -26,17 +28,22 @@ def _kkr(prob, ref_build):
     return m, t0
 
 
-def _noalloc(lib, m: np.ndarray, t0: np.ndarray, stream) -> tuple[int, np.ndarray]:
+def _noalloc(lib, m: np.ndarray, t0: np.ndarray, stream) -> tuple[int, np.ndarray, int]:
+    """One call on caller-owned device buffers: (status, tau00, change of the device's free bytes
+    across the call)."""
     import torch
     n, b = m.shape[0], t0.shape[0]
     dm = torch.from_numpy(np.asfortranarray(m).ravel(order="F").view(np.float64).copy()).cuda()
     dt = torch.from_numpy(np.asfortranarray(t0).ravel(order="F").view(np.float64).copy()).cuda()
     dout = torch.zeros(2 * b * b, dtype=torch.float64, device="cuda")
     torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
     rc = lib.b200tau_solve_dense_noalloc(ctypes.c_void_p(dm.data_ptr()), n, n, ctypes.c_void_p(dt.data_ptr()), b,
                                          ctypes.c_void_p(dout.data_ptr()), ctypes.c_void_p(stream))
+    torch.cuda.synchronize()
+    free1 = torch.cuda.mem_get_info()[0]
     out = dout.cpu().numpy().view(np.complex128).reshape(b, b, order="F")
-    return rc, out
+    return rc, out, free1 - free0
 
 
 def test_noalloc_matches_allocating_entry_twice(ref):
@@ -49,12 +56,20 @@ def test_noalloc_matches_allocating_entry_twice(ref):
     try:
         cases = [W.config_small(seed=7),
                  W.make_problem("bcc", 5.42, 2, 3, [-0.2 + 0.1j], 8, n_species=2, liz_lmax=[3] * 9 + [2] * 6)]
+        # a first call loads the library's kernels and its scratch array onto the device (lazy
+        # module loading), which the free-memory check below must not count
+        m, t0 = _kkr(cases[1], ref.build_kkr)
+        assert _noalloc(lib, m, t0, stream)[0] == T.OK
         for prob in cases:  # two calls in a row, different n
             m, t0 = _kkr(prob, ref.build_kkr)
-            rc, got = _noalloc(lib, m, t0, stream)
+            rc, got, dfree = _noalloc(lib, m, t0, stream)
             assert rc == T.OK
+            assert dfree == 0, dfree  # no device memory was allocated by the call
             want = s.solve_tau00_dense(m, t0)
             assert np.abs(got - want).max() <= 1e-12 * np.abs(want).max()
+            b = t0.shape[0]
+            oracle = ref.calculate_tau(prob, 0, 0, ref.ZBLOCKLU_CPP).reshape(b, b).T + t0
+            assert np.abs(got - oracle).max() <= 1e-12 * np.abs(oracle).max()
     finally:
         s.close()
 
