@@ -308,12 +308,19 @@ def run_workload(args, world, rank, local):
     out = torch.empty(nj * b * b * 2, dtype=torch.float64, device=f"cuda:{local}")
     res = {}
     fallbacks = 0
+    phases = {}
     for name, prec in (("fp64", T.PREC_FP64), ("mixed", T.PREC_MIXED)):
         ms = timed(lambda: s.solve_jobs_device(jobs, out.data_ptr(), prec))
         s.sync()
         res[name] = (ms, out.cpu().numpy().view(np.complex128).reshape(nj, -1).copy())
         if name == "mixed":
             fallbacks = s.last_fallback_count
+        # device time per phase of one more step (CUDA events on the library stream)
+        s.set_profiling(True)
+        s.solve_jobs_device(jobs, out.data_ptr(), prec)
+        s.sync()
+        phases[name] = s.profile_phases()
+        s.set_profiling(False)
     f, m = res["fp64"][1], res["mixed"][1]
     err = float(max(np.abs(m[j] - f[j]).max() / np.abs(f[j]).max() for j in range(nj)))
     head = "mixed" if kind == "noncollinear" else "fp64"
@@ -326,6 +333,7 @@ def run_workload(args, world, rank, local):
                            "effective_tflops": flops / (res["mixed"][0] * 1e-3) / 1e12},
                  "err_mixed_vs_fp64_on_tau00_l": err,
                  "mixed_jobs_resolved_in_fp64": fallbacks,
+                 "phase_ms_per_step": phases,
                  "algorithmic_flops_per_step": flops})
     print(json.dumps(line))
     s.close()

@@ -163,6 +163,19 @@ int b200tau_solve_dense(b200tau_ctx *ctx, const double *m, int n, int ldm,
 int b200tau_solve_dense_noalloc(const double *m, int n, int ldm, const double *t0, int b,
                                 double *tau00, void *stream);
 
+/* Full tau = M^-1 T of one job, T = blockdiag(t_j) over every LIZ site j: the contract of the
+ * reference's solveTauFullzgetrf (src/MultipleScattering/linearSolvers_CPU.cpp:125-144; cuSOLVER
+ * variant linearSolvers_CUDA.cu:331-361), which the Kubo current matrix calls
+ * (src/Kubo/CurrentMatrix.cpp:184-222).  tau_full is n x n complex, column-major, host memory, in
+ * the reference's site order (central site first), n = n_spin_cant * nrmat of the job's atom.
+ * FP64 block factors of M (pivoting as b200tau_set_pivoting), M^-1 formed from them on the device,
+ * then each block column scaled by its site's t-matrix.  Two documented differences from the
+ * reference, both invisible when every site has the same lmax and the tmatStore group holds one
+ * energy (Kubo's use): t_j comes from the job's energy iie (the reference always reads the
+ * group's first energy) and each site's block has the site's own size (the reference places
+ * kkrsz_ns x kkrsz_ns blocks at multiples of kkrsz_ns). */
+int b200tau_solve_tau_full(b200tau_ctx *ctx, const b200tau_job *job, double *tau_full, int n);
+
 /* Build only: the KKR matrix M = 1 - t G for one job in the reference's site
  * order (central site first), written to host memory (n x n, ld = n) where
  * n = n_spin_cant * nrmat.  Parity hook for buildKKRMatrix*; not on the hot

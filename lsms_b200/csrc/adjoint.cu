@@ -224,7 +224,7 @@ cudaError_t gemm_launch(const JobDev *jobs, int njobs, int k, int max_m, int max
                         long *launches) {
   if (max_m <= 0 || max_n <= 0) return cudaSuccess;
   const int smem = 4 * kKc * kT * (int)sizeof(double2);
-  cudaError_t e = cudaFuncSetAttribute(zgemm_view_kernel<Op, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  cudaError_t e = ensure_smem(zgemm_view_kernel<Op, MODE>, smem);
   if (e != cudaSuccess) return e;
   zgemm_view_kernel<Op, MODE><<<dim3((max_n + kT - 1) / kT, (max_m + kT - 1) / kT, njobs), 256, smem, s>>>(jobs, k, Op());
   if (launches) *launches += 1;
@@ -324,7 +324,54 @@ __global__ void __launch_bounds__(256) vjp_assemble_kernel(const JobDev *__restr
   }
 }
 
+// Full tau = M^-1 T (T = blockdiag of the sites' t-matrices, positions order) into M's storage:
+// one CTA per (256 rows, position p, job), one row per thread; a thread reads the bp elements of
+// its row in the position's column block of M^-1 and writes the bp products with t_p.  With panel
+// pivoting V holds (P M)^-1, and column j of M^-1 is column rowpos[j] of V.
+__global__ void __launch_bounds__(256) tau_full_kernel(const JobDev *__restrict__ jobs, TmatView tv) {
+  const JobDev &J = jobs[blockIdx.z];
+  const int p = blockIdx.y;
+  if (p >= J.L || J.inactive) return;
+  const int off = J.off[p], bp = J.off[p + 1] - off;
+  const int site = J.perm[p];
+  const int kk = bp / tv.ns;  // (lmax + 1)^2 of the site
+  __shared__ double2 ts[kMaxB][kMaxB + 1];
+  // the site's t block, rows / columns s kk + l for the site's own l < kk (the build's gather)
+  const double2 *tb = tv.tmat + (long)J.store[site] * tv.tmat_ld + (long)J.iie * tv.blk + tv.jsm(J.ispin);
+  for (int e = threadIdx.x; e < bp * bp; e += 256) {
+    const int r = e % bp, c = e / bp;
+    const int sr = r / kk, lr = r - sr * kk, sc = c / kk, lc = c - sc * kk;
+    ts[r][c] = tb[(sr * tv.kkrsz + lr) + (long)(sc * tv.kkrsz + lc) * tv.bstore];
+  }
+  __syncthreads();
+  const int r = blockIdx.x * 256 + threadIdx.x;
+  if (r >= J.N) return;
+  const int *__restrict__ rowpos = J.piv != nullptr ? J.piv + J.ld : nullptr;
+  double2 v[kMaxB];
+#pragma unroll
+  for (int k = 0; k < kMaxB; ++k) {
+    const int j = off + k;
+    const int col = k < bp ? (rowpos != nullptr ? rowpos[j] : j) : 0;
+    v[k] = k < bp ? J.V[(size_t)r + (size_t)col * J.ld] : make_double2(0.0, 0.0);
+  }
+  for (int c = 0; c < bp; ++c) {
+    double2 acc = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int k = 0; k < kMaxB; ++k)
+      if (k < bp) acc = cfma(v[k], ts[k][c], acc);
+    J.M[(size_t)r + (size_t)(off + c) * J.ld] = acc;
+  }
+}
+
 }  // namespace
+
+cudaError_t launch_tau_full(const JobDev *jobs, int njobs, int max_L, int max_N, const TmatView &tv, cudaStream_t s,
+                            long *launches) {
+  if (njobs <= 0) return cudaSuccess;
+  tau_full_kernel<<<dim3((max_N + 255) / 256, max_L, njobs), 256, 0, s>>>(jobs, tv);
+  if (launches) *launches += 1;
+  return cudaGetLastError();
+}
 
 cudaError_t launch_inverse(const JobDev *jobs, int njobs, int max_n, int max_N, cudaStream_t s, long *launches) {
   if (njobs <= 0) return cudaSuccess;

@@ -294,6 +294,31 @@ void fill_slot(b200tau_ctx *ctx, JobDev &J, int slot, int ld, const Plan &p) {
   J.piv = nullptr;
 }
 
+// N x N workspace per slot for M^-1 (adjoint, full tau).
+int ensure_v(b200tau_ctx *ctx, int ld, int slots) {
+  const size_t v_need = (size_t)ld * ld;
+  if (ctx->d_V && v_need <= ctx->v_elems && slots <= ctx->v_slots) return B200TAU_OK;
+  CK(cudaStreamSynchronize(ctx->stream));
+  cudaFree(ctx->d_V);
+  ctx->d_V = nullptr;
+  ctx->v_elems = std::max(v_need, ctx->v_elems);
+  ctx->v_slots = std::max(slots, ctx->v_slots);
+  CK(cudaMalloc(&ctx->d_V, sizeof(double2) * ctx->v_elems * ctx->v_slots));
+  return B200TAU_OK;
+}
+
+TmatView tmat_view(const b200tau_ctx *ctx) {
+  TmatView v;
+  v.tmat = ctx->d_tmat;
+  v.tmat_ld = ctx->tmat_ld;
+  v.blk = ctx->blk;
+  v.kkrsz = ctx->kkrsz;
+  v.ns = ctx->ns;
+  v.bstore = ctx->ns * ctx->kkrsz;
+  v.colpol = ctx->npola != ctx->ns ? 1 : 0;
+  return v;
+}
+
 // The slot's panel-pivoting buffer (ensure_piv has sized it for the call).
 int *slot_piv(const b200tau_ctx *ctx, int slot) { return ctx->d_piv + (size_t)slot * ctx->piv_ints; }
 
@@ -1285,14 +1310,7 @@ int b200tau_solve_vjp(b200tau_ctx *ctx, const b200tau_job *jobs, int njobs, cons
   const int slots = choose_slots(ctx, ld, njobs, p, v_need * sizeof(double2));
   if ((rc = ensure_workspace(ctx, ld, slots, p))) return rc;
   if ((rc = ensure_jobs(ctx, slots))) return rc;
-  if (!ctx->d_V || v_need > ctx->v_elems || slots > ctx->v_slots) {
-    CK(cudaStreamSynchronize(ctx->stream));
-    cudaFree(ctx->d_V);
-    ctx->d_V = nullptr;
-    ctx->v_elems = std::max(v_need, ctx->v_elems);
-    ctx->v_slots = std::max(slots, ctx->v_slots);
-    CK(cudaMalloc(&ctx->d_V, sizeof(double2) * ctx->v_elems * ctx->v_slots));
-  }
+  if ((rc = ensure_v(ctx, ld, slots))) return rc;
   // output blocks: job j's sites start at block site_off[j] (caller's job order)
   std::vector<long> site_off(njobs + 1, 0);
   for (int j = 0; j < njobs; ++j) site_off[j + 1] = site_off[j] + ctx->atoms[jobs[j].atom].L;
@@ -1329,6 +1347,76 @@ int b200tau_solve_vjp(b200tau_ctx *ctx, const b200tau_job *jobs, int njobs, cons
     CK(cudaMemcpyAsync(dlogdet, adj.dlogdet, sizeof(double2) * bb * nblk, cudaMemcpyDeviceToHost, ctx->stream));
   CK(cudaStreamSynchronize(ctx->stream));
   return check_err_flags(ctx);
+}
+
+int b200tau_solve_tau_full(b200tau_ctx *ctx, const b200tau_job *job, double *tau_full, int n) {
+  if (!ctx) return B200TAU_ERR_ARG;
+  if (!job || !tau_full) return fail(ctx, B200TAU_ERR_ARG, "solve_tau_full: bad arguments");
+  int rc = validate_jobs(ctx, job, 1);
+  if (rc) return rc;
+  const AtomDev &a = ctx->atoms[job->atom];
+  if (n != a.N) return fail(ctx, B200TAU_ERR_ARG, "solve_tau_full: n %d != N %d", n, a.N);
+  CK(cudaSetDevice(ctx->device));
+  const int ld = round_up(a.N, 64);
+  Plan p;  // FP64 factors in M's own storage; M^-1 from them (no right-hand side to refine)
+  p.fk = kFactorFP64;
+  p.steps = 0;
+  p.f_separate = false;
+  if ((rc = ensure_workspace(ctx, ld, std::max(1, ctx->slots), p))) return rc;
+  if ((rc = ensure_jobs(ctx, 1))) return rc;
+  if ((rc = ensure_v(ctx, ld, 1))) return rc;
+  const bool panel = use_panel(ctx, a.N);
+  if (panel && (rc = ensure_piv(ctx, ld, 1))) return rc;
+  JobDev J;
+  std::memset(&J, 0, sizeof(J));
+  J.energy = make_double2(job->energy[0], job->energy[1]);
+  J.prel = make_double2(job->prel[0], job->prel[1]);
+  J.pos = a.pos;
+  J.lmax = a.lmax;
+  J.store = a.store;
+  J.perm = a.perm;
+  J.off = a.off;
+  fill_slot(ctx, J, 0, ld, p);
+  J.conv = nullptr;
+  J.cnorm = nullptr;
+  J.V = ctx->d_V;
+  if (panel) J.piv = slot_piv(ctx, 0);
+  J.L = a.L;
+  J.N = a.N;
+  J.b = a.b;
+  J.n = a.N - a.b;
+  J.iie = job->iie;
+  J.ispin = job->ispin;
+  CK(cudaMemcpyAsync(ctx->d_jobs, &J, sizeof(J), cudaMemcpyHostToDevice, ctx->stream));
+  if ((rc = reset_slot_status(ctx, 1))) return rc;
+  ctx->launches = 0;
+  CK(launch_kkr_build(ctx->d_jobs, 1, a.L, build_params(ctx, p), ctx->d_err, ctx->stream, &ctx->launches));
+  CK(launch_eliminate(kFactorFP64, ctx->d_jobs, 1, J.n, J.N, ctx->d_info, ctx->stream, &ctx->launches, nullptr,
+                      nullptr, ctx->d_err, false, nullptr, panel));
+  CK(launch_inverse(ctx->d_jobs, 1, J.n, J.N, ctx->stream, &ctx->launches));
+  CK(launch_tau_full(ctx->d_jobs, 1, a.L, a.N, tmat_view(ctx), ctx->stream, &ctx->launches));
+  // reference site order (central site first): rows/cols [0, r) <-> [b, N), [r, N) <-> [0, b)
+  const int r = a.N - a.b, b = a.b;
+  const size_t es = sizeof(double2);
+  double2 *hm = reinterpret_cast<double2 *>(tau_full);
+  const double2 *W = J.M;
+  if (r > 0) {
+    CK(cudaMemcpy2DAsync(hm + b + (size_t)b * n, n * es, W, ld * es, r * es, r, cudaMemcpyDeviceToHost,
+                         ctx->stream));
+    CK(cudaMemcpy2DAsync(hm + b, n * es, W + (size_t)r * ld, ld * es, r * es, b, cudaMemcpyDeviceToHost,
+                         ctx->stream));
+    CK(cudaMemcpy2DAsync(hm + (size_t)b * n, n * es, W + r, ld * es, b * es, r, cudaMemcpyDeviceToHost,
+                         ctx->stream));
+  }
+  CK(cudaMemcpy2DAsync(hm, n * es, W + r + (size_t)r * ld, ld * es, b * es, b, cudaMemcpyDeviceToHost,
+                       ctx->stream));
+  int info = 0;
+  CK(cudaMemcpyAsync(&info, ctx->d_info, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaMemcpyAsync(ctx->h_err, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+  CK(cudaStreamSynchronize(ctx->stream));
+  if ((rc = check_host_err(ctx))) return rc;
+  if (info) return fail(ctx, B200TAU_ERR_SINGULAR, "solve_tau_full: singular pivot (info %d)", info);
+  return B200TAU_OK;
 }
 
 int b200tau_build_kkr(b200tau_ctx *ctx, const b200tau_job *job, double *m_out, int n) {

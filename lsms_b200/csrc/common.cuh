@@ -263,6 +263,19 @@ cudaError_t launch_flow_sweep(const JobDev *jobs, int njobs, int b, int max_N, b
 // has not converged (its conv word is not kConverged), else 0.
 cudaError_t add_fallback_gate_node(cudaGraph_t g, cudaGraphNode_t *node, const JobDev *jobs, int njobs,
                                    cudaGraphConditionalHandle h);
+// The device tmatStore as the kernels that read t blocks see it: the b x b block of (store,
+// energy iie, spin) at tmat + store tmat_ld + iie blk + jsm(spin), leading dimension bstore.
+struct TmatView {
+  const double2 *tmat;
+  long tmat_ld;
+  int blk, kkrsz, ns, bstore;
+  int colpol;  // collinear spin-polarised: spin 1's block follows spin 0's
+  __host__ __device__ long jsm(int ispin) const { return colpol ? (long)kkrsz * kkrsz * ispin : 0; }
+};
+// Full tau = M^-1 T into M's storage (positions order), from V = M^-1 (or (P M)^-1 with panel
+// pivoting) and the sites' t-matrices; the contract of the reference's solveTauFullzgetrf.
+cudaError_t launch_tau_full(const JobDev *jobs, int njobs, int max_L, int max_N, const TmatView &tv, cudaStream_t s,
+                            long *launches);
 // Adjoint (adjoint.cu), FP64 factors: V = M^-1 from the block factors in F, then per LIZ site the
 // tau00 cotangent pull-back and d ln det M / d t (needs G in M, X refined, V).
 cudaError_t launch_inverse(const JobDev *jobs, int njobs, int max_n, int max_N, cudaStream_t s, long *launches);

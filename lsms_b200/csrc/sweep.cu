@@ -344,14 +344,12 @@ cudaError_t sweep_impl(const JobDev *jobs, int njobs, bool forward, int mode, cu
   cudaError_t e;
   if (forward) {
     const int smem = SweepSmem<T, V>::kForward;
-    if ((e = cudaFuncSetAttribute(forward_sweep_kernel<T, V, BC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  smem)) != cudaSuccess)
+    if ((e = ensure_smem(forward_sweep_kernel<T, V, BC>, smem)) != cudaSuccess)
       return e;
     return launch_cluster(forward_sweep_kernel<T, V, BC>, cs, njobs, 256, smem, s, jobs);
   }
   const int smem = SweepSmem<T, V>::kBackward;
-  if ((e = cudaFuncSetAttribute(backward_sweep_kernel<T, V, BC>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                smem)) != cudaSuccess)
+  if ((e = ensure_smem(backward_sweep_kernel<T, V, BC>, smem)) != cudaSuccess)
     return e;
   return launch_cluster(backward_sweep_kernel<T, V, BC>, cs, njobs, 256, smem, s, jobs, mode);
 }

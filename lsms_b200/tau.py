@@ -53,7 +53,7 @@ EXPORTS = (
     "b200tau_profile_read", "b200tau_set_mixed_engine", "b200tau_solve_dense_noalloc",
     "b200tau_profile_phases", "b200tau_set_mixed_sweep", "b200tau_solve_vjp",
     "b200tau_last_fallback_count", "b200tau_set_mixed_fallback", "b200tau_set_build_wait",
-    "b200tau_set_pivoting",
+    "b200tau_set_pivoting", "b200tau_solve_tau_full",
 )
 
 
@@ -111,6 +111,7 @@ def load_library():
     lib.b200tau_set_mixed_fallback.argtypes = [P, I]
     lib.b200tau_set_build_wait.argtypes = [P, L]
     lib.b200tau_set_pivoting.argtypes = [P, I]
+    lib.b200tau_solve_tau_full.argtypes = [P, P, P, I]
     _lib = lib
     return lib
 
@@ -313,6 +314,14 @@ class TauSolver:
         gl = [g[offs[k]:offs[k + 1]].transpose(0, 2, 1).copy() for k in range(n)]
         dl = None if d is None else [d[offs[k]:offs[k + 1]].transpose(0, 2, 1).copy() for k in range(n)]
         return tau.copy(), gl, dl
+
+    def solve_tau_full(self, atom: int, iie: int, ispin: int, energy: complex, n: int) -> np.ndarray:
+        """Full tau = M^-1 T (numpy [row, col], reference site order): solveTauFullzgetrf's
+        contract (linearSolvers_CPU.cpp:125-144), as the Kubo current matrix uses it."""
+        jobs = make_jobs([(atom, iie, ispin, energy)])
+        out = np.zeros((n * n,), np.complex128)
+        self._check(self.lib.b200tau_solve_tau_full(self.ctx, ctypes.cast(jobs, ctypes.c_void_p), _ptr(out), n))
+        return out.reshape(n, n).T.copy()
 
     def build_kkr(self, atom: int, iie: int, ispin: int, energy: complex, n: int) -> np.ndarray:
         """The device-built KKR matrix in the reference's site order (numpy [row, col])."""

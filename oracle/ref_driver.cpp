@@ -26,6 +26,8 @@ void calculateTauMatrix(LSMSSystemParameters &lsms, LocalTypeInfo &local,
 void buildKKRMatrixCPU(LSMSSystemParameters &lsms, LocalTypeInfo &local,
                        AtomData &atom, int ispin, int iie, Complex energy,
                        Complex prel, Matrix<Complex> &m);
+void solveTauFullzgetrf(LSMSSystemParameters &lsms, LocalTypeInfo &local, AtomData &atom, Matrix<Complex> &m,
+                        Matrix<Complex> &tau, int ispin);
 
 namespace {
 
@@ -139,6 +141,31 @@ int tauref_build_kkr(int lmax, int n_spin_cant, int n_spin_pola, int numLIZ,
     for (int i = 0; i < nrmat_ns; i++) {
       m_out[2 * ((size_t)i + (size_t)nrmat_ns * j)] = m(i, j).real();
       m_out[2 * ((size_t)i + (size_t)nrmat_ns * j) + 1] = m(i, j).imag();
+    }
+  return nrmat_ns;
+}
+
+// Full tau = M^-1 T: the reference's C++ build followed by its solveTauFullzgetrf
+// (src/MultipleScattering/linearSolvers_CPU.cpp:125-144), as src/Kubo/CurrentMatrix.cpp:184-190
+// calls them.
+int tauref_tau_full(int lmax, int n_spin_cant, int n_spin_pola, int numLIZ, const double *pos,
+                    const int *lizlmax, const int *storeIdx, int nstore, int group_size,
+                    const double *tmat, int iie, int ispin, double e_re, double e_im,
+                    double *tau_out) {
+  RefProblem p;
+  setup(p, lmax, n_spin_cant, n_spin_pola, 0x2000, numLIZ, pos, lizlmax,
+        storeIdx, nstore, group_size, tmat, nullptr, nullptr);
+  AtomData &atom = p.local.atom[0];
+  const Complex energy(e_re, e_im);
+  const Complex prel = std::sqrt(energy * (1.0 + energy * c2inv));
+  const int nrmat_ns = n_spin_cant * atom.nrmat;
+  Matrix<Complex> m(nrmat_ns, nrmat_ns), tau(nrmat_ns, nrmat_ns);
+  buildKKRMatrixCPU(p.lsms, p.local, atom, ispin, iie, energy, prel, m);
+  solveTauFullzgetrf(p.lsms, p.local, atom, m, tau, ispin);
+  for (int j = 0; j < nrmat_ns; j++)
+    for (int i = 0; i < nrmat_ns; i++) {
+      tau_out[2 * ((size_t)i + (size_t)nrmat_ns * j)] = tau(i, j).real();
+      tau_out[2 * ((size_t)i + (size_t)nrmat_ns * j) + 1] = tau(i, j).imag();
     }
   return nrmat_ns;
 }

@@ -44,6 +44,7 @@ def lib():
                                           D, D, P, P, P]
         _lib.tauref_build_kkr.argtypes = [I, I, I, I, P, P, P, I, I, P, I, I, D, D, P]
         _lib.tauref_tables.argtypes = [I, P, P, P]
+        _lib.tauref_tau_full.argtypes = [I, I, I, I, P, P, P, I, I, P, I, I, D, D, P]
         _lib.tauref_set_num_threads.argtypes = [I]
     return _lib
 
@@ -100,3 +101,15 @@ def build_kkr(prob, iie: int, ispin: int = 0) -> np.ndarray:
                            _ptr(pos), _ptr(lm), _ptr(si), tm.shape[0], tm.shape[1], _ptr(tm),
                            iie, ispin, e.real, e.imag, _ptr(m))
     return m.reshape(n, n).T.copy()
+
+
+def tau_full(prob, iie: int, ispin: int = 0) -> np.ndarray:
+    """The reference's solveTauFullzgetrf on its own M: tau = M^-1 T (N x N, numpy [row, col])."""
+    pos, lm, si, tm = _common(prob)
+    n = prob.nrmat_ns
+    out = np.zeros((n * n,), np.complex128)
+    e = complex(prob.energies[iie])
+    lib().tauref_tau_full(prob.lmax, prob.n_spin_cant, prob.n_spin_pola, prob.num_liz,
+                          _ptr(pos), _ptr(lm), _ptr(si), tm.shape[0], tm.shape[1], _ptr(tm),
+                          iie, ispin, e.real, e.imag, _ptr(out))
+    return out.reshape(n, n).T.copy()
