@@ -229,6 +229,14 @@ long b200tau_last_fallback_count(const b200tau_ctx *ctx);
  * returns its last refinement iterate. */
 int b200tau_set_mixed_fallback(b200tau_ctx *ctx, int enable);
 
+/* Run each wave of b200tau_solve / b200tau_solve_device as one CUDA graph (1, the default) or as
+ * separate kernel launches (0).  A wave's pipeline (KKR build, block elimination, refinement,
+ * tau00_l) is captured on first use of its shape (job count, sizes, buffers) and replayed for every
+ * later wave of that shape, so a call costs the host a few copies and one or two graph launches.
+ * Profiling (b200tau_set_profiling) times the separate launches instead.  No counterpart in the
+ * reference. */
+int b200tau_set_graphs(b200tau_ctx *ctx, int enable);
+
 /* Row pivoting of the block elimination (B200TAU_PIVOT_*), both precisions.  BLOCK pivots inside
  * each 64 x 64 diagonal block, as the reference's GPU solver inverts its diagonal blocks
  * (zblock_lu_cuda_c.cu:218-259).  PANEL picks each 64-column step's rows from every remaining

@@ -62,6 +62,15 @@ struct FallbackGraph {
   cudaGraphExec_t exec = nullptr;
 };
 
+// One captured wave pipeline (capi.cu, wave_graph): build, elimination, refinement and tau00_l of
+// every wave with the same shape and buffers; `launches` kernels per launch.
+struct WaveGraph {
+  std::vector<long long> key;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  long launches = 0;
+};
+
 struct b200tau_ctx {
   int device = 0;
   int lmax = 3, ns = 1, npola = 1, kkrsz = 16, b = 16, blk = 1024;
@@ -140,6 +149,8 @@ struct b200tau_ctx {
   // the mixed path's FP64 re-solve as graphs with a conditional body (fallback_graph)
   cudaStream_t cap_stream = nullptr;
   std::vector<FallbackGraph> fb;  // most recently used last
+  std::vector<WaveGraph> wg;      // captured wave pipelines, most recently used last
+  bool graphs_on = true;          // b200tau_set_graphs
   // converged flags after the first refinement rounds, copied back without a wait: the next
   // call's estimate of how many jobs the later rounds' sweeps serve
   int *h_hint = nullptr;
@@ -530,6 +541,20 @@ void drop_fallback_graphs(b200tau_ctx *ctx) {
 
 // Graph shapes kept per context: the waves of a call are full but for the last one.
 constexpr size_t kFallbackGraphs = 4;
+// Wave pipelines kept per context (the waves of an uneven batch have a few shapes).
+constexpr size_t kWaveGraphs = 16;
+
+void destroy_wave_graph(WaveGraph &g) {
+  if (g.exec) cudaGraphExecDestroy(g.exec);
+  if (g.graph) cudaGraphDestroy(g.graph);
+  g.exec = nullptr;
+  g.graph = nullptr;
+}
+
+void drop_wave_graphs(b200tau_ctx *ctx) {
+  for (auto &g : ctx->wg) destroy_wave_graph(g);
+  ctx->wg.clear();
+}
 
 // The FP64 re-solve of a mixed wave as one graph: a gate kernel, then a conditional node whose
 // body - the re-solve records (converged jobs inactive), FP64 block elimination, the FP64
@@ -688,6 +713,73 @@ int run_pipeline(b200tau_ctx *ctx, const std::vector<JobDev> &h, int nw, int max
   return phase_end(ctx, 2);
 }
 
+// The device pipeline of a wave whose records are in ctx->d_jobs, as one CUDA graph: KKR build,
+// block elimination (with its look-ahead stream), the initial solve and the refinement rounds (or
+// tau00 from the Schur block), tau00_l.  Every kernel reads its job's sizes and pointers from the
+// records in device memory, so one graph serves every wave of the same shape and buffers: a solve
+// call then costs the host a record copy and a graph launch, and a host that stalls between the
+// launches of a wave can no longer leave the GPU idle.  Captured on first use of its key; the
+// refinement's later rounds size their sweep clusters for all of the wave's jobs.  The FP64
+// re-solve of unconverged mixed jobs stays a separate graph (fallback_graph).
+int wave_graph(b200tau_ctx *ctx, int nw, int maxL, int maxn, int maxN, int ld, const Plan &p, bool panel,
+               const TcMaps *tc, WaveGraph **out) {
+  const bool fp32_sweep = p.fk == kFactorFP32 && ctx->mixed_sweep == B200TAU_SWEEP_FP32;
+  const std::vector<long long> key = {
+      nw, maxL, maxn, maxN, ld, ctx->b, ctx->ns, ctx->kkrsz, (long long)p.fk, p.steps, p.f_separate ? 1 : 0,
+      fp32_sweep ? 1 : 0, panel ? 1 : 0, tc != nullptr ? 1 : 0, ctx->slots, (long long)ctx->f_bytes,
+      ctx->tmat_ld, ctx->group_size, ctx->table_polls, (long long)(uintptr_t)ctx->d_jobs,
+      (long long)(uintptr_t)ctx->d_info, (long long)(uintptr_t)ctx->d_active, (long long)(uintptr_t)ctx->d_err,
+      (long long)(uintptr_t)ctx->d_tmat, (long long)(uintptr_t)ctx->d_tdiag, (long long)(uintptr_t)ctx->d_F,
+      (long long)(uintptr_t)ctx->d_pack, ctx->tc_ld, ctx->tc_slots};
+  for (size_t i = 0; i < ctx->wg.size(); ++i)
+    if (ctx->wg[i].key == key) {
+      const WaveGraph g = ctx->wg[i];  // most recently used last
+      ctx->wg.erase(ctx->wg.begin() + (long)i);
+      ctx->wg.push_back(g);
+      *out = &ctx->wg.back();
+      return B200TAU_OK;
+    }
+  if (!ctx->cap_stream) CK(cudaStreamCreateWithFlags(&ctx->cap_stream, cudaStreamNonBlocking));
+  WaveGraph g;
+  g.key = key;
+  cudaStream_t cs = ctx->cap_stream;
+  long n = 0;
+  cudaError_t e = cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal);
+  if (e == cudaSuccess) {
+    e = launch_kkr_build(ctx->d_jobs, nw, maxL, build_params(ctx, p), ctx->d_err, cs, &n);
+    if (e == cudaSuccess)
+      e = launch_eliminate(p.fk, ctx->d_jobs, nw, maxn, maxN, ctx->d_info, cs, &n, nullptr, tc, ctx->d_err, false,
+                           &ctx->la, panel);
+    if (p.steps > 0) {
+      const CUtensorMap *fmap = tc ? &tc->tFu : nullptr;
+      if (e == cudaSuccess)
+        e = launch_refine_begin(p.fk, ctx->d_jobs, nw, maxn, maxN, ctx->b, ctx->d_info, cs, &n, fp32_sweep, fmap);
+      for (int it = 0; it < p.steps && e == cudaSuccess; ++it)
+        e = launch_refine_round(p.fk, ctx->d_jobs, nw, maxn, maxN, ctx->b, true, ctx->d_info, cs, &n, fp32_sweep,
+                                fmap, 0, ctx->d_active);
+      if (e == cudaSuccess) e = launch_refine_end(ctx->d_jobs, nw, ctx->ns, ctx->kkrsz, cs, &n);
+    } else if (e == cudaSuccess) {
+      e = launch_finalize_direct(p.fk, ctx->d_jobs, nw, ctx->ns, ctx->kkrsz, ctx->d_info, cs, &n);
+    }
+    const cudaError_t ec = cudaStreamEndCapture(cs, &g.graph);
+    if (e == cudaSuccess) e = ec;
+  }
+  if (e == cudaSuccess) e = cudaGraphInstantiate(&g.exec, g.graph, 0);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    destroy_wave_graph(g);
+    return fail(ctx, B200TAU_ERR_CUDA, "capturing the wave pipeline: %s", cudaGetErrorString(e));
+  }
+  g.launches = n;
+  if (ctx->wg.size() >= kWaveGraphs) {
+    destroy_wave_graph(ctx->wg.front());
+    ctx->wg.erase(ctx->wg.begin());
+  }
+  ctx->wg.push_back(g);
+  *out = &ctx->wg.back();
+  return B200TAU_OK;
+}
+
 // Device buffers of one b200tau_solve_vjp call (job-indexed in the caller's order).
 struct AdjointBufs {
   const double2 *taubar;   // njobs x b x b
@@ -747,6 +839,25 @@ int run_wave(b200tau_ctx *ctx, const b200tau_job *jobs, const int *idx, int nw, 
   CK(cudaMemcpyAsync(ctx->d_jobs, h.data(), sizeof(JobDev) * nw, cudaMemcpyHostToDevice, ctx->stream));
   int rc = reset_slot_status(ctx, nw);
   if (rc) return rc;
+  if (ctx->graphs_on && !ctx->profiling && adj == nullptr) {
+    const TcMaps *tc = nullptr;
+    if (p.fk == kFactorFP32 && ctx->mixed_engine == B200TAU_ENGINE_TENSOR) {
+      if ((rc = ensure_tc(ctx, ld, std::max(nw, ctx->slots)))) return rc;
+      if ((rc = encode_factor_map(ctx, ld, ctx->slots))) return rc;
+      tc = &ctx->tc;
+    }
+    WaveGraph *g = nullptr;
+    if ((rc = wave_graph(ctx, nw, maxL, maxn, maxN, ld, p, panel, tc, &g))) return rc;
+    CK(cudaGraphLaunch(g->exec, ctx->stream));
+    ctx->launches += g->launches;
+    if (p.fk != kFactorFP32 || !ctx->fallback_on || p.steps == 0) return B200TAU_OK;
+    cudaGraphExec_t fb = nullptr;
+    if ((rc = ensure_fallback(ctx, ld)) || (rc = fallback_graph(ctx, nw, ld, ctx->b, ctx->ns, ctx->kkrsz, panel, &fb)))
+      return rc;
+    CK(cudaGraphLaunch(fb, ctx->stream));
+    ctx->launches += 1;
+    return B200TAU_OK;
+  }
   if (rc || (rc = phase_begin(ctx))) return rc;
   CK(launch_kkr_build(ctx->d_jobs, nw, maxL, build_params(ctx, p), ctx->d_err, ctx->stream, &ctx->launches));
   if ((rc = phase_end(ctx, 0))) return rc;
@@ -948,6 +1059,7 @@ void b200tau_destroy(b200tau_ctx *ctx) {
   if (ctx->la.diag) cudaEventDestroy(ctx->la.diag);
   if (ctx->la.s2) cudaStreamDestroy(ctx->la.s2);
   drop_fallback_graphs(ctx);
+  drop_wave_graphs(ctx);
   if (ctx->cap_stream) cudaStreamDestroy(ctx->cap_stream);
   if (ctx->hint_ev) cudaEventDestroy(ctx->hint_ev);
   if (ctx->h_hint) cudaFreeHost(ctx->h_hint);
@@ -1025,6 +1137,12 @@ int b200tau_set_mixed_engine(b200tau_ctx *ctx, int engine) {
   if (engine != B200TAU_ENGINE_TENSOR && engine != B200TAU_ENGINE_SIMT)
     return fail(ctx, B200TAU_ERR_ARG, "unknown engine %d", engine);
   ctx->mixed_engine = engine;
+  return B200TAU_OK;
+}
+
+int b200tau_set_graphs(b200tau_ctx *ctx, int enable) {
+  if (!ctx) return B200TAU_ERR_ARG;
+  ctx->graphs_on = enable != 0;
   return B200TAU_OK;
 }
 

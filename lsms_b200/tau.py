@@ -53,7 +53,7 @@ EXPORTS = (
     "b200tau_profile_read", "b200tau_set_mixed_engine", "b200tau_solve_dense_noalloc",
     "b200tau_profile_phases", "b200tau_set_mixed_sweep", "b200tau_solve_vjp",
     "b200tau_last_fallback_count", "b200tau_set_mixed_fallback", "b200tau_set_build_wait",
-    "b200tau_set_pivoting", "b200tau_solve_tau_full",
+    "b200tau_set_pivoting", "b200tau_solve_tau_full", "b200tau_set_graphs",
 )
 
 
@@ -112,6 +112,7 @@ def load_library():
     lib.b200tau_set_build_wait.argtypes = [P, L]
     lib.b200tau_set_pivoting.argtypes = [P, I]
     lib.b200tau_solve_tau_full.argtypes = [P, P, P, I]
+    lib.b200tau_set_graphs.argtypes = [P, I]
     _lib = lib
     return lib
 
@@ -197,6 +198,10 @@ class TauSolver:
     def set_mixed_fallback(self, enable: bool):
         """Re-solve unconverged mixed-precision jobs by FP64 block LU (default on)."""
         self._check(self.lib.b200tau_set_mixed_fallback(self.ctx, int(bool(enable))))
+
+    def set_graphs(self, enable: bool):
+        """Each wave as one captured CUDA graph (default) or as separate launches."""
+        self._check(self.lib.b200tau_set_graphs(self.ctx, int(bool(enable))))
 
     def set_pivoting(self, mode: int):
         """Row pivoting of the elimination: PIVOT_AUTO (default), PIVOT_BLOCK or PIVOT_PANEL."""

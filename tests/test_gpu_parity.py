@@ -348,3 +348,24 @@ def port_tau00_raw(prob, iie, tau00_l):
     Udb = np.kron(Ud, np.eye(kk))
     mg = Udb @ big_l @ Ub
     return mg + prob.t_block(int(prob.liz_store_idx[0]), iie)
+
+
+def test_wave_graphs_match_separate_launches(solver_factory):
+    """A wave replayed from its captured CUDA graph gives the results of the same kernels launched
+    one by one (FP64 bit for bit; MIXED within 1e-12, its later sweeps may size clusters
+    differently), and a second call replays the graph."""
+    prob = W.config_n2160(npts=6)
+    s = _solver(solver_factory, prob)
+    jobs = T.make_jobs([(0, i, 0, prob.energies[i]) for i in range(6)])
+    try:
+        s.set_graphs(False)
+        f_sep = s.solve_jobs(jobs, T.PREC_FP64)
+        m_sep = s.solve_jobs(jobs, T.PREC_MIXED)
+        s.set_graphs(True)
+        for _ in range(2):
+            f_g = s.solve_jobs(jobs, T.PREC_FP64)
+            m_g = s.solve_jobs(jobs, T.PREC_MIXED)
+            assert np.array_equal(f_g, f_sep)
+            assert max(tau_err(prob, i, 0, m_g[i], m_sep[i]) for i in range(6)) <= 1e-12
+    finally:
+        s.set_graphs(True)
