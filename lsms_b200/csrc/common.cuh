@@ -251,8 +251,6 @@ cudaError_t launch_refine_end(const JobDev *jobs, int njobs, int ns, int kkrsz, 
 // X (+)= Y).  `fp32_arith` selects FP32 arithmetic on FP32 factors.  max_N bounds the jobs' N.
 cudaError_t launch_sweep(FactorKind fk, const JobDev *jobs, int njobs, int b, int max_N, bool forward, int mode,
                          bool fp32_arith, const CUtensorMap *fmap, cudaStream_t s, int active_hint = 0);
-// Cluster size of the sweeps for a wave of njobs (sweep.cu).
-int sweep_cluster_size(int njobs);
 // The dataflow sweeps for FP32 factors in FP32 arithmetic with b <= 16 (sweep_flow.cu), operand
 // units loaded through `fmap` (TcMaps::tFu over the jobs' factor slots).  Sets *launched when it
 // took the launch; false (and cudaSuccess) without a map or when the shape does not fit its

@@ -20,6 +20,9 @@
 
 #include <cuda_runtime.h>
 
+#include <mutex>
+#include <vector>
+
 #include "common.cuh"
 #include "cluster.cuh"
 #include "cplx.cuh"
@@ -338,19 +341,65 @@ __global__ void __launch_bounds__(256) backward_sweep_kernel(const JobDev *__res
   cp_async_wait<0>();
 }
 
+// Clusters of `kern` (cs CTAs of 256 threads, smem bytes each) resident at once, cached per
+// (kernel, cs, smem); 0 when the query fails.
+int resident_clusters(const void *kern, int cs, int smem) {
+  struct Entry {
+    const void *kern;
+    int cs, smem, dev, v;
+  };
+  static std::mutex mu;
+  static std::vector<Entry> cache;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return 0;
+  std::lock_guard<std::mutex> lock(mu);
+  for (const Entry &c : cache)
+    if (c.kern == kern && c.cs == cs && c.smem == smem && c.dev == dev) return c.v;
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(cs, 1, 1);
+  cfg.blockDim = dim3(256, 1, 1);
+  cfg.dynamicSmemBytes = smem;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = cs;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  int v = 0;
+  if (cudaOccupancyMaxActiveClusters(&v, kern, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    v = 0;
+  }
+  cache.push_back({kern, cs, smem, dev, v});
+  return v;
+}
+
+// The largest power-of-two cluster (up to 8 CTAs) whose clusters for every job are resident at
+// once, at the kernel's real occupancy (several CTAs per SM where the shared memory allows): the
+// per-step latency chain of a job shrinks with its cluster, so one full wave of the largest
+// clusters is the fastest.
+template <typename K>
+int cluster_for(K *kern, int smem, int njobs) {
+  for (int cs = kMaxCluster; cs > 1; cs >>= 1)
+    if (resident_clusters(reinterpret_cast<const void *>(kern), cs, smem) >= njobs) return cs;
+  return 1;
+}
+
 template <typename T, typename V, int BC>
 cudaError_t sweep_impl(const JobDev *jobs, int njobs, bool forward, int mode, cudaStream_t s) {
-  const int cs = sweep_cluster_size(njobs);
   cudaError_t e;
   if (forward) {
     const int smem = SweepSmem<T, V>::kForward;
     if ((e = ensure_smem(forward_sweep_kernel<T, V, BC>, smem)) != cudaSuccess)
       return e;
+    const int cs = cluster_for(forward_sweep_kernel<T, V, BC>, smem, njobs);
     return launch_cluster(forward_sweep_kernel<T, V, BC>, cs, njobs, 256, smem, s, jobs);
   }
   const int smem = SweepSmem<T, V>::kBackward;
   if ((e = ensure_smem(backward_sweep_kernel<T, V, BC>, smem)) != cudaSuccess)
     return e;
+  const int cs = cluster_for(backward_sweep_kernel<T, V, BC>, smem, njobs);
   return launch_cluster(backward_sweep_kernel<T, V, BC>, cs, njobs, 256, smem, s, jobs, mode);
 }
 
@@ -362,13 +411,6 @@ cudaError_t sweep_b(const JobDev *jobs, int njobs, int b, bool forward, int mode
 
 }  // namespace
 
-// The largest power of two up to 8 with cs * njobs CTAs resident at once (one CTA per SM at
-// the sweeps' shared-memory sizes), so that one wave of jobs fills the GPU once.
-int sweep_cluster_size(int njobs) {
-  int cs = kMaxCluster;
-  while (cs > 1 && cs * njobs > tc_num_sms()) cs >>= 1;
-  return cs;
-}
 
 cudaError_t launch_sweep(FactorKind fk, const JobDev *jobs, int njobs, int b, int max_N, bool forward, int mode,
                          bool fp32_arith, const CUtensorMap *fmap, cudaStream_t s, int active_hint) {

@@ -541,7 +541,8 @@ struct Deferred {
 // Refinement rounds only (the initial solve has B = 0 above the central block).  own_max:
 // resident tiles per CTA (ceil(tiles / cs)).
 __global__ void __launch_bounds__(kBlock, 1)
-    forward_flow_kernel(const JobDev *__restrict__ jobs, int own_max, const __grid_constant__ CUtensorMap fmap) {
+    forward_flow_kernel(const JobDev *__restrict__ jobs, int own_max, const __grid_constant__ CUtensorMap fmap,
+                        int col0) {
   const JobDev &J = jobs[blockIdx.y];
   // uniform over the cluster: the flag changes only between launches
   if (converged(J.conv) || J.n == 0 || J.inactive) return;
@@ -549,7 +550,10 @@ __global__ void __launch_bounds__(kBlock, 1)
   const FlowLayout L = flow_layout(cs, own_max, true);
   extern __shared__ __align__(1024) unsigned char sm_raw[];
   const FlowSmem S(aligned_smem(sm_raw), L);
-  const int n = J.n, N = J.N, ld = J.ld, b = J.b, ns = L.ns, nsm = ns - 1, lns = __ffs(ns) - 1;
+  // this launch's right-hand-side columns: [col0, col0 + b) of R and Y
+  const int n = J.n, N = J.N, ld = J.ld, b = min(kCols, J.b - col0), ns = L.ns, nsm = ns - 1, lns = __ffs(ns) - 1;
+  double2 *const Rb = J.R + (size_t)col0 * ld;
+  double2 *const Yb = J.Y + (size_t)col0 * ld;
   int *conv = J.conv;
   const int tid = threadIdx.x, warp = tid >> 5, m = 32 * (warp & 3) + (tid & 31), r = m >> 1, p = m & 1;
   const int c0 = 8 * ((warp >> 2) & 1);
@@ -562,7 +566,7 @@ __global__ void __launch_bounds__(kBlock, 1)
       const int t = q + i * cs;
       for (int e = tid; e < kTileElems; e += kThreads) {
         const int c = e >> 6, rr = e & 63, gr = 64 * t + rr;
-        S.tiles[i * kTileElems + e] = (c < b && gr < N) ? to_v<float2>(__ldcg(J.R + (size_t)gr + (size_t)c * ld))
+        S.tiles[i * kTileElems + e] = (c < b && gr < N) ? to_v<float2>(__ldcg(Rb + (size_t)gr + (size_t)c * ld))
                                                         : make_float2(0.f, 0.f);
       }
     }
@@ -631,7 +635,7 @@ __global__ void __launch_bounds__(kBlock, 1)
           if (!ok) break;
           const float *dst = reinterpret_cast<const float *>(S.slots + slot * kTileElems);
           const bool live = r < kbd;
-          double *Yd = reinterpret_cast<double *>(J.Y);
+          double *Yd = reinterpret_cast<double *>(Yb);
 #pragma unroll
           for (int i = 0; i < 8; ++i) {
             const int c = c0 + i;
@@ -658,7 +662,7 @@ __global__ void __launch_bounds__(kBlock, 1)
         if (64 * t + 63 < n) continue;
         for (int e = tid; e < kTileElems; e += kThreads) {
           const int c = e >> 6, gr = 64 * t + (e & 63);
-          if (c < b && gr >= n && gr < N) J.R[(size_t)gr + (size_t)c * ld] = to_d(S.tiles[i * kTileElems + e]);
+          if (c < b && gr >= n && gr < N) Rb[(size_t)gr + (size_t)c * ld] = to_d(S.tiles[i * kTileElems + e]);
         }
       }
     } else if (tid == 0) {
@@ -672,14 +676,18 @@ __global__ void __launch_bounds__(kBlock, 1)
 // (and skips converged jobs).
 __global__ void __launch_bounds__(kBlock, 1)
     backward_flow_kernel(const JobDev *__restrict__ jobs, int own_max, int mode,
-                         const __grid_constant__ CUtensorMap fmap) {
+                         const __grid_constant__ CUtensorMap fmap, int col0) {
   const JobDev &J = jobs[blockIdx.y];
   if ((mode == 1 && converged(J.conv)) || J.inactive) return;
   const int q = cluster_rank(), cs = cluster_size(), csm = cs - 1, lcs = __ffs(cs) - 1;
   const FlowLayout L = flow_layout(cs, own_max, false);
   extern __shared__ __align__(1024) unsigned char sm_raw[];
   const FlowSmem S(aligned_smem(sm_raw), L);
-  const int n = J.n, ld = J.ld, b = J.b, ns = L.ns, nsm = ns - 1, lns = __ffs(ns) - 1;
+  // bc: rows of the central block; b: this launch's right-hand-side columns [col0, col0 + b) of Y, X
+  const int n = J.n, ld = J.ld, bc = J.b, b = min(kCols, J.b - col0), ns = L.ns, nsm = ns - 1,
+            lns = __ffs(ns) - 1;
+  const double2 *const Yb = J.Y + (size_t)col0 * ld;
+  double2 *const Xb = J.X + (size_t)col0 * ld;
   int *conv = J.conv;
   const int tid = threadIdx.x;
   const int kstart = n > 0 ? ((n - 1) / 64) * 64 : 0;  // last block
@@ -694,25 +702,25 @@ __global__ void __launch_bounds__(kBlock, 1)
       const int t = q + i * cs;
       for (int e = tid; e < kTileElems; e += kThreads) {
         const int c = e >> 6, gr = 64 * t + (e & 63);
-        S.tiles[i * kTileElems + e] = (c < b && gr < n) ? to_v<float2>(__ldcg(J.Y + (size_t)gr + (size_t)c * ld))
+        S.tiles[i * kTileElems + e] = (c < b && gr < n) ? to_v<float2>(__ldcg(Yb + (size_t)gr + (size_t)c * ld))
                                                         : make_float2(0.f, 0.f);
       }
     }
     // step 0, the central block from the Schur solve: every CTA fills its own slot 0 (column-major)
     for (int e = tid; e < kTileElems; e += kThreads) {
       const int c = e >> 6, row = e & 63;
-      S.slots[e] = (row < b && c < b) ? to_v<float2>(__ldcg(J.Y + (size_t)(n + row) + (size_t)c * ld))
-                                      : make_float2(0.f, 0.f);
+      S.slots[e] = (row < bc && c < b) ? to_v<float2>(__ldcg(Yb + (size_t)(n + row) + (size_t)c * ld))
+                                       : make_float2(0.f, 0.f);
     }
     if (q == 0) {  // X_c (+)= Y_c
-      for (int e = tid; e < b * b; e += kThreads) {
-        const size_t idx = (size_t)(n + e % b) + (size_t)(e / b) * ld;
-        const double2 y = __ldcg(J.Y + idx);
+      for (int e = tid; e < bc * b; e += kThreads) {
+        const size_t idx = (size_t)(n + e % bc) + (size_t)(e / bc) * ld;
+        const double2 y = __ldcg(Yb + idx);
         if (mode == 0) {
-          J.X[idx] = y;
+          Xb[idx] = y;
         } else {
-          const double2 x = J.X[idx];
-          J.X[idx] = make_double2(x.x + y.x, x.y + y.y);
+          const double2 x = Xb[idx];
+          Xb[idx] = make_double2(x.x + y.x, x.y + y.y);
         }
       }
     }
@@ -722,7 +730,7 @@ __global__ void __launch_bounds__(kBlock, 1)
   const uint32_t tmem = *S.tmem;
   if (tid == 0) mbar_arrive_local(S.full, kWarps);
 
-  BwdItems it{n, b, cs, csm, q, kstart, nsteps};
+  BwdItems it{n, bc, cs, csm, q, kstart, nsteps};
   it.begin();
   if (tid >= kThreads) {
     if (tid == kThreads)
@@ -741,7 +749,7 @@ __global__ void __launch_bounds__(kBlock, 1)
       if (!ok) break;
       const int ks = s == 0 ? n : kstart - 64 * (s - 1);
       const int tnext = s + 1 < nsteps ? (kstart - 64 * s) / 64 : -1;  // tile of block s + 1
-      if (!it.fin && it.s == s) build_b(S.bstep, S.slots + (s & nsm) * kTileElems, s == 0 ? b : min(64, n - ks));
+      if (!it.fin && it.s == s) build_b(S.bstep, S.slots + (s & nsm) * kTileElems, s == 0 ? bc : min(64, n - ks));
       fence_proxy_async();
       compute_sync();  // every warp is done with slot s % ns
       if (tid == 0) mbar_arrive_cluster(S.empty + (s & nsm), bwd_producer(s + ns, p0, csm));
@@ -787,10 +795,10 @@ __global__ void __launch_bounds__(kBlock, 1)
                 const size_t idx = (size_t)(kn + r0 + e) + (size_t)c * ld;
                 const double2 yd = make_double2(e ? y.z : y.x, e ? y.w : y.y);
                 if (mode == 0) {
-                  J.X[idx] = yd;
+                  Xb[idx] = yd;
                 } else {
-                  const double2 x = J.X[idx];
-                  J.X[idx] = make_double2(x.x + yd.x, x.y + yd.y);
+                  const double2 x = Xb[idx];
+                  Xb[idx] = make_double2(x.x + yd.x, x.y + yd.y);
                 }
               }
             }
@@ -850,7 +858,7 @@ int active_clusters(const void *kern, int cs, int smem) {
 cudaError_t launch_flow_sweep(const JobDev *jobs, int njobs, int b, int max_N, bool forward, int mode,
                               const CUtensorMap *fmap, cudaStream_t s, bool *launched, int active_hint) {
   *launched = false;
-  if (njobs <= 0 || b > kCols || max_N <= 0 || fmap == nullptr) return cudaSuccess;
+  if (njobs <= 0 || b > 2 * kCols || max_N <= 0 || fmap == nullptr) return cudaSuccess;
   const int T = (max_N + 63) / 64;
   const void *kern = forward ? reinterpret_cast<const void *>(forward_flow_kernel)
                              : reinterpret_cast<const void *>(backward_flow_kernel);
@@ -872,10 +880,14 @@ cudaError_t launch_flow_sweep(const JobDev *jobs, int njobs, int b, int max_N, b
   const FlowLayout L = flow_layout(cs, (T + cs - 1) / cs, forward);
   cudaError_t e = ensure_smem(kern, L.total);
   if (e != cudaSuccess) return e;
-  if (forward)
-    e = launch_cluster(forward_flow_kernel, cs, njobs, kBlock, L.total, s, jobs, L.own, *fmap);
-  else
-    e = launch_cluster(backward_flow_kernel, cs, njobs, kBlock, L.total, s, jobs, L.own, mode, *fmap);
+  // the sweeps are column-separable: more than kCols right-hand-side columns take one launch per
+  // kCols of them (the factor units stream once per launch)
+  for (int col0 = 0; col0 < b && e == cudaSuccess; col0 += kCols) {
+    if (forward)
+      e = launch_cluster(forward_flow_kernel, cs, njobs, kBlock, L.total, s, jobs, L.own, *fmap, col0);
+    else
+      e = launch_cluster(backward_flow_kernel, cs, njobs, kBlock, L.total, s, jobs, L.own, mode, *fmap, col0);
+  }
   if (e == cudaSuccess) *launched = true;
   return e;
 }
