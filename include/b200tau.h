@@ -183,9 +183,21 @@ int b200tau_solve_tau_full(b200tau_ctx *ctx, const b200tau_job *job, double *tau
 int b200tau_build_kkr(b200tau_ctx *ctx, const b200tau_job *job, double *m_out,
                       int n);
 
+/* Keep the factors of a forward solve for the adjoint (1), or not (0, the default).  While on, a
+ * PREC_FP64 b200tau_solve / b200tau_solve_device whose jobs fit one wave (and whose matrices are
+ * eliminated with BLOCK pivoting) leaves its KKR matrices, FP64 block factors and refined
+ * solutions in the workspace, and the next b200tau_solve_vjp on the same jobs in the same order
+ * reuses them: no KKR build, no elimination, no refinement, only M^-1 from the kept factors and
+ * the per-site contractions.  Any other call on the context (another solve, an upload, a dense,
+ * full-tau or build call) drops them; so does the vjp that uses them.  The forward pass of an
+ * LSMS energy point then pays one factorisation for tau00 and its derivatives.  No counterpart in
+ * the reference. */
+int b200tau_set_keep_factors(b200tau_ctx *ctx, int enable);
+
 /* Reverse-mode derivatives, for each job, of tau00 and of ln det M with respect to the
  * t-matrix t_j of every LIZ site j, from the FP64 block factors of the job's own forward solve
- * (one factorisation; M^-1 is formed from the factors).  No counterpart in the reference.
+ * (one factorisation; M^-1 is formed from the factors; with b200tau_set_keep_factors those of the
+ * preceding forward solve of the same jobs).  No counterpart in the reference.
  *   taubar  (in)  b x b cotangent on the raw tau00 = [M^-1]_00 t_0 of each job (not minus t0,
  *                 unrotated), jobs one after another (2 b^2 doubles per job).
  *   tau00   (out) that tau00 per job, or NULL.

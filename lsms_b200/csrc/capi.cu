@@ -151,6 +151,13 @@ struct b200tau_ctx {
   std::vector<FallbackGraph> fb;  // most recently used last
   std::vector<WaveGraph> wg;      // captured wave pipelines, most recently used last
   bool graphs_on = true;          // b200tau_set_graphs
+  // b200tau_set_keep_factors: the last FP64 solve's wave (factors F, KKR matrix M, refined X, slots
+  // in `kept_order` order), reusable once by b200tau_solve_vjp on the same jobs
+  bool keep_factors = false;
+  bool kept_valid = false;
+  std::vector<b200tau_job> kept_jobs;
+  std::vector<int> kept_order;
+  int kept_ld = 0;
   // converged flags after the first refinement rounds, copied back without a wait: the next
   // call's estimate of how many jobs the later rounds' sweeps serve
   int *h_hint = nullptr;
@@ -789,7 +796,7 @@ struct AdjointBufs {
 };
 
 int run_wave(b200tau_ctx *ctx, const b200tau_job *jobs, const int *idx, int nw, int ld, const Plan &p,
-             double2 *out_base, const AdjointBufs *adj = nullptr) {
+             double2 *out_base, const AdjointBufs *adj = nullptr, bool reuse_factors = false) {
   std::vector<JobDev> h(nw);
   int maxL = 0, maxN = 0, maxn = 0;
   for (int w = 0; w < nw; ++w) maxN = std::max(maxN, ctx->atoms[jobs[idx[w]].atom].N);
@@ -837,6 +844,18 @@ int run_wave(b200tau_ctx *ctx, const b200tau_job *jobs, const int *idx, int nw, 
     maxn = std::max(maxn, a.N - a.b);
   }
   CK(cudaMemcpyAsync(ctx->d_jobs, h.data(), sizeof(JobDev) * nw, cudaMemcpyHostToDevice, ctx->stream));
+  if (reuse_factors) {
+    // the forward solve of these jobs left M, its FP64 block factors and the refined X in these
+    // slots: raw tau00 from X, then the adjoint's own launches, no second factorisation
+    CK(launch_refine_end(ctx->d_jobs, nw, ctx->ns, ctx->kkrsz, ctx->stream, &ctx->launches));
+    BuildParams gp = build_params(ctx, p);
+    gp.f_kind = 0;
+    gp.g_mode = 1;
+    CK(launch_kkr_build(ctx->d_jobs, nw, maxL, gp, ctx->d_err, ctx->stream, &ctx->launches));
+    CK(launch_inverse(ctx->d_jobs, nw, maxn, maxN, ctx->stream, &ctx->launches));
+    CK(launch_vjp_assemble(ctx->d_jobs, nw, maxL, ctx->kkrsz, ctx->ns, ctx->stream, &ctx->launches));
+    return B200TAU_OK;
+  }
   int rc = reset_slot_status(ctx, nw);
   if (rc) return rc;
   if (ctx->graphs_on && !ctx->profiling && adj == nullptr) {
@@ -951,6 +970,7 @@ int solve_impl(b200tau_ctx *ctx, const b200tau_job *jobs, int njobs, int prec, d
   if (use_panel(ctx, maxN) && (rc = ensure_piv(ctx, ld, slots))) return rc;
   ctx->launches = 0;
   if (ctx->d_fbcount) CK(cudaMemsetAsync(ctx->d_fbcount, 0, sizeof(int), ctx->stream));
+  ctx->kept_valid = false;
   for (int w0 = 0; w0 < njobs; w0 += slots) {
     const int nw = std::min(slots, njobs - w0);
     if ((rc = run_wave(ctx, jobs, &order[w0], nw, ld, p, dev_out))) return rc;
@@ -958,7 +978,29 @@ int solve_impl(b200tau_ctx *ctx, const b200tau_job *jobs, int njobs, int prec, d
   }
   ctx->info_order = order;
   ctx->info_jobs = njobs;
+  // one FP64 wave with M kept beside its block factors, X refined, pivots inside the diagonal blocks:
+  // what b200tau_solve_vjp needs from a forward solve
+  if (ctx->keep_factors && njobs <= slots && p.fk == kFactorFP64 && p.f_separate && p.steps > 0 &&
+      !use_panel(ctx, maxN)) {
+    ctx->kept_jobs.assign(jobs, jobs + njobs);
+    ctx->kept_order = order;
+    ctx->kept_ld = ld;
+    ctx->kept_valid = true;
+  }
   return B200TAU_OK;
+}
+
+bool same_jobs(const b200tau_job &a, const b200tau_job &b) {
+  return a.atom == b.atom && a.iie == b.iie && a.ispin == b.ispin && a.energy[0] == b.energy[0] &&
+         a.energy[1] == b.energy[1] && a.prel[0] == b.prel[0] && a.prel[1] == b.prel[1];
+}
+
+// Does the kept forward wave hold exactly these jobs (same order)?
+bool kept_matches(const b200tau_ctx *ctx, const b200tau_job *jobs, int njobs) {
+  if (!ctx->kept_valid || (int)ctx->kept_jobs.size() != njobs) return false;
+  for (int j = 0; j < njobs; ++j)
+    if (!same_jobs(ctx->kept_jobs[j], jobs[j])) return false;
+  return true;
 }
 
 // The device error word as copied to ctx->h_err by the caller's last enqueued read (the stream
@@ -1140,6 +1182,13 @@ int b200tau_set_mixed_engine(b200tau_ctx *ctx, int engine) {
   return B200TAU_OK;
 }
 
+int b200tau_set_keep_factors(b200tau_ctx *ctx, int enable) {
+  if (!ctx) return B200TAU_ERR_ARG;
+  ctx->keep_factors = enable != 0;
+  if (!enable) ctx->kept_valid = false;
+  return B200TAU_OK;
+}
+
 int b200tau_set_graphs(b200tau_ctx *ctx, int enable) {
   if (!ctx) return B200TAU_ERR_ARG;
   ctx->graphs_on = enable != 0;
@@ -1186,6 +1235,7 @@ int b200tau_set_refinement(b200tau_ctx *ctx, int prec, int steps) {
 
 int b200tau_upload_tmat(b200tau_ctx *ctx, const double *tmat_store, long ld, int nstore, int blk_size) {
   if (!ctx) return B200TAU_ERR_ARG;
+  ctx->kept_valid = false;
   if (!tmat_store || nstore <= 0 || blk_size != ctx->blk || ld < blk_size || ld % blk_size)
     return fail(ctx, B200TAU_ERR_ARG, "upload_tmat: bad arguments (ld %ld, nstore %d, blk %d, expected blk %d)",
                 ld, nstore, blk_size, ctx->blk);
@@ -1237,6 +1287,7 @@ int b200tau_set_atom(b200tau_ctx *ctx, int atom, int num_liz, const double *liz_
                      const int *liz_lmax, const int *liz_store_idx, const double *ubr,
                      const double *ubrd) {
   if (!ctx) return B200TAU_ERR_ARG;
+  ctx->kept_valid = false;
   if (atom < 0 || num_liz < 1 || !liz_pos || !liz_lmax || !liz_store_idx)
     return fail(ctx, B200TAU_ERR_ARG, "set_atom: bad arguments");
   if (ctx->ns == 2 && (!ubr || !ubrd))
@@ -1350,6 +1401,7 @@ int b200tau_sync(b200tau_ctx *ctx) {
 int b200tau_solve_dense(b200tau_ctx *ctx, const double *m, int n, int ldm, const double *t0, int b,
                         int prec, double *tau00) {
   if (!ctx) return B200TAU_ERR_ARG;
+  ctx->kept_valid = false;
   if (!m || !t0 || !tau00 || n < 1 || b < 1 || b > n || b > kMaxB || ldm < n)
     return fail(ctx, B200TAU_ERR_ARG, "solve_dense: bad arguments (n %d, b %d, ldm %d)", n, b, ldm);
   int rc = check_prec(ctx, prec);
@@ -1425,7 +1477,10 @@ int b200tau_solve_vjp(b200tau_ctx *ctx, const b200tau_job *jobs, int njobs, cons
   const int maxN = ctx->atoms[jobs[order[0]].atom].N;
   const int ld = round_up(maxN, 64);
   const size_t v_need = (size_t)ld * ld;
-  const int slots = choose_slots(ctx, ld, njobs, p, v_need * sizeof(double2));
+  // the factors kept by a forward FP64 solve of these jobs (b200tau_set_keep_factors), used once
+  const bool reuse = kept_matches(ctx, jobs, njobs) && ctx->kept_ld == ld && ctx->kept_order == order;
+  ctx->kept_valid = false;
+  const int slots = reuse ? njobs : choose_slots(ctx, ld, njobs, p, v_need * sizeof(double2));
   if ((rc = ensure_workspace(ctx, ld, slots, p))) return rc;
   if ((rc = ensure_jobs(ctx, slots))) return rc;
   if ((rc = ensure_v(ctx, ld, slots))) return rc;
@@ -1453,7 +1508,7 @@ int b200tau_solve_vjp(b200tau_ctx *ctx, const b200tau_job *jobs, int njobs, cons
   std::vector<int> info(slots);
   for (int w0 = 0; w0 < njobs; w0 += slots) {
     const int nw = std::min(slots, njobs - w0);
-    if ((rc = run_wave(ctx, jobs, &order[w0], nw, ld, p, ctx->d_out, &adj))) return rc;
+    if ((rc = run_wave(ctx, jobs, &order[w0], nw, ld, p, ctx->d_out, &adj, reuse))) return rc;
     CK(cudaMemcpyAsync(info.data(), ctx->d_info, sizeof(int) * nw, cudaMemcpyDeviceToHost, ctx->stream));
     CK(cudaStreamSynchronize(ctx->stream));
     if ((rc = check_info(ctx, info.data(), &order[w0], nw))) return rc;
@@ -1469,6 +1524,7 @@ int b200tau_solve_vjp(b200tau_ctx *ctx, const b200tau_job *jobs, int njobs, cons
 
 int b200tau_solve_tau_full(b200tau_ctx *ctx, const b200tau_job *job, double *tau_full, int n) {
   if (!ctx) return B200TAU_ERR_ARG;
+  ctx->kept_valid = false;
   if (!job || !tau_full) return fail(ctx, B200TAU_ERR_ARG, "solve_tau_full: bad arguments");
   int rc = validate_jobs(ctx, job, 1);
   if (rc) return rc;
@@ -1539,6 +1595,7 @@ int b200tau_solve_tau_full(b200tau_ctx *ctx, const b200tau_job *job, double *tau
 
 int b200tau_build_kkr(b200tau_ctx *ctx, const b200tau_job *job, double *m_out, int n) {
   if (!ctx) return B200TAU_ERR_ARG;
+  ctx->kept_valid = false;
   if (!job || !m_out) return fail(ctx, B200TAU_ERR_ARG, "build_kkr: bad arguments");
   int rc = validate_jobs(ctx, job, 1);
   if (rc) return rc;

@@ -54,6 +54,7 @@ EXPORTS = (
     "b200tau_profile_phases", "b200tau_set_mixed_sweep", "b200tau_solve_vjp",
     "b200tau_last_fallback_count", "b200tau_set_mixed_fallback", "b200tau_set_build_wait",
     "b200tau_set_pivoting", "b200tau_solve_tau_full", "b200tau_set_graphs",
+    "b200tau_set_keep_factors",
 )
 
 
@@ -113,6 +114,7 @@ def load_library():
     lib.b200tau_set_pivoting.argtypes = [P, I]
     lib.b200tau_solve_tau_full.argtypes = [P, P, P, I]
     lib.b200tau_set_graphs.argtypes = [P, I]
+    lib.b200tau_set_keep_factors.argtypes = [P, I]
     _lib = lib
     return lib
 
@@ -198,6 +200,10 @@ class TauSolver:
     def set_mixed_fallback(self, enable: bool):
         """Re-solve unconverged mixed-precision jobs by FP64 block LU (default on)."""
         self._check(self.lib.b200tau_set_mixed_fallback(self.ctx, int(bool(enable))))
+
+    def set_keep_factors(self, enable: bool):
+        """Keep an FP64 solve's factors for the next solve_vjp on the same jobs."""
+        self._check(self.lib.b200tau_set_keep_factors(self.ctx, int(bool(enable))))
 
     def set_graphs(self, enable: bool):
         """Each wave as one captured CUDA graph (default) or as separate launches."""

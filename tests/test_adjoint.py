@@ -163,3 +163,44 @@ def test_autograd_function_gradient_of_a_real_loss(solver_factory):
     cs = A.complex_step(prob, iie, np.conj(w.numpy()), pairs)
     for (site, l), (dl, _) in zip(pairs, cs):
         assert abs(delta.grad[site, l].item() - dl.real) <= TOL_CS * np.abs([c[0] for c in cs]).max()
+
+
+@pytest.mark.gpu
+def test_vjp_reuses_the_forward_factors():
+    """With b200tau_set_keep_factors, the vjp after an FP64 forward solve of the same jobs
+    reuses that solve's factors: no KKR build of M, no elimination and no refinement launches (the
+    launch count drops by at least the elimination's three launches per 64-column step), and the
+    gradients are those of a vjp with its own factorisation, bit for bit.  The kept factors serve
+    one vjp; the next vjp factorises again."""
+    prob = W.make_problem("fcc", 6.82, 6, 3, [0.45 + 0.05j, 0.2 + 0.2j], 23, n_species=None)
+    assert prob.nrmat_ns == 1392
+    s = T.TauSolver(3, 1, 1)
+    try:
+        s.load_problem(prob)
+        jobs = T.make_jobs([(0, i, 0, prob.energies[i]) for i in range(2)])
+        rng = np.random.default_rng(9)
+        tb = rng.normal(size=(2, 16, 16)) + 1j * rng.normal(size=(2, 16, 16))
+        Ls = [prob.num_liz] * 2
+        ref_out = s.solve_vjp(jobs, tb, Ls)
+        full_launches = s.last_launch_count
+        s.set_keep_factors(True)
+        fwd = s.solve_jobs(jobs, T.PREC_FP64)
+        kept_out = s.solve_vjp(jobs, tb, Ls)
+        kept_launches = s.last_launch_count
+        again = s.solve_vjp(jobs, tb, Ls)  # the kept factors were used: this one factorises
+        again_launches = s.last_launch_count
+        s.set_keep_factors(False)
+        steps = (prob.nrmat_ns - 16 + 63) // 64
+        assert kept_launches <= full_launches - 3 * steps, (kept_launches, full_launches)
+        assert again_launches == full_launches
+        for a, b in zip(ref_out, kept_out):
+            if isinstance(a, list):
+                for x, y in zip(a, b):
+                    assert np.array_equal(x, y)
+            else:
+                assert np.array_equal(a, b)
+        for i in range(2):  # the forward tau00_l is the vjp's tau00 minus t0
+            t0 = prob.t_block(int(prob.liz_store_idx[0]), i)
+            assert np.abs(fwd[i].reshape(16, 16).T + t0 - kept_out[0][i]).max() <= 1e-13 * np.abs(t0).max()
+    finally:
+        s.close()
