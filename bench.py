@@ -39,10 +39,14 @@ sys.path.insert(0, ROOT)
 
 METRIC = "tau00 solves/s at N=2160 c128: mixed vs plain FP64 at <=1e-10 rel err; %peak"
 N_ENERGIES = 31
+DATA = "synthetic (seeded phase-shift t-matrices, fcc LIZ)"
+CONFIG = {"workload": "fcc LIZ 135 sites a=6.82, lmax 3, N=2160, kkrsz_ns 16, 31-point semicircle contour "
+                      "-0.3..0.7 Ry, one atom per GPU"}
 # DRAM bytes (read + write) of the trailing update per elimination step of this workload (the
-# update of the next diagonal tile plus the interior launch): the ncu capture of a 24-job interior
-# launch at k = 192 (profiles/tc_update_contour2160_e24.md) measured 17.4 B per trailing-block
-# entry; scaled to 31 jobs and the average trailing block over the 34 steps (1.476e6 entries).
+# update of the next diagonal tile plus the interior launch): an ncu capture of the trailing-update
+# kernel on a 24-job interior launch at k = 192 measured 17.4 B per trailing-block entry; scaled to
+# 31 jobs and the average trailing block over the 34 steps (1.476e6 entries).  Not measured by
+# this run (a kernel under ncu is not timed).
 TRAFFIC_PER_LAUNCH = 796.1e6
 
 
@@ -134,7 +138,10 @@ def measured_peaks():
 
 
 def run_reference(args, world, rank):
-    """Reference CPU implementation timed on the host cores (rank 0 only)."""
+    """Reference CPU implementation timed on the host cores (rank 0 only): the reference's own
+    calculateTauMatrix (oracle/_ref, build 0x2000 + zblock_lu 0x2005) on the same workload as the
+    GPU arm.  A step is the whole 31-point contour when --steps K of them fit about two and a half
+    minutes, else the first energies of the contour that do (every step the same sample)."""
     if rank != 0:
         return
     from lsms_b200 import workloads as W
@@ -144,43 +151,86 @@ def run_reference(args, world, rank):
         return
     cores = os.cpu_count() or 1
     reflib.set_num_threads(cores)
-    prob = W.config_n2160(npts=N_ENERGIES)
-    for i in range(args.warmup):
-        reflib.calculate_tau(prob, i % N_ENERGIES, 0, reflib.ZBLOCKLU_CPP)
+    prob = W.config_n2160(seed=2, npts=N_ENERGIES)
     t0 = time.perf_counter()
-    for i in range(args.steps):
-        reflib.calculate_tau(prob, i % N_ENERGIES, 0, reflib.ZBLOCKLU_CPP)
+    reflib.calculate_tau(prob, 0, 0, reflib.ZBLOCKLU_CPP)  # one solve: the time of a solve
+    t_solve = time.perf_counter() - t0
+    per_step = int(min(N_ENERGIES, max(1, 150.0 / max(1, args.steps + args.warmup) / max(t_solve, 1e-3))))
+
+    def step():
+        for i in range(per_step):
+            reflib.calculate_tau(prob, i, 0, reflib.ZBLOCKLU_CPP)
+
+    for _ in range(args.warmup):
+        step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        step()
     dt = (time.perf_counter() - t0) / args.steps
-    value = 1.0 / dt
+    value = per_step / dt
+    sample = (f"the {per_step} first of the 31 contour solves at N=2160 per step, one after another, "
+              f"OpenBLAS on {cores} threads")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-        "config": {"workload": "fcc LIZ 135 sites, lmax 3, N=2160, 31-point contour; one solve per step",
-                   "solver": "reference calculateTauMatrix build 0x2000 + zblocklu_cpp 0x2005"},
-        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "reference",
-                         "sample": f"{args.steps} solves at N=2160 (energies cycled)"},
+        "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": DATA,
+        "config": dict(CONFIG, solver="reference calculateTauMatrix build 0x2000 + zblocklu_cpp 0x2005",
+                       solves_per_step=per_step),
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
 
 
 def cpu_baseline(prob, seconds_budget=20.0):
+    """The reference's calculateTauMatrix on the host cores over the contour (within the budget);
+    returns the baseline entry and the reference's tau00_l of the energies it solved."""
     from oracle import reflib
     if not reflib.available():
-        return None
+        return None, []
     cores = os.cpu_count() or 1
     reflib.set_num_threads(cores)
     reflib.calculate_tau(prob, 0, 0, reflib.ZBLOCKLU_CPP)  # warm-up
+    outs = []
     n, t0 = 0, time.perf_counter()
     while n < 3 or (time.perf_counter() - t0 < seconds_budget and n < N_ENERGIES):
-        reflib.calculate_tau(prob, n % N_ENERGIES, 0, reflib.ZBLOCKLU_CPP)
+        outs.append(reflib.calculate_tau(prob, n % N_ENERGIES, 0, reflib.ZBLOCKLU_CPP))
         n += 1
         if time.perf_counter() - t0 > seconds_budget:
             break
     dt = time.perf_counter() - t0
-    return {"value": n / dt, "unit": "solves/s", "cores": cores, "kind": "reference",
-            "sample": f"{n} of the 31 contour solves at N=2160, one after another, OpenBLAS on {cores} threads"}
+    return ({"value": n / dt, "unit": "solves/s", "cores": cores, "kind": "reference",
+             "sample": f"{n} of the 31 contour solves at N=2160, one after another, OpenBLAS on {cores} threads"},
+            outs)
+
+
+def cusolver_comparator(s, prob, ne, local, steps=3):
+    """The reference GPU path's library solve (cuSOLVER zgetrf + zgetrs, as the reference's solver
+    0x13 calls it, linearSolvers_CUDA.cu:316-322) on the same KKR matrices, via torch.linalg.solve:
+    factor + solve of the ne built matrices with kkrsz_ns right-hand sides (no build, no tau00
+    post-processing), device time per step of ne solves."""
+    import torch
+    N, b = prob.nrmat_ns, prob.kkrsz_ns
+    dev = f"cuda:{local}"
+    ms = torch.empty(ne, N, N, dtype=torch.complex128, device=dev)
+    rhs = torch.zeros(ne, N, b, dtype=torch.complex128, device=dev)
+    for i in range(ne):
+        ms[i] = torch.from_numpy(s.build_kkr(0, i, 0, prob.energies[i], N))
+        rhs[i, :b] = torch.from_numpy(prob.t_block(int(prob.liz_store_idx[0]), i))
+    torch.linalg.solve(ms, rhs)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        x = torch.linalg.solve(ms, rhs)
+    e1.record()
+    e1.synchronize()
+    t = e0.elapsed_time(e1) / steps
+    del ms, rhs, x
+    torch.cuda.empty_cache()
+    return {"value": ne / (t * 1e-3), "unit": "solves/s", "ms_per_step": t,
+            "note": "cuSOLVER batched LU + solve (torch.linalg.solve) of the same 31 KKR matrices, "
+                    "16 right-hand sides, factor and solve only"}
 
 
 WORKLOADS = {
@@ -248,11 +298,15 @@ def run_comparators(args, local):
 def run_workload(args, world, rank, local):
     """The other configurations of the benchmark's table, one JSON line each (not the headline):
     one step = every job of the configuration in one batched call."""
+    line = workload_line(args.workload, args.steps, args.warmup, world, rank, local)
+    print(json.dumps(line))
+
+
+def workload_line(kind, steps, warmup, world, rank, local):
     import torch
     from lsms_b200 import tau as T
     from lsms_b200 import workloads as W
     torch.cuda.set_device(local)
-    kind = args.workload
     wl = {"batched": W.config_batched, "noncollinear": W.config_noncollinear_batch,
           "adjoint": W.config_adjoint_batch}[kind](seed=3 + rank)
     b = wl.kkrsz_ns
@@ -267,7 +321,7 @@ def run_workload(args, world, rank, local):
     nj = len(specs)
     flops = sum(algorithmic_flops(wl.nrmat_ns(a), b, wl.atoms[a].num_liz) for a, _, _, _ in specs)
     stream = torch.cuda.ExternalStream(s.stream, device=f"cuda:{local}")
-    steps, warmup = max(1, args.steps), max(1, min(args.warmup, 1))
+    steps, warmup = max(1, steps), max(1, min(warmup, 1))
 
     def timed(fn):
         for _ in range(warmup):
@@ -302,9 +356,8 @@ def run_workload(args, world, rank, local):
                      "ms_per_step": ms, "dtype": "c128",
                      "tau00_vs_forward_fp64": float(np.abs(tau - fwd).max() / np.abs(fwd).max()),
                      "note": "host buffers in and out (taubar, tau00, L gradient blocks per job)"})
-        print(json.dumps(line))
         s.close()
-        return
+        return line
     out = torch.empty(nj * b * b * 2, dtype=torch.float64, device=f"cuda:{local}")
     res = {}
     fallbacks = 0
@@ -335,8 +388,8 @@ def run_workload(args, world, rank, local):
                  "mixed_jobs_resolved_in_fp64": fallbacks,
                  "phase_ms_per_step": phases,
                  "algorithmic_flops_per_step": flops})
-    print(json.dumps(line))
     s.close()
+    return line
 
 
 def main():
@@ -346,6 +399,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the cuSOLVER comparator and the batched / non-collinear keys of the line")
     ap.add_argument("--workload", default="contour2160", choices=["contour2160", *WORKLOADS],
                     help="contour2160 = the headline line; the others print their own line")
     ap.add_argument("--energies", type=int, default=N_ENERGIES,
@@ -471,9 +526,39 @@ def main():
         e2e_times.append(time.perf_counter() - t0)
     e2e_s = max_over_ranks(statistics.median(e2e_times))
 
-    cpu = None
+    # --- config 2 as the reference runs it: FP64, one energy per call -------------------------
+    one = [T.make_jobs([(0, i, 0, prob.energies[i])]) for i in range(ne)]
+    for i in range(ne):
+        s.solve_jobs_device(one[i], out.data_ptr(), T.PREC_FP64)
+    s.sync()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(ne):
+        s.solve_jobs_device(one[i], out.data_ptr() + 16 * b * b * i, T.PREC_FP64)
+    e1.record(stream)
+    s.sync()
+    one_ms = max_over_ranks(e0.elapsed_time(e1) / ne)
+
+    cpu, ref_outs = None, []
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(prob)
+        cpu, ref_outs = cpu_baseline(prob)
+    err_ref = None
+    if ref_outs:  # the GPU outputs against the reference's own tau00_l, on tau00 (+ t0)
+        def rel(x, want):
+            return float(np.abs(x - want).max() / np.abs(want).max())
+        errs_m = [rel(a[i] + t0l[i], ref_outs[i] + t0l[i]) for i in range(len(ref_outs))]
+        errs_f = [rel(f[i] + t0l[i], ref_outs[i] + t0l[i]) for i in range(len(ref_outs))]
+        err_ref = {"mixed": max(errs_m), "fp64": max(errs_f), "energies": len(ref_outs),
+                   "tolerance": {"mixed": 1e-10, "fp64": 1e-12},
+                   "metric": "max |tau00 - tau00_ref| / max |tau00_ref| per energy, max over energies"}
+
+    extras = {}
+    if rank == 0 and world == 1 and not args.no_extras:
+        extras["cusolver_zgesv"] = cusolver_comparator(s, prob, ne, local)
+        for kind in ("batched", "noncollinear"):
+            wlne = workload_line(kind, 1, 1, world, rank, local)
+            extras[kind] = {k: wlne[k] for k in ("config", "value", "fp64", "mixed", "err_mixed_vs_fp64_on_tau00_l",
+                                                 "mixed_jobs_resolved_in_fp64", "phase_ms_per_step")}
 
     value = world * ne / (ms_mixed * 1e-3)
     fp64_value = world * ne / (ms_fp64 * 1e-3)
@@ -482,16 +567,20 @@ def main():
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_mixed, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "c64 trailing updates + c128 refinement",
-            "data": "synthetic (seeded phase-shift t-matrices, fcc LIZ)",
-            "config": {"workload": "fcc LIZ 135 sites a=6.82, lmax 3, N=2160, kkrsz_ns 16, "
-                                   "31-point semicircle contour -0.3..0.7 Ry, one atom per GPU",
+            "data": DATA,
+            "config": {**CONFIG,
                        "solves_per_step": ne, "l2": "inputs larger than L2 "
                        f"({ne} x {N * N * 16 / 1e6:.0f} MB KKR matrices per step)",
-                       "refinement_steps_mixed": "up to 6, per job until the correction estimate < 1e-12",
+                       "refinement_steps_mixed": "up to 10, per job until the correction estimate < 1e-12",
                        "refinement_steps_fp64": 1},
             "fp64": {"value": fp64_value, "unit": "solves/s", "ms_per_step": ms_fp64,
                      "mixed_over_fp64": value / fp64_value},
+            "fp64_one_energy_per_call": {"value": world / (one_ms * 1e-3), "unit": "solves/s",
+                                         "ms_per_solve": one_ms,
+                                         "note": "the reference's calling pattern: one b200tau call per "
+                                                 "(atom, energy), FP64, inputs resident"},
             "err_mixed_vs_fp64": err,
+            "err_vs_reference": err_ref,
             "phase_ms_per_step_mixed": phases,
             "flops_per_solve": flops_per_solve,
             "effective_tflops_mixed": value * flops_per_solve / 1e12,
@@ -500,7 +589,11 @@ def main():
                          "bound": "tensor",
                          "achieved": achieved, "unit": "TFLOP/s",
                          "peak": tf32_peak, "frac": (achieved / tf32_peak) if achieved else None,
+                         "executed_frac": (3.0 * achieved / tf32_peak) if achieved else None,
                          "traffic": TRAFFIC_PER_LAUNCH, "traffic_unit": "bytes per elimination step",
+                         "traffic_source": "ncu capture of the trailing-update kernel (dram__bytes_read.sum + "
+                                           "dram__bytes_write.sum), scaled to this workload; not measured in "
+                                           "this run",
                          "launches_timed": k_launches, "device_ms": k_ms, "algorithmic_flops": k_flops,
                          "flops_note": "algorithmic complex FLOPs 8 m n kb; the tensor pipe executes 3x "
                                        "that (hi*hi + hi*lo + lo*hi)",
@@ -516,6 +609,7 @@ def main():
             "gpu_launches": int(launches),
             "clocks": sampler.summary(),
             "cpu_baseline": cpu,
+            "configs": extras or None,
         }
         print(json.dumps(line))
     s.close()

@@ -103,7 +103,7 @@ int b200tau_set_atom(b200tau_ctx *ctx, int atom, int num_liz,
  * R = [0; t0] - M X against the unmodified KKR matrix and applies the correction from the
  * stored block factors (the refinement of the reference's zcgesv / cusolverDnIRSXgesv
  * solvers, linearSolvers_CPU.cpp:148-174, linearSolvers_CUDA.cu:424-469, on the N x b
- * system).  Defaults: FP64 1 step, MIXED 6 steps, of which each job runs only as many as it
+ * system).  Defaults: FP64 1 step, MIXED 10 steps, of which each job runs only as many as it
  * needs: after every step, a job whose estimated remaining error (the relative size c of the
  * correction just applied times its contraction c / c_previous) is below 1e-12 of tau00 stops.
  * A MIXED job whose corrections stop shrinking, or that has not converged after the last step,
@@ -251,12 +251,13 @@ int b200tau_set_graphs(b200tau_ctx *ctx, int enable);
 
 /* Row pivoting of the block elimination (B200TAU_PIVOT_*), both precisions.  BLOCK pivots inside
  * each 64 x 64 diagonal block, as the reference's GPU solver inverts its diagonal blocks
- * (zblock_lu_cuda_c.cu:218-259).  PANEL picks each 64-column step's rows from every remaining
- * row of the panel by a tournament of partial-pivoting eliminations, then moves them into place
- * in every column: the quality of LAPACK's zgetrf over the column (the reference's CPU path pivots
- * with zgetrf inside blocks of ~N/3 rows, zblock_lu_cpp.cpp:58, linearSolvers_CPU.cpp:270), at
- * the cost of the tournament and the row moves; ill-conditioned matrices need it for the MIXED
- * refinement to converge.  Pivots never come from the central site's rows, so FP64 with 0
+ * (zblock_lu_cuda_c.cu:218-259).  PANEL picks each 64-column step's rows from the whole
+ * remaining column: the diagonal block's own rows and the rows of largest magnitude in the panel
+ * (256 candidates) go through a partial-pivoting elimination, whose pivot rows then move into
+ * place in every column.  That approaches LAPACK's zgetrf over the column (the reference's CPU
+ * path pivots with zgetrf inside blocks of ~N/3 rows, zblock_lu_cpp.cpp:58,
+ * linearSolvers_CPU.cpp:270), at the cost of the selection and the row moves; ill-conditioned
+ * matrices need it for the MIXED refinement to converge.  Pivots never come from the central site's rows, so FP64 with 0
  * refinement steps still reads tau00 from the Schur complement.  b200tau_solve_vjp always
  * uses BLOCK. */
 int b200tau_set_pivoting(b200tau_ctx *ctx, int mode);

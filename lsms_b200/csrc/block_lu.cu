@@ -608,7 +608,7 @@ constexpr int kSparseGrid = 2 * 148;
 // s waits for the inverse before step k + 1.  Only the diagonal inverse moves off s, so the packs of step k + 1 are
 // written after every tile of step k has read those of step k.
 // With panel pivoting the first update covers the whole first tile column (the next step's panel,
-// every row), the second stream also runs the next step's tournament and applies its row moves to
+// every row), the second stream also runs the next step's row selection and applies its row moves to
 // the columns left of the other tiles, and the main stream applies them to the other columns once
 // their update is done.
 template <typename T, typename S>

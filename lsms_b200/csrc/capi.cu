@@ -128,7 +128,7 @@ struct b200tau_ctx {
   int max_slots = 64;
   // refinement rounds, FP64 and MIXED; MIXED stops early per job once the correction estimate
   // is below kRefineTol of tau00 (block_lu.cu, converge_check_kernel)
-  int refine_steps[2] = {1, 6};
+  int refine_steps[2] = {1, 10};
   // profiling of the trailing-update launches (b200tau_set_profiling)
   bool profiling = false;
   std::vector<cudaEvent_t> events;
@@ -195,7 +195,7 @@ void free_atom(AtomDev &a) {
 
 inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
 
-// B200TAU_PIVOT_AUTO takes panel pivoting from this N up: the tournament's latency per step is then
+// B200TAU_PIVOT_AUTO takes panel pivoting from this N up: the row selection's latency per step is then
 // small beside the trailing update, and these (non-collinear, N = 4320) matrices need it.
 constexpr int kPanelAutoN = 3000;
 

@@ -17,20 +17,16 @@ constexpr int kNdlm = (kMaxLend + 1) * (kMaxLend + 2) / 2;       // 28 P_lm valu
 constexpr int kNdlj = (kMaxLend + 1) * (kMaxLend + 1);           // 49 D_lm values
 constexpr int kMaxTerms = kMaxLmax + 1;                          // Gaunt terms per G element
 constexpr int kNb = 64;                                         // elimination block width
-// Panel pivoting (pivot.cu): candidate rows per tournament leaf, and nodes merged per level.
-constexpr int kPivLeafRows = 256;
-constexpr int kPivFanIn = 4;
+// Panel pivoting (pivot.cu): candidate rows of a step's partial-pivoting elimination.
+constexpr int kPivCands = 256;
 // Per-job pivot buffer of panel pivoting (ints), for leading dimension ld:
 //   [0, ld)                  perm: the original row at each physical row position
 //   [ld, 2 ld)               rowpos: the physical position of each original row (after elimination)
 //   [2 ld, 2 ld + 1 + 4 kNb) the step's row moves: count, kNb*2 destinations, kNb*2 sources
-//   then two areas of pivot_sets(ld) x kNb candidate rows (tournament levels, alternating)
-__host__ __device__ constexpr int pivot_sets(int ld) { return (ld + kPivLeafRows - 1) / kPivLeafRows; }
+//   [.., + ld)               the step's row magnitudes over the panel columns (float bits)
 __host__ __device__ constexpr int pivot_moves_offset(int ld) { return 2 * ld; }
-__host__ __device__ constexpr int pivot_sets_offset(int ld, int which) {
-  return 2 * ld + 1 + 4 * kNb + which * pivot_sets(ld) * kNb;
-}
-__host__ __device__ constexpr int pivot_ints(int ld) { return pivot_sets_offset(ld, 2); }
+__host__ __device__ constexpr int pivot_mags_offset(int ld) { return 2 * ld + 1 + 4 * kNb; }
+__host__ __device__ constexpr int pivot_ints(int ld) { return pivot_mags_offset(ld) + ld; }
 // Columns of one tile of the tensor-core trailing update (tc_update.cu).
 constexpr int kTcTileCols = 256;
 // A refining job stops once its estimated remaining error on tau00 is below this fraction of
@@ -208,7 +204,7 @@ cudaError_t launch_eliminate(FactorKind fk, const JobDev *jobs, int njobs, int m
                              const TcMaps *tc, int *err, bool sparse_jobs = false,
                              const Lookahead *la = nullptr, bool panel = false);
 // Panel pivoting (pivot.cu), for the records with a pivot buffer: the identity permutation; the
-// tournament that picks step k's kb rows from [k, n) and writes the step's row moves; those moves
+// selection that picks step k's kb rows from [k, n) and writes the step's row moves; those moves
 // applied to columns [c0, c1) of F; and the final row positions for the residual.
 cudaError_t launch_pivot_init(const JobDev *jobs, int njobs, cudaStream_t s, long *launches);
 cudaError_t launch_panel_select(FactorKind fk, const JobDev *jobs, int njobs, int k, int max_n, cudaStream_t s,

@@ -6,129 +6,213 @@
 // (linearSolvers_CPU.cpp:76-96) pivots over the whole column.  Restricting the pivots of a 64-column
 // step to its own diagonal block is enough for the collinear contour matrices, but the
 // non-collinear N = 4320 matrices (condition numbers up to ~1e7) then lose most of the FP32
-// factorisation's accuracy and the mixed refinement stalls.  Here the rows of step k come from a
-// tournament over every candidate row [k, n) (communication-avoiding "tournament pivoting"):
-//   leaves    every 256 candidate rows of the panel columns k..k+kb-1 run Gaussian elimination
-//             with partial pivoting (GEPP) and nominate the kb rows it pivots on;
-//   merges    the nominees of 4 nodes run GEPP again on their panel rows (re-read from F) and
-//             nominate kb of them; repeated until one node is left.
-// The root's kb rows then move to positions k..k+kb-1 (the rows displaced from there take the
-// vacated positions): a permutation of at most 2 kb rows, applied to every column of F, so the
-// factor storage is that of LAPACK's P M = L U and the kernels of the elimination and of the
-// sweeps run unchanged.  The permutation of the whole elimination is tracked per job (perm), and
-// its inverse (rowpos) makes the refinement's residual land in the permuted row order.  Pivots
-// come only from rows [k, n), never from the central site's rows, so the trailing b x b block
-// still holds the Schur complement 1 - Delta.
+// factorisation's accuracy and the mixed refinement stalls.  Here step k's rows come from every
+// candidate row [k, n), in two launches:
+//   magnitudes  every row below the diagonal block gets max_j |re| + |im| over the panel columns
+//               k..k+kb-1 (one thread per row, coalesced over the column-major panel);
+//   selection   one CTA per job: the kPivCands - kb rows of largest magnitude (a radix select on
+//               the float bits, compacted in row order, so the choice is deterministic) join the
+//               kb rows of the diagonal block, and Gaussian elimination with partial pivoting
+//               (GEPP) on these candidates' panel rows picks the kb pivot rows in pivot order.
+// That is the node of communication-avoiding "tournament pivoting" with a magnitude filter in
+// front: a row that is small in every panel column is not a candidate.  On the non-collinear
+// N = 4320 matrices a numpy emulation of the whole mixed solve gives the first refinement round an
+// error of 1.6e-3 .. 1e-2 with it, 1.6e-3 .. 5e-3 with a full tournament over all rows and
+// 5e-3 .. 9e-2 with the pivots restricted to the diagonal block.
+// The kb rows then move to positions k..k+kb-1 (the rows displaced from there take the vacated
+// positions): a permutation of at most 2 kb rows, applied to every column of F, so the factor
+// storage is that of LAPACK's P M = L U and the kernels of the elimination and of the sweeps run
+// unchanged.  The permutation of the whole elimination is tracked per job (perm), and its inverse
+// (rowpos) makes the refinement's residual land in the permuted row order.  Pivots come only from
+// rows [k, n), never from the central site's rows, so the trailing b x b block still holds the
+// Schur complement 1 - Delta.
 //
 // Selection arithmetic is FP32 on either factor type (it only ranks pivot magnitudes, |re| + |im|
-// as izamax, ties to the lower candidate); the factorisation itself is unchanged.
+// as izamax, ties to the earlier candidate); the factorisation itself is unchanged.
 
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <climits>
 
 #include "common.cuh"
 
 namespace b200 {
 namespace {
 
-constexpr int kSelThreads = kPivLeafRows;  // one candidate row per thread
-static_assert(kSelThreads == 256, "selection thread layout");
+constexpr int kSelThreads = 1024;                  // (candidate, 16-column group) per thread
+constexpr int kGroups = kSelThreads / kPivCands;   // column groups of the panel
+constexpr int kGroupCols = kNb / kGroups;          // 16
+static_assert(kGroups * kGroupCols == kNb, "selection thread layout");
 
 __device__ __forceinline__ float2 to_f2(double2 a) { return make_float2((float)a.x, (float)a.y); }
 __device__ __forceinline__ float2 to_f2(float2 a) { return a; }
+__device__ __forceinline__ float cabs1f(float2 a) { return fabsf(a.x) + fabsf(a.y); }
 
-// Node counts of a job's tournament: level 0 has ceil(m / leaf) nodes, each level above merges
-// kPivFanIn of them.
-__device__ __forceinline__ int nodes_at(int m, int level) {
-  int nodes = (m + kPivLeafRows - 1) / kPivLeafRows;
-  for (int l = 0; l < level; ++l) nodes = (nodes + kPivFanIn - 1) / kPivFanIn;
-  return nodes;
-}
-
-// One tournament node: candidates (one per thread), GEPP on their panel rows in shared memory,
-// the kb nominees in pivot order.  The root also writes the step's row moves and applies them to
-// the job's permutation.
+// Row magnitudes below the diagonal block of step k: mags[row] = max_j |F[row, k + j]|_1 over the
+// kb panel columns, as float bits (a NaN ranks as zero).
 template <typename T>
-__global__ void __launch_bounds__(kSelThreads) panel_select_kernel(const JobDev *__restrict__ jobs, int k,
-                                                                   int level) {
+__global__ void __launch_bounds__(256) panel_mags_kernel(const JobDev *__restrict__ jobs, int k) {
   const JobDev &J = jobs[blockIdx.y];
   if (J.inactive || J.piv == nullptr || k >= J.n) return;
   const int kb = min(kNb, J.n - k);
-  const int m = J.n - k;  // candidate rows [k, n)
-  const int nodes = nodes_at(m, level);
-  if (level > 0 && nodes_at(m, level - 1) <= 1) return;  // this job's root was at a lower level
-  const int node = blockIdx.x;
-  if (node >= nodes) return;
-  const bool root = nodes == 1;
-  const int ld = J.ld;
-  int *__restrict__ piv = J.piv;
-  const int *__restrict__ sets_in = piv + pivot_sets_offset(ld, (level + 1) & 1);
-  int *__restrict__ sets_out = piv + pivot_sets_offset(ld, level & 1);
-
-  extern __shared__ __align__(16) unsigned char sel_smem[];
-  float2(*A)[kPivLeafRows] = reinterpret_cast<float2(*)[kPivLeafRows]>(sel_smem);  // A[col][cand]
-  __shared__ int s_cand[kPivLeafRows];
-  __shared__ int s_out[kNb];
-  __shared__ float s_wv[2][kSelThreads / 32];
-  __shared__ int s_wi[2][kSelThreads / 32];
-
-  const int r = threadIdx.x, lane = r & 31, warp = r >> 5;
-  int cand = -1;
-  if (level == 0) {
-    const int row = k + node * kPivLeafRows + r;
-    if (row < J.n) cand = row;
-  } else {
-    const int prev = nodes_at(m, level - 1);
-    const int set = node * kPivFanIn + r / kNb;
-    if (set < prev) cand = sets_in[set * kNb + r % kNb];
+  const int row = k + kb + blockIdx.x * 256 + threadIdx.x;
+  if (row >= J.n) return;
+  const T *__restrict__ F = static_cast<const T *>(J.F);
+  float m = 0.f;
+  for (int j = 0; j < kb; ++j) {
+    const float v = cabs1f(to_f2(F[(size_t)row + (size_t)(k + j) * J.ld]));
+    m = v > m ? v : m;  // (a NaN compares false)
   }
-  s_cand[r] = cand;
-  const int R = __syncthreads_count(cand >= 0);
+  J.piv[pivot_mags_offset(J.ld) + row] = __float_as_int(m);
+}
 
-  if (R <= kb) {  // every candidate is a nominee (the last steps, or sparse merges)
-    if (r == 0) {
-      int c = 0;
-      for (int i = 0; i < kPivLeafRows; ++i)
-        if (s_cand[i] >= 0) s_out[c++] = s_cand[i];
-      for (; c < kNb; ++c) s_out[c] = -1;
+// Block-wide exclusive prefix sum of one int per thread (kSelThreads threads); returns the total.
+__device__ __forceinline__ int block_scan(int v, int *s_warp, int &excl) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
+  }
+  if (lane == 31) s_warp[warp] = x;
+  __syncthreads();
+  if (warp == 0) {
+    int w = s_warp[lane];
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, w, o);
+      if (lane >= o) w += y;
     }
+    s_warp[lane] = w;  // inclusive over warps
+  }
+  __syncthreads();
+  const int total = s_warp[31];
+  excl = (warp > 0 ? s_warp[warp - 1] : 0) + x - v;
+  __syncthreads();  // s_warp is reused by the next scan
+  return total;
+}
+
+// Step k's selection, one CTA per job (see the file comment); the kb pivot rows in pivot order
+// become the step's row moves, also applied to the job's permutation.
+template <typename T>
+__global__ void __launch_bounds__(kSelThreads) panel_select_kernel(const JobDev *__restrict__ jobs, int k) {
+  const JobDev &J = jobs[blockIdx.x];
+  if (J.inactive || J.piv == nullptr || k >= J.n) return;
+  const int kb = min(kNb, J.n - k);
+  const int n = J.n, ld = J.ld;
+  int *__restrict__ piv = J.piv;
+  const unsigned *__restrict__ mags = reinterpret_cast<const unsigned *>(piv + pivot_mags_offset(ld));
+  extern __shared__ __align__(16) unsigned char sel_smem[];
+  float2(*A)[kPivCands] = reinterpret_cast<float2(*)[kPivCands]>(sel_smem);  // A[col][cand]
+  __shared__ int s_cand[kPivCands];
+  __shared__ int s_out[kNb];
+  __shared__ int s_hist[256];
+  __shared__ int s_warp[32];
+  __shared__ unsigned s_prefix;
+  __shared__ int s_remain;
+  __shared__ float s_wv[2][kPivCands / 32];
+  __shared__ int s_wi[2][kPivCands / 32];
+  const int tid = threadIdx.x;
+
+  // --- candidates: the diagonal block's rows, then the largest rows below it ---
+  const int lo = k + kb, m2 = n - lo;  // rows below the diagonal block
+  const int K2 = min(m2, kPivCands - kb);
+  if (tid < kb) s_cand[tid] = k + tid;
+  if (K2 == m2) {
+    for (int i = tid; i < m2; i += kSelThreads) s_cand[kb + i] = lo + i;
+  } else {
+    // radix select (8 bits at a time, most significant first) of the K2-th largest key
+    unsigned prefix = 0u, mask = 0u;
+    int remain = K2;
+    for (int shift = 24; shift >= 0; shift -= 8) {
+      if (tid < 256) s_hist[tid] = 0;
+      __syncthreads();
+      for (int i = tid; i < m2; i += kSelThreads) {
+        const unsigned key = mags[lo + i];
+        if ((key & mask) == prefix) atomicAdd(&s_hist[(key >> shift) & 255u], 1);
+      }
+      __syncthreads();
+      if (tid == 0) {
+        int cum = 0, d = 0;
+        for (d = 255; d > 0; --d) {
+          if (cum + s_hist[d] >= remain) break;
+          cum += s_hist[d];
+        }
+        s_prefix = prefix | ((unsigned)d << shift);
+        s_remain = remain - cum;
+      }
+      __syncthreads();
+      prefix = s_prefix;
+      remain = s_remain;
+      mask |= 255u << shift;
+      __syncthreads();
+    }
+    // keys above the threshold, then `remain` of the keys equal to it, each in row order
+    const int chunk = (m2 + kSelThreads - 1) / kSelThreads;
+    const int r0 = min(m2, tid * chunk), r1 = min(m2, r0 + chunk);
+    int ngt = 0, neq = 0;
+    for (int i = r0; i < r1; ++i) {
+      const unsigned key = mags[lo + i];
+      ngt += key > prefix;
+      neq += key == prefix;
+    }
+    int bgt = 0, beq = 0;
+    const int tgt = block_scan(ngt, s_warp, bgt);
+    block_scan(neq, s_warp, beq);
+    for (int i = r0; i < r1; ++i) {
+      const unsigned key = mags[lo + i];
+      if (key > prefix) {
+        s_cand[kb + bgt++] = lo + i;
+      } else if (key == prefix) {
+        if (beq < remain) s_cand[kb + tgt + beq] = lo + i;
+        ++beq;
+      }
+    }
+  }
+  __syncthreads();
+  const int R = kb + K2;  // candidates
+
+  // --- GEPP on the candidates' panel rows ---
+  if (R <= kb) {  // the last step: the block's own rows, in place
+    if (tid < kb) s_out[tid] = k + tid;
     __syncthreads();
   } else {
     const T *__restrict__ F = static_cast<const T *>(J.F);
-    // panel rows into shared memory; at the leaves consecutive threads read consecutive rows
-    for (int j = 0; j < kb; ++j)
-      A[j][r] = cand >= 0 ? to_f2(F[(size_t)cand + (size_t)(k + j) * ld]) : make_float2(0.f, 0.f);
+    const int r = tid & (kPivCands - 1), g = tid / kPivCands, c0 = g * kGroupCols;
+    const int cand = r < R ? s_cand[r] : -1;
+    for (int j = c0; j < c0 + kGroupCols; ++j)
+      A[j][r] = (cand >= 0 && j < kb) ? to_f2(F[(size_t)cand + (size_t)(k + j) * ld]) : make_float2(0.f, 0.f);
     __syncthreads();
     bool taken = false;
     for (int p = 0; p < kb; ++p) {
-      const int par = p & 1;
-      float v = -1.f;
-      if (cand >= 0 && !taken) {
-        const float2 a = A[p][r];
-        v = fabsf(a.x) + fabsf(a.y);
-        if (!(v == v)) v = 0.f;  // a NaN ranks as zero, so a row in range is still chosen
-      }
-      int idx = r;
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {  // warp arg-max, ties to the lower candidate
-        const float ov = __shfl_xor_sync(0xffffffffu, v, o);
-        const int oi = __shfl_xor_sync(0xffffffffu, idx, o);
-        if (ov > v || (ov == v && oi < idx)) {
-          v = ov;
-          idx = oi;
+      const int par = p & 1, gp = p / kGroupCols;
+      if (g == gp) {  // the threads holding column p rank their rows: warp arg-max, ties low
+        float v = -1.f;
+        if (cand >= 0 && !taken) {
+          v = cabs1f(A[p][r]);
+          if (!(v == v)) v = 0.f;  // a NaN ranks as zero, so a row in range is still chosen
         }
-      }
-      if (lane == 0) {
-        s_wv[par][warp] = v;
-        s_wi[par][warp] = idx;
+        int idx = r;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          const float ov = __shfl_xor_sync(0xffffffffu, v, o);
+          const int oi = __shfl_xor_sync(0xffffffffu, idx, o);
+          if (ov > v || (ov == v && oi < idx)) {
+            v = ov;
+            idx = oi;
+          }
+        }
+        if ((tid & 31) == 0) {
+          s_wv[par][r >> 5] = v;
+          s_wi[par][r >> 5] = idx;
+        }
       }
       __syncthreads();
       float bv = s_wv[par][0];
       int bi = s_wi[par][0];
 #pragma unroll
-      for (int w = 1; w < kSelThreads / 32; ++w) {
+      for (int w = 1; w < kPivCands / 32; ++w) {
         const float ov = s_wv[par][w];
         const int oi = s_wi[par][w];
         if (ov > bv || (ov == bv && oi < bi)) {
@@ -138,8 +222,9 @@ __global__ void __launch_bounds__(kSelThreads) panel_select_kernel(const JobDev 
       }
       // R > kb > p candidates remain untaken, each ranked >= 0: bi is one of them
       if (r == bi) taken = true;
-      if (r == 0) s_out[p] = s_cand[bi];
-      if (cand >= 0 && !taken && p + 1 < kb) {
+      if (tid == 0) s_out[p] = s_cand[bi];
+      const int jlo = max(p + 1, c0), jhi = min(kb, c0 + kGroupCols);
+      if (cand >= 0 && !taken && jlo < jhi) {
         const float2 d = A[p][bi];
         const float dd = d.x * d.x + d.y * d.y;
         float2 f = make_float2(0.f, 0.f);
@@ -147,7 +232,7 @@ __global__ void __launch_bounds__(kSelThreads) panel_select_kernel(const JobDev 
           const float2 a = A[p][r];
           f = make_float2((a.x * d.x + a.y * d.y) / dd, (a.y * d.x - a.x * d.y) / dd);
         }
-        for (int j = p + 1; j < kb; ++j) {
+        for (int j = jlo; j < jhi; ++j) {
           const float2 pj = A[j][bi];
           float2 x = A[j][r];
           x.x -= f.x * pj.x - f.y * pj.y;
@@ -158,18 +243,14 @@ __global__ void __launch_bounds__(kSelThreads) panel_select_kernel(const JobDev 
       __syncthreads();
     }
   }
-  if (!root) {
-    if (r < kNb) sets_out[node * kNb + r] = s_out[r];
-    return;
-  }
-  if (r != 0) return;
-  // the root: moves that bring the nominees to k..k+kb-1 (pivot order) and the displaced rows to
-  // the vacated positions; a permutation of at most 2 kb positions, also applied to perm
+  if (tid != 0) return;
+  // the moves that bring the pivot rows to k..k+kb-1 (pivot order) and the displaced rows to the
+  // vacated positions; a permutation of at most 2 kb positions, also applied to perm
   int *mv = piv + pivot_moves_offset(ld);
   int *dst = mv + 1, *src = mv + 1 + 2 * kNb;
-  // kb distinct nominees in [k, n) by construction; anything else leaves the rows in place
+  // kb distinct rows in [k, n) by construction; anything else leaves the rows in place
   for (int p = 0; p < kb; ++p)
-    if (s_out[p] < k || s_out[p] >= J.n) {
+    if (s_out[p] < k || s_out[p] >= n) {
       mv[0] = 0;
       return;
     }
@@ -249,18 +330,17 @@ __global__ void pivot_finish_kernel(const JobDev *__restrict__ jobs) {
 
 template <typename T>
 cudaError_t select_impl(const JobDev *jobs, int njobs, int k, int max_n, cudaStream_t s, long *launches) {
-  const int m = max_n - k;
-  if (m <= 0) return cudaSuccess;
-  const int smem = kNb * kPivLeafRows * (int)sizeof(float2);
+  if (max_n - k <= 0) return cudaSuccess;
+  const int m = max_n - k - kNb;  // rows below the diagonal block, at most
+  const int smem = kNb * kPivCands * (int)sizeof(float2);
   cudaError_t e = ensure_smem(panel_select_kernel<T>, smem);
   if (e != cudaSuccess) return e;
-  int nodes = (m + kPivLeafRows - 1) / kPivLeafRows;
-  for (int level = 0;; ++level) {
-    panel_select_kernel<T><<<dim3(nodes, njobs), kSelThreads, smem, s>>>(jobs, k, level);
+  if (m > kPivCands - kNb) {  // magnitudes are ranked only when the candidates must be filtered
+    panel_mags_kernel<T><<<dim3((m + 255) / 256, njobs), 256, 0, s>>>(jobs, k);
     if (launches) *launches += 1;
-    if (nodes == 1) break;
-    nodes = (nodes + kPivFanIn - 1) / kPivFanIn;
   }
+  panel_select_kernel<T><<<njobs, kSelThreads, smem, s>>>(jobs, k);
+  if (launches) *launches += 1;
   return cudaGetLastError();
 }
 

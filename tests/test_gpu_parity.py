@@ -147,7 +147,7 @@ def test_mixed_resolves_unconverged_jobs_in_fp64(solver_factory):
         forced = s.solve_jobs(jobs, T.PREC_MIXED)
         assert s.last_fallback_count == len(idx)
     finally:
-        s.set_refinement(T.PREC_MIXED, 6)
+        s.set_refinement(T.PREC_MIXED, 10)
     errs = [tau_err(prob, i, 0, forced[k], fp64[k]) for k, i in enumerate(idx)]
     assert max(errs) <= TOL_FP64, errs
     mixed = s.solve_jobs(jobs, T.PREC_MIXED)
@@ -257,7 +257,7 @@ def test_mixed_without_refinement_is_fp32_accurate(solver_factory, ref):
     try:
         out = s.calculate_tau_matrix(0, 0, prob.energies[0], 0, T.PREC_MIXED)
     finally:
-        s.set_refinement(T.PREC_MIXED, 6)
+        s.set_refinement(T.PREC_MIXED, 10)
     want = ref.calculate_tau(prob, 0, 0, ref.ZBLOCKLU_CPP)
     err = tau_err(prob, 0, 0, out, want)
     assert 1e-12 < err < 1e-3, err

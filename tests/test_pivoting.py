@@ -1,7 +1,8 @@
 """Panel pivoting (B200TAU_PIVOT_PANEL): every 64-column step picks its rows from the whole
-remaining column by a tournament of partial-pivoting eliminations, as LAPACK's zgetrf does over a
-column (the reference's CPU solver pivots with zgetrf inside ~N/3-row blocks,
-zblock_lu_cpp.cpp:58; its zgesv path, linearSolvers_CPU.cpp:76-96, over the whole column).
+remaining column (a partial-pivoting elimination on the diagonal block's rows and the panel's rows
+of largest magnitude), approaching LAPACK's zgetrf over a column (the reference's CPU solver
+pivots with zgetrf inside ~N/3-row blocks, zblock_lu_cpp.cpp:58; its zgesv path,
+linearSolvers_CPU.cpp:76-96, over the whole column).
 
 Parity: FP64 within 1e-12 of the reference's tau00 where the matrices allow it (N = 240, 2160);
 at N = 4320 (non-collinear, condition numbers 1e5..1e7) within the spread of the reference's own
