@@ -52,7 +52,7 @@ extern "C" {
 #define B200TAU_SWEEP_FP64 0 /* mixed path: correction solve in FP64 arithmetic on FP32 factors */
 #define B200TAU_SWEEP_FP32 1 /* mixed path: correction solve in FP32, as zcgesv (default) */
 
-#define B200TAU_PIVOT_AUTO 0  /* PANEL from N = 3000 up, else BLOCK (default) */
+#define B200TAU_PIVOT_AUTO 0  /* PANEL for MIXED factors from N = 3000 up, else BLOCK (default) */
 #define B200TAU_PIVOT_BLOCK 1 /* pivots inside each 64 x 64 diagonal block */
 #define B200TAU_PIVOT_PANEL 2 /* pivots from the whole remaining column of each 64-column panel */
 

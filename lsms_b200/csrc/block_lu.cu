@@ -797,7 +797,7 @@ __global__ void copy_to_factor_kernel(const double2 *__restrict__ M, T *__restri
 
 // The FP64 re-solve records of a mixed wave (launch_fallback_prepare).
 __global__ void fallback_prepare_kernel(const JobDev *__restrict__ jobs, JobDev *__restrict__ out, int njobs,
-                                        double2 *f64, size_t f64_stride, int *count) {
+                                        double2 *f64, size_t f64_stride, int *count, int panel) {
   const int w = blockIdx.x * blockDim.x + threadIdx.x;
   if (w >= njobs) return;
   JobDev J = jobs[w];
@@ -808,6 +808,7 @@ __global__ void fallback_prepare_kernel(const JobDev *__restrict__ jobs, JobDev 
     J.F = f64 + (size_t)w * f64_stride;
     J.conv = nullptr;  // the FP64 rounds run unconditionally
     J.cnorm = nullptr;
+    if (!panel) J.piv = nullptr;  // pivots inside the diagonal blocks: rows stay in place
     atomicAdd(count, 1);
   }
   out[w] = J;
@@ -838,9 +839,9 @@ __global__ void __launch_bounds__(256) copy_jobs_to_factor_kernel(const JobDev *
 }  // namespace
 
 cudaError_t launch_fallback_prepare(const JobDev *jobs, JobDev *out, int njobs, double2 *f64, size_t f64_stride,
-                                    int max_N, int *count, cudaStream_t s, long *launches) {
+                                    int max_N, int *count, bool panel, cudaStream_t s, long *launches) {
   if (njobs <= 0) return cudaSuccess;
-  fallback_prepare_kernel<<<(njobs + 63) / 64, 64, 0, s>>>(jobs, out, njobs, f64, f64_stride, count);
+  fallback_prepare_kernel<<<(njobs + 63) / 64, 64, 0, s>>>(jobs, out, njobs, f64, f64_stride, count, panel ? 1 : 0);
   copy_jobs_to_factor_kernel<<<dim3(std::min(max_N, 64), njobs), 256, 0, s>>>(out);
   if (launches) *launches += 2;
   return cudaGetLastError();

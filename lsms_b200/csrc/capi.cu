@@ -195,12 +195,16 @@ void free_atom(AtomDev &a) {
 
 inline int round_up(int x, int m) { return (x + m - 1) / m * m; }
 
-// B200TAU_PIVOT_AUTO takes panel pivoting from this N up: the row selection's latency per step is then
-// small beside the trailing update, and these (non-collinear, N = 4320) matrices need it.
+// B200TAU_PIVOT_AUTO takes panel pivoting for FP32 factors from this N up: the row selection's
+// latency per step is then small beside the trailing update, and the MIXED refinement of these
+// (non-collinear, N = 4320) matrices needs it.  FP64 factors keep the pivots inside the diagonal
+// blocks: as accurate on these matrices (within the reference's own zgesv / zblock_lu spread) and
+// faster.
 constexpr int kPanelAutoN = 3000;
 
-bool use_panel(const b200tau_ctx *ctx, int maxN) {
-  return ctx->pivoting == B200TAU_PIVOT_PANEL || (ctx->pivoting == B200TAU_PIVOT_AUTO && maxN >= kPanelAutoN);
+bool use_panel(const b200tau_ctx *ctx, int maxN, FactorKind fk) {
+  return ctx->pivoting == B200TAU_PIVOT_PANEL ||
+         (ctx->pivoting == B200TAU_PIVOT_AUTO && fk == kFactorFP32 && maxN >= kPanelAutoN);
 }
 
 int ensure_piv(b200tau_ctx *ctx, int ld, int slots) {
@@ -606,7 +610,7 @@ int fallback_graph(b200tau_ctx *ctx, int nw, int ld, int b, int ns, int kkrsz, b
     e = cudaStreamBeginCaptureToGraph(ctx->cap_stream, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
       e = launch_fallback_prepare(ctx->d_jobs, ctx->d_jobs3, nw, ctx->d_ffb, (size_t)ld * ld, maxN, ctx->d_fbcount,
-                                  ctx->cap_stream, nullptr);
+                                  panel, ctx->cap_stream, nullptr);
       if (e == cudaSuccess)
         e = launch_eliminate(kFactorFP64, ctx->d_jobs3, nw, maxn, maxN, finfo, ctx->cap_stream, nullptr, nullptr,
                              nullptr, ctx->d_err, true, nullptr, panel);
@@ -687,7 +691,7 @@ int run_refinement(b200tau_ctx *ctx, const std::vector<JobDev> &h, int nw, int m
   // the same kernels and arithmetic as a PREC_FP64 solve of the job.
   cudaGraphExec_t fb = nullptr;
   int rc = ensure_fallback(ctx, h[0].ld);
-  if (rc || (rc = fallback_graph(ctx, nw, h[0].ld, b, ns, kkrsz, panel, &fb))) return rc;
+  if (rc || (rc = fallback_graph(ctx, nw, h[0].ld, b, ns, kkrsz, use_panel(ctx, maxN, kFactorFP64), &fb))) return rc;
   CK(cudaGraphLaunch(fb, ctx->stream));
   ctx->launches += 1;
   return B200TAU_OK;
@@ -801,7 +805,7 @@ int run_wave(b200tau_ctx *ctx, const b200tau_job *jobs, const int *idx, int nw, 
   int maxL = 0, maxN = 0, maxn = 0;
   for (int w = 0; w < nw; ++w) maxN = std::max(maxN, ctx->atoms[jobs[idx[w]].atom].N);
   // the adjoint forms M^-1 from block factors without row moves
-  const bool panel = adj == nullptr && use_panel(ctx, maxN);
+  const bool panel = adj == nullptr && use_panel(ctx, maxN, p.fk);
   for (int w = 0; w < nw; ++w) {
     const b200tau_job &jb = jobs[idx[w]];
     const AtomDev &a = ctx->atoms[jb.atom];
@@ -871,7 +875,8 @@ int run_wave(b200tau_ctx *ctx, const b200tau_job *jobs, const int *idx, int nw, 
     ctx->launches += g->launches;
     if (p.fk != kFactorFP32 || !ctx->fallback_on || p.steps == 0) return B200TAU_OK;
     cudaGraphExec_t fb = nullptr;
-    if ((rc = ensure_fallback(ctx, ld)) || (rc = fallback_graph(ctx, nw, ld, ctx->b, ctx->ns, ctx->kkrsz, panel, &fb)))
+    if ((rc = ensure_fallback(ctx, ld)) ||
+        (rc = fallback_graph(ctx, nw, ld, ctx->b, ctx->ns, ctx->kkrsz, use_panel(ctx, maxN, kFactorFP64), &fb)))
       return rc;
     CK(cudaGraphLaunch(fb, ctx->stream));
     ctx->launches += 1;
@@ -967,7 +972,9 @@ int solve_impl(b200tau_ctx *ctx, const b200tau_job *jobs, int njobs, int prec, d
   if ((rc = ensure_workspace(ctx, ld, slots, p))) return rc;
   if ((rc = ensure_jobs(ctx, slots))) return rc;
   if ((rc = ensure_host_info(ctx, njobs))) return rc;
-  if (use_panel(ctx, maxN) && (rc = ensure_piv(ctx, ld, slots))) return rc;
+  // (the FP64 re-solve of unconverged MIXED jobs may pivot differently from the wave)
+  if ((use_panel(ctx, maxN, p.fk) || use_panel(ctx, maxN, kFactorFP64)) && (rc = ensure_piv(ctx, ld, slots)))
+    return rc;
   ctx->launches = 0;
   if (ctx->d_fbcount) CK(cudaMemsetAsync(ctx->d_fbcount, 0, sizeof(int), ctx->stream));
   ctx->kept_valid = false;
@@ -981,7 +988,7 @@ int solve_impl(b200tau_ctx *ctx, const b200tau_job *jobs, int njobs, int prec, d
   // one FP64 wave with M kept beside its block factors, X refined, pivots inside the diagonal blocks:
   // what b200tau_solve_vjp needs from a forward solve
   if (ctx->keep_factors && njobs <= slots && p.fk == kFactorFP64 && p.f_separate && p.steps > 0 &&
-      !use_panel(ctx, maxN)) {
+      !use_panel(ctx, maxN, p.fk)) {
     ctx->kept_jobs.assign(jobs, jobs + njobs);
     ctx->kept_order = order;
     ctx->kept_ld = ld;
@@ -1440,7 +1447,7 @@ int b200tau_solve_dense(b200tau_ctx *ctx, const double *m, int n, int ldm, const
   J.t0_ld = b;
   J.out = ctx->d_out;
   J.out_mode = 1;
-  const bool panel = use_panel(ctx, n);
+  const bool panel = use_panel(ctx, n, p.fk);
   if (panel) {
     if ((rc = ensure_piv(ctx, ld, 1))) return rc;
     J.piv = slot_piv(ctx, 0);
@@ -1539,7 +1546,7 @@ int b200tau_solve_tau_full(b200tau_ctx *ctx, const b200tau_job *job, double *tau
   if ((rc = ensure_workspace(ctx, ld, std::max(1, ctx->slots), p))) return rc;
   if ((rc = ensure_jobs(ctx, 1))) return rc;
   if ((rc = ensure_v(ctx, ld, 1))) return rc;
-  const bool panel = use_panel(ctx, a.N);
+  const bool panel = use_panel(ctx, a.N, kFactorFP64);
   if (panel && (rc = ensure_piv(ctx, ld, 1))) return rc;
   JobDev J;
   std::memset(&J, 0, sizeof(J));

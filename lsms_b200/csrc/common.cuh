@@ -216,9 +216,10 @@ cudaError_t launch_pivot_finish(const JobDev *jobs, int njobs, cudaStream_t s, l
 cudaError_t launch_copy_to_factor(FactorKind fk, const double2 *M, void *F, int n, int ld, cudaStream_t s);
 // FP64 re-solve of the mixed jobs whose refinement did not converge, on the device: out[w] is
 // jobs[w] with F at f64 + w * f64_stride (an FP64 copy of M is made there) and no converged flag,
-// or an inactive record when jobs[w] converged; `count` accumulates the re-solved jobs.
+// or an inactive record when jobs[w] converged; `count` accumulates the re-solved jobs.  Without
+// `panel` the records lose their pivot buffer (the re-solve pivots inside the diagonal blocks).
 cudaError_t launch_fallback_prepare(const JobDev *jobs, JobDev *out, int njobs, double2 *f64, size_t f64_stride,
-                                    int max_N, int *count, cudaStream_t s, long *launches);
+                                    int max_N, int *count, bool panel, cudaStream_t s, long *launches);
 // tau00 from the Schur block directly (no refinement): out = S^-1 t0 (- t0, rotated).
 cudaError_t launch_finalize_direct(FactorKind fk, const JobDev *jobs, int njobs, int ns, int kkrsz,
                                    int *info, cudaStream_t s, long *launches);

@@ -301,10 +301,11 @@ def test_noncollinear_n4320_matches_reference(solver_factory, ref):
     """Non-collinear kkrsz_ns = 32 over the 135-site fcc LIZ (N = 4320), spin-dependent phase
     shifts with a random moment per site (condition numbers 1e5..1e7), five (atom, energy) jobs.
     The reference's own two solvers disagree on these matrices by `spread` = |zgesv (0x2001) -
-    zblock_lu (0x2005)| (up to ~4e-11); the FP64 path (panel pivoting, the default at this size)
-    must agree with zgesv within max(1e-12, spread) and with zblock_lu within max(1e-12,
-    2 spread), on the full path (device-built M) and solver-only on the reference's own M; the
-    MIXED path within 1e-10 of FP64 without re-solving any job in FP64."""
+    zblock_lu (0x2005)| (up to ~4e-11); the FP64 path, with its default pivots inside the diagonal
+    blocks and with panel pivoting forced, must agree with zgesv within max(1e-12, spread) and with
+    zblock_lu within max(1e-12, 2 spread), on the full path (device-built M) and solver-only on the
+    reference's own M; the MIXED path (panel pivoting, the default at this size) within 1e-10 of
+    FP64 without re-solving any job in FP64."""
     wl = W.config_noncollinear_batch(n_atoms=2)
     s = solver_factory(3, 2, 2)
     s.upload_tmat(wl.tmat_store)
@@ -315,6 +316,11 @@ def test_noncollinear_n4320_matches_reference(solver_factory, ref):
     fp64 = s.solve_jobs(T.make_jobs(specs), T.PREC_FP64)
     mixed = s.solve_jobs(T.make_jobs(specs), T.PREC_MIXED)
     assert s.last_fallback_count == 0
+    s.set_pivoting(T.PIVOT_PANEL)
+    try:
+        fp64_panel = s.solve_jobs(T.make_jobs(specs), T.PREC_FP64)
+    finally:
+        s.set_pivoting(T.PIVOT_AUTO)
     for k, (a, iie) in enumerate(picks):
         prob = wl.problem(a)
         assert prob.nrmat_ns == 4320
@@ -322,8 +328,9 @@ def test_noncollinear_n4320_matches_reference(solver_factory, ref):
         zgesv = ref.calculate_tau(prob, iie, 0, ref.ZGESV)
         spread = tau_err(prob, iie, 0, zgesv, blocklu)
         tol_z, tol_b = max(TOL_FP64, spread), max(TOL_FP64, 2 * spread)
-        assert tau_err(prob, iie, 0, fp64[k], zgesv) <= tol_z, (a, iie, tau_err(prob, iie, 0, fp64[k], zgesv), spread)
-        assert tau_err(prob, iie, 0, fp64[k], blocklu) <= tol_b, (a, iie, tau_err(prob, iie, 0, fp64[k], blocklu), spread)
+        for got in (fp64[k], fp64_panel[k]):
+            assert tau_err(prob, iie, 0, got, zgesv) <= tol_z, (a, iie, tau_err(prob, iie, 0, got, zgesv), spread)
+            assert tau_err(prob, iie, 0, got, blocklu) <= tol_b, (a, iie, tau_err(prob, iie, 0, got, blocklu), spread)
         assert tau_err(prob, iie, 0, mixed[k], fp64[k]) <= TOL_MIXED, (a, iie, tau_err(prob, iie, 0, mixed[k], fp64[k]))
         if k < 2:  # solver-only on the reference's own matrix
             m = ref.build_kkr(prob, iie)
