@@ -28,7 +28,7 @@
 namespace b200tau_lsms {
 
 // The precision used by the adapter (B200TAU_PREC_*); the linearSolver id that selects this
-// build path is decoded by the caller.
+// build path (a new id in the reference's linearSolver bitfield) is decoded by the caller.
 inline int &precision() {
   static thread_local int prec = B200TAU_PREC_MIXED;
   return prec;

@@ -10,7 +10,8 @@ import numpy as np
 import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-REF = "/root/reference"
+# the reference tree, as oracle/Makefile reads it (REF, with the same default)
+REF = os.environ.get("REF", "/root/reference")
 LIBDIR = os.path.join(ROOT, "lsms_b200", "_lib")
 
 
