@@ -730,7 +730,7 @@ int run_pipeline(b200tau_ctx *ctx, const std::vector<JobDev> &h, int nw, int max
 // records in device memory, so one graph serves every wave of the same shape and buffers: a solve
 // call then costs the host a record copy and a graph launch, and a host that stalls between the
 // launches of a wave can no longer leave the GPU idle.  Captured on first use of its key; the
-// refinement's later rounds size their sweep clusters for all of the wave's jobs.  The FP64
+// refinement's later rounds size their sweep clusters for a quarter of the wave's jobs.  The FP64
 // re-solve of unconverged mixed jobs stays a separate graph (fallback_graph).
 int wave_graph(b200tau_ctx *ctx, int nw, int maxL, int maxn, int maxN, int ld, const Plan &p, bool panel,
                const TcMaps *tc, WaveGraph **out) {
@@ -765,9 +765,12 @@ int wave_graph(b200tau_ctx *ctx, int nw, int maxL, int maxn, int maxN, int ld, c
       const CUtensorMap *fmap = tc ? &tc->tFu : nullptr;
       if (e == cudaSuccess)
         e = launch_refine_begin(p.fk, ctx->d_jobs, nw, maxn, maxN, ctx->b, ctx->d_info, cs, &n, fp32_sweep, fmap);
+      // rounds after kHintAfterRounds size their sweep clusters for a quarter of the wave (most jobs
+      // have converged by then; if more are left their clusters run in two waves, which costs about
+      // what the smaller clusters would)
       for (int it = 0; it < p.steps && e == cudaSuccess; ++it)
         e = launch_refine_round(p.fk, ctx->d_jobs, nw, maxn, maxN, ctx->b, true, ctx->d_info, cs, &n, fp32_sweep,
-                                fmap, 0, ctx->d_active);
+                                fmap, it >= kHintAfterRounds ? std::max(1, (nw + 3) / 4) : 0, ctx->d_active);
       if (e == cudaSuccess) e = launch_refine_end(ctx->d_jobs, nw, ctx->ns, ctx->kkrsz, cs, &n);
     } else if (e == cudaSuccess) {
       e = launch_finalize_direct(p.fk, ctx->d_jobs, nw, ctx->ns, ctx->kkrsz, ctx->d_info, cs, &n);

@@ -375,10 +375,11 @@ int resident_clusters(const void *kern, int cs, int smem) {
   return v;
 }
 
-// The largest power-of-two cluster (up to 8 CTAs) whose clusters for every job are resident at
+// The largest power-of-two cluster (up to 8 CTAs) whose clusters for `want` jobs are resident at
 // once, at the kernel's real occupancy (several CTAs per SM where the shared memory allows): the
 // per-step latency chain of a job shrinks with its cluster, so one full wave of the largest
-// clusters is the fastest.
+// clusters is the fastest.  `want` is the number of jobs expected to work (converged jobs' clusters
+// leave at once), so late refinement rounds with few jobs left take larger clusters.
 template <typename K>
 int cluster_for(K *kern, int smem, int njobs) {
   for (int cs = kMaxCluster; cs > 1; cs >>= 1)
@@ -387,26 +388,28 @@ int cluster_for(K *kern, int smem, int njobs) {
 }
 
 template <typename T, typename V, int BC>
-cudaError_t sweep_impl(const JobDev *jobs, int njobs, bool forward, int mode, cudaStream_t s) {
+cudaError_t sweep_impl(const JobDev *jobs, int njobs, bool forward, int mode, cudaStream_t s, int want) {
   cudaError_t e;
   if (forward) {
     const int smem = SweepSmem<T, V>::kForward;
     if ((e = ensure_smem(forward_sweep_kernel<T, V, BC>, smem)) != cudaSuccess)
       return e;
-    const int cs = cluster_for(forward_sweep_kernel<T, V, BC>, smem, njobs);
+    const int cs = cluster_for(forward_sweep_kernel<T, V, BC>, smem, want);
     return launch_cluster(forward_sweep_kernel<T, V, BC>, cs, njobs, 256, smem, s, jobs);
   }
   const int smem = SweepSmem<T, V>::kBackward;
   if ((e = ensure_smem(backward_sweep_kernel<T, V, BC>, smem)) != cudaSuccess)
     return e;
-  const int cs = cluster_for(backward_sweep_kernel<T, V, BC>, smem, njobs);
+  const int cs = cluster_for(backward_sweep_kernel<T, V, BC>, smem, want);
   return launch_cluster(backward_sweep_kernel<T, V, BC>, cs, njobs, 256, smem, s, jobs, mode);
 }
 
 template <typename T, typename V>
-cudaError_t sweep_b(const JobDev *jobs, int njobs, int b, bool forward, int mode, cudaStream_t s) {
-  return b <= 16 ? sweep_impl<T, V, 16>(jobs, njobs, forward, mode, s)
-                 : sweep_impl<T, V, 32>(jobs, njobs, forward, mode, s);
+cudaError_t sweep_b(const JobDev *jobs, int njobs, int b, bool forward, int mode, cudaStream_t s,
+                    int active_hint = 0) {
+  const int want = active_hint > 0 && active_hint < njobs ? active_hint : njobs;
+  return b <= 16 ? sweep_impl<T, V, 16>(jobs, njobs, forward, mode, s, want)
+                 : sweep_impl<T, V, 32>(jobs, njobs, forward, mode, s, want);
 }
 
 }  // namespace
@@ -416,14 +419,14 @@ cudaError_t launch_sweep(FactorKind fk, const JobDev *jobs, int njobs, int b, in
                          bool fp32_arith, const CUtensorMap *fmap, cudaStream_t s, int active_hint) {
   if (njobs <= 0) return cudaSuccess;
   if (b < 1 || b > kMaxB || (forward && mode != 1)) return cudaErrorInvalidValue;
-  if (fk == kFactorFP64) return sweep_b<double2, double2>(jobs, njobs, b, forward, mode, s);
+  if (fk == kFactorFP64) return sweep_b<double2, double2>(jobs, njobs, b, forward, mode, s, active_hint);
   if (fp32_arith) {
     bool done = false;
     const cudaError_t e = launch_flow_sweep(jobs, njobs, b, max_N, forward, mode, fmap, s, &done, active_hint);
     if (e != cudaSuccess || done) return e;
-    return sweep_b<float2, float2>(jobs, njobs, b, forward, mode, s);
+    return sweep_b<float2, float2>(jobs, njobs, b, forward, mode, s, active_hint);
   }
-  return sweep_b<float2, double2>(jobs, njobs, b, forward, mode, s);
+  return sweep_b<float2, double2>(jobs, njobs, b, forward, mode, s, active_hint);
 }
 
 }  // namespace b200
