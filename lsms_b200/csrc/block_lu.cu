@@ -55,8 +55,8 @@ constexpr int kRg = kDiagThreads / kNb;  // row groups
 constexpr int kRq = kNb / kRg;           // rows per thread
 
 template <typename T>
-__global__ void __launch_bounds__(kDiagThreads) diag_inverse_kernel(const JobDev *__restrict__ jobs, int k,
-                                                                    int *info) {
+__global__ void __launch_bounds__(kDiagThreads, 2) diag_inverse_kernel(const JobDev *__restrict__ jobs, int k,
+                                                                       int *info) {
   constexpr int NB = kNb;
   const JobDev &J = jobs[blockIdx.x];
   if (k >= J.n || J.inactive) return;
@@ -617,7 +617,20 @@ cudaError_t eliminate_lookahead(const JobDev *jobs, int njobs, int max_n, int ma
                                 int smem_diag, int smem_gemm, bool panel) {
   cudaError_t e;
   const FactorKind fk = sizeof(T) == sizeof(double2) ? kFactorFP64 : kFactorFP32;
-  const int free_sms = njobs < tc_num_sms() / 2 ? njobs : tc_num_sms() / 2;
+  // SMs left to the second stream's work during the interior update.  The update is a persistent
+  // kernel with a fixed share of tiles per CTA, so a CTA of it that cannot start (an inverse took
+  // its SM) delays the whole launch: without panel pivoting the inverses, which the scheduler may
+  // spread one per SM, get one SM per job.  With panel pivoting the row selection (one block per
+  // SM) runs first on the second stream, in waves over the SMs left to it, and the inverses then
+  // pack at their occupancy: one wave of those is enough, and the update keeps more SMs.
+  int per_sm = 1;
+  if (panel && (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, diag_inverse_kernel<T>, kDiagThreads,
+                                                               smem_diag) != cudaSuccess ||
+                per_sm < 1)) {
+    cudaGetLastError();
+    per_sm = 1;
+  }
+  const int free_sms = std::min((njobs + per_sm - 1) / per_sm, tc_num_sms() / 2);
   if (panel) {
     if ((e = launch_pivot_init(jobs, njobs, s, launches)) != cudaSuccess) return e;
     if ((e = launch_panel_select(fk, jobs, njobs, 0, max_n, s, launches)) != cudaSuccess) return e;
@@ -684,11 +697,9 @@ cudaError_t eliminate_impl(const JobDev *jobs, int njobs, int max_n, int max_N, 
   cudaError_t e;
   if ((e = ensure_smem(diag_inverse_kernel<T>, smem_diag)) != cudaSuccess)
     return e;
-  if ((e = cudaFuncSetAttribute(zgemm_tile_kernel<S, kOverwrite>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem_gemm)) != cudaSuccess)
+  if ((e = ensure_smem(zgemm_tile_kernel<S, kOverwrite>, smem_gemm)) != cudaSuccess)
     return e;
-  if ((e = cudaFuncSetAttribute(zgemm_tile_kernel<S, kSubtract>,
-                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem_gemm)) != cudaSuccess)
+  if ((e = ensure_smem(zgemm_tile_kernel<S, kSubtract>, smem_gemm)) != cudaSuccess)
     return e;
   // Look-ahead (tensor-core path): the update of step k first covers the tile holding the next
   // step's diagonal block; the next diagonal inverse then runs on the second stream while the other
