@@ -466,7 +466,7 @@ int encode_factor_map(b200tau_ctx *ctx, int ld, int slots) {
   EncodeTiledFn enc = reinterpret_cast<EncodeTiledFn>(fn);
   const cuuint64_t dims[3] = {(cuuint64_t)2 * ld, (cuuint64_t)ld, (cuuint64_t)slots};
   const cuuint64_t strides[2] = {(cuuint64_t)2 * ld * sizeof(float), (cuuint64_t)ctx->f_bytes};
-  const cuuint32_t box[3] = {128, 64, 1};
+  const cuuint32_t box[3] = {128, (cuuint32_t)kTcPieceCols, 1};
   const cuuint32_t estr[3] = {1, 1, 1};
   CUresult r = enc(&ctx->tc.tF, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, ctx->d_F, dims, strides, box, estr,
                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,

@@ -149,13 +149,15 @@ struct KernelTimer {
 // Per wave slot: A pack 2 ld rows x 128 floats (hi and lo), B pack ld rows x 128 floats.
 struct TcMaps {
   CUtensorMap tA_hi, tA_lo, tB_hi, tB_lo;
-  CUtensorMap tF;   // the wave's FP32 factor slots as floats {2 ld, ld, slots}, box {128, 64, 1}
+  CUtensorMap tF;   // the wave's FP32 factor slots as floats {2 ld, ld, slots}, box {128, kTcPieceCols, 1}
   CUtensorMap tFu;  // the same slots, box {32, 32, 1}, MN-major TF32 swizzle: a quarter of a sweep unit
   float *a_hi = nullptr, *a_lo = nullptr, *b_hi = nullptr, *b_lo = nullptr;
   size_t a_slot = 0, b_slot = 0;  // floats per slot
 };
 // K floats per TMA box of the operand packs (64-byte rows, 64-byte swizzle)
 constexpr int kTcChunk = 16;
+// columns of F per TMA reduce-add of the update's epilogue
+constexpr int kTcPieceCols = 32;
 size_t tc_smem_bytes();
 int tc_num_sms();
 cudaError_t tc_prepare();

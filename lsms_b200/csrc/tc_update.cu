@@ -13,8 +13,8 @@
 //   Atil (2m x 2K) expands every complex a of A21 into [[ar, -ai], [ai, ar]],
 // i.e. one real GEMM with M = 2m, N = n, K = 2 kb and 8 m n kb real FLOPs, the complex FLOP count.
 // tc_pack_kernel writes Atil and Bhat K-major (128 floats per row, hi and lo parts) once per
-// step; tc_update_kernel loads 128 x 32 / 256 x 32 float boxes of them with TMA (128-byte
-// swizzle) into a 2-stage shared-memory ring and issues tcgen05.mma kind::tf32 (M = 128,
+// step; tc_update_kernel loads 128 x 16 / 256 x 16 float boxes of them with TMA (64-byte
+// swizzle) into a 4-stage shared-memory ring and issues tcgen05.mma kind::tf32 (M = 128,
 // N = 256, K = 8) from one thread; the 128 x 256 FP32 accumulator lives in TMEM (256 columns);
 // four epilogue warps move it out with tcgen05.ld into shared memory and TMA reduce-add it (negated)
 // onto F, so the C tile's read-modify-write is done by L2 asynchronously to the SM.
@@ -38,11 +38,11 @@ constexpr int kTN = kTcTileCols;  // columns per tile
 constexpr int kTK = kTcChunk;     // floats per K chunk (64 bytes: one 64-byte swizzle span)
 constexpr int kKReal = 2 * kNb;   // 128 real K per step
 constexpr int kChunks = kKReal / kTK;
-constexpr int kStages = 3;
+constexpr int kStages = 4;  // 3 x 48 KB in flight per SM covers the L2 latency at the MMA rate
 constexpr int kABytes = kTM * kTK * 4;  // 8 KB
 constexpr int kBBytes = kTN * kTK * 4;  // 16 KB
 constexpr int kStageBytes = 2 * kABytes + 2 * kBBytes;
-constexpr int kPieceCols = 64;          // epilogue: columns per TMA reduce-add
+constexpr int kPieceCols = kTcPieceCols;  // epilogue: columns per TMA reduce-add
 constexpr int kAccCols = kTN;           // TMEM columns per accumulator (two of them)
 constexpr long kWaitBound = 1L << 22;
 
@@ -178,7 +178,7 @@ __device__ __forceinline__ void mbar_arrive(unsigned long long *b) {
 }
 
 // Persistent: one CTA per SM loops over the launch's tiles.  Warp 0 (one thread) streams the
-// operand chunks through a 3-stage ring; warp 1 owns TMEM (2 x 256 columns) and issues the MMAs
+// operand chunks through a 4-stage ring; warp 1 owns TMEM (2 x 256 columns) and issues the MMAs
 // of tile i into accumulator i % 2; warps 2..5 drain the other accumulator meanwhile (tcgen05.ld ->
 // negated -> shared-memory staging -> TMA reduce-add onto F), so one tile's epilogue overlaps
 // the next tile's MMAs.
@@ -295,7 +295,7 @@ __global__ void __launch_bounds__(192, 1)
       }
     }
   } else {
-    // Epilogue, warps 2..5 -> TMEM lane quarter (warp % 4), 32 real rows each.  Each 64-column
+    // Epilogue, warps 2..5 -> TMEM lane quarter (warp % 4), 32 real rows each.  Each 32-column
     // piece of the accumulator is negated into a staging buffer (two, alternating) and added onto
     // F by one TMA reduce-add (cp.reduce.async.bulk.tensor .add.f32): the read-modify-write of the
     // C tile happens in L2, asynchronously to the SM.  Rows/columns of a tile beyond the trailing
@@ -417,6 +417,8 @@ __global__ void __launch_bounds__(256) tc_pack_kernel(const JobDev *__restrict__
 }
 
 }  // namespace
+
+static_assert(sizeof(TcSmem) + 1024 <= 232448, "tc_update shared memory above the per-block limit");
 
 size_t tc_smem_bytes() { return sizeof(TcSmem) + 1024; }
 
