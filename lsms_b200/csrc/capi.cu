@@ -411,7 +411,7 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
 // 3-D float tensor (128 floats per row, `rows` rows per slot, `slots` slots) read in
-// kTcChunk x box_rows boxes with 64-byte swizzle; out-of-range rows read as zero.
+// kTcChunk x box_rows boxes with 128-byte swizzle; out-of-range rows read as zero.
 int encode_pack_map(b200tau_ctx *ctx, EncodeTiledFn enc, CUtensorMap *map, float *base, int rows, int slots,
                     int box_rows) {
   const cuuint64_t dims[3] = {128, (cuuint64_t)rows, (cuuint64_t)slots};
@@ -419,7 +419,7 @@ int encode_pack_map(b200tau_ctx *ctx, EncodeTiledFn enc, CUtensorMap *map, float
   const cuuint32_t box[3] = {(cuuint32_t)kTcChunk, (cuuint32_t)box_rows, 1};
   const cuuint32_t estr[3] = {1, 1, 1};
   const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, estr,
-                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
+                         CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                          CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(ctx, B200TAU_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
   return B200TAU_OK;

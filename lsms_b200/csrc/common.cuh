@@ -154,8 +154,8 @@ struct TcMaps {
   float *a_hi = nullptr, *a_lo = nullptr, *b_hi = nullptr, *b_lo = nullptr;
   size_t a_slot = 0, b_slot = 0;  // floats per slot
 };
-// K floats per TMA box of the operand packs (64-byte rows, 64-byte swizzle)
-constexpr int kTcChunk = 16;
+// K floats per TMA box of the operand packs (128-byte rows, 128-byte swizzle)
+constexpr int kTcChunk = 32;
 // columns of F per TMA reduce-add of the update's epilogue
 constexpr int kTcPieceCols = 32;
 size_t tc_smem_bytes();

@@ -13,8 +13,8 @@
 //   Atil (2m x 2K) expands every complex a of A21 into [[ar, -ai], [ai, ar]],
 // i.e. one real GEMM with M = 2m, N = n, K = 2 kb and 8 m n kb real FLOPs, the complex FLOP count.
 // tc_pack_kernel writes Atil and Bhat K-major (128 floats per row, hi and lo parts) once per
-// step; tc_update_kernel loads 128 x 16 / 256 x 16 float boxes of them with TMA (64-byte
-// swizzle) into a 4-stage shared-memory ring and issues tcgen05.mma kind::tf32 (M = 128,
+// step; tc_update_kernel loads 128 x 32 / 256 x 32 float boxes of them with TMA (128-byte
+// swizzle) into a 2-stage shared-memory ring and issues tcgen05.mma kind::tf32 (M = 128,
 // N = 256, K = 8) from one thread; the 128 x 256 FP32 accumulator lives in TMEM (256 columns);
 // four epilogue warps move it out with tcgen05.ld into shared memory and TMA reduce-add it (negated)
 // onto F, so the C tile's read-modify-write is done by L2 asynchronously to the SM.
@@ -35,12 +35,14 @@ namespace {
 
 constexpr int kTM = 128;          // real rows per tile (64 complex rows)
 constexpr int kTN = kTcTileCols;  // columns per tile
-constexpr int kTK = kTcChunk;     // floats per K chunk (64 bytes: one 64-byte swizzle span)
+constexpr int kTK = kTcChunk;     // floats per K chunk (128 bytes: one 128-byte swizzle span)
 constexpr int kKReal = 2 * kNb;   // 128 real K per step
 constexpr int kChunks = kKReal / kTK;
-constexpr int kStages = 4;  // 3 x 48 KB in flight per SM covers the L2 latency at the MMA rate
-constexpr int kABytes = kTM * kTK * 4;  // 8 KB
-constexpr int kBBytes = kTN * kTK * 4;  // 16 KB
+// Two 96 KB stages.  A box row is one TMA request, so 128-byte rows move twice the bytes per
+// request of 64-byte ones; the TMA request rate, not L2 bandwidth, bounds the operand stream.
+constexpr int kStages = 2;
+constexpr int kABytes = kTM * kTK * 4;  // 16 KB
+constexpr int kBBytes = kTN * kTK * 4;  // 32 KB
 constexpr int kStageBytes = 2 * kABytes + 2 * kBBytes;
 constexpr int kPieceCols = kTcPieceCols;  // epilogue: columns per TMA reduce-add
 constexpr int kAccCols = kTN;           // TMEM columns per accumulator (two of them)
@@ -100,16 +102,16 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, i
       : "memory");
 }
 
-// K-major, 64-byte-swizzled operand: rows 64 B apart, 8-row groups 512 B apart (SBO),
-// LBO unused (1), descriptor version 1 (sm_100), layout type 4 = SWIZZLE_64B.
+// K-major, 128-byte-swizzled operand: rows 128 B apart, 8-row groups 1024 B apart (SBO),
+// LBO unused (1), descriptor version 1 (sm_100), layout type 2 = SWIZZLE_128B.
 __device__ __forceinline__ uint64_t smem_desc(const void *p) {
   const uint64_t addr = su32(p);
   uint64_t d = 0;
   d |= (addr >> 4) & 0x3FFFull;
   d |= (uint64_t)1 << 16;              // LBO (ignored for swizzled K-major)
-  d |= (uint64_t)(512 >> 4) << 32;     // SBO
+  d |= (uint64_t)(1024 >> 4) << 32;    // SBO
   d |= (uint64_t)1 << 46;              // version
-  d |= (uint64_t)4 << 61;              // SWIZZLE_64B
+  d |= (uint64_t)2 << 61;              // SWIZZLE_128B
   return d;
 }
 
@@ -178,7 +180,7 @@ __device__ __forceinline__ void mbar_arrive(unsigned long long *b) {
 }
 
 // Persistent: one CTA per SM loops over the launch's tiles.  Warp 0 (one thread) streams the
-// operand chunks through a 4-stage ring; warp 1 owns TMEM (2 x 256 columns) and issues the MMAs
+// operand chunks through a 2-stage ring; warp 1 owns TMEM (2 x 256 columns) and issues the MMAs
 // of tile i into accumulator i % 2; warps 2..5 drain the other accumulator meanwhile (tcgen05.ld ->
 // negated -> shared-memory staging -> TMA reduce-add onto F), so one tile's epilogue overlaps
 // the next tile's MMAs.
