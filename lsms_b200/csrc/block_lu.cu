@@ -44,29 +44,39 @@ template <> struct Vec2<float> { using t = float2; };
 // partial pivoting inside the block on |re| + |im| (izamax's measure; ties go to the lowest row).
 // Rows are never interchanged: step p pivots on the not-yet-used row pv with the largest
 // |A[pv][p]|, and the permutation is applied when the block is written back (for the in-place
-// result P, A^-1[i][pv_k] = P[pv_i][k]).  The block lives in registers, thread (c, g) holding
-// column c and rows g + kRg q; per step the pivot column (the multipliers) and the scaled pivot
-// row pass through shared memory, with two barriers.  The column-p entries follow the same rank-1
-// update as the others because the published pivot row holds dinv + 1 in column p:
-// A[r][p] - f_r (dinv + 1) = -f_r dinv, since A[r][p] = f_r.
+// result P, A^-1[i][pv_k] = P[pv_i][k]).
+// One Gauss-Jordan step as a single rank-1 update of the whole block, A[r][c] -= g_r u_c, with
+//   u = row pv, except u_p = d + 1 (d = A[pv][p]);   g_r = A[r][p] / d (r != pv),  g_pv = 1 - 1/d:
+// row pv becomes A[pv][c] / d, column p becomes -A[r][p] / d, and A[pv][p] becomes 1/d, as the
+// in-place inverse needs, with no special cases in the update.
+// Layout: warp w holds columns 8w .. 8w + 7 and lane l rows l and l + 32, in registers (the step
+// loop is not unrolled: an unrolled body outgrows the instruction caches).  Per step the warp
+// holding column p finds the pivot (warp argmax) and publishes g; after the one block barrier of
+// the step, in every warp the lane holding row pv publishes u over the warp's columns (a per-warp
+// slot in shared memory, read only by that warp) and all lanes apply the update.
 // ---------------------------------------------------------------------------------------------
 constexpr int kDiagThreads = 256;
-constexpr int kRg = kDiagThreads / kNb;  // row groups
-constexpr int kRq = kNb / kRg;           // rows per thread
+constexpr int kDiagWarps = kDiagThreads / 32;
+static_assert(kDiagWarps * 8 == kNb && kNb == 64, "diagonal inverse layout: 8 columns per warp, 2 rows per lane");
 
-template <typename T>
-__global__ void __launch_bounds__(kDiagThreads, 2) diag_inverse_kernel(const JobDev *__restrict__ jobs, int k,
-                                                                       int *info) {
+// PER_SM = blocks per SM the register budget allows: 1 (the update's chains unconstrained, for the
+// elimination that keeps one SM per job free for the inverses) or 2 (two per SM, for the
+// elimination with panel pivoting, which leaves fewer SMs to them).
+template <typename T, int PER_SM>
+__global__ void __launch_bounds__(kDiagThreads, PER_SM) diag_inverse_kernel(const JobDev *__restrict__ jobs, int k,
+                                                                            int *info) {
   constexpr int NB = kNb;
   const JobDev &J = jobs[blockIdx.x];
   if (k >= J.n || J.inactive) return;
   const int kb = min(NB, J.n - k);
   extern __shared__ __align__(16) double2 dyn_smem[];
   double2(*As)[NB + 1] = reinterpret_cast<double2(*)[NB + 1]>(dyn_smem);  // staging As[row][col]
-  __shared__ double2 s_f[2][NB];   // column p before the step: the multipliers
-  __shared__ double2 s_rp[2][NB];  // pivot row scaled by dinv, dinv + 1 in column p
-  __shared__ double s_cval[2][kRg];
-  __shared__ int s_cidx[2][kRg];
+  __shared__ double2 s_f[NB];                 // column p before the step (the pivot warp's scratch)
+  __shared__ double2 s_g[2][NB];              // the step's row factors g, by step parity
+  __shared__ double2 s_row[kDiagWarps][8];    // per warp: u over the warp's columns
+  __shared__ double2 s_dinv;                  // 1 / d (the pivot warp's scratch)
+  __shared__ int s_pvp[2];
+  __shared__ int s_sing[2];
   __shared__ int s_pv[NB], s_inv[NB];
   T *__restrict__ Fk = static_cast<T *>(J.F) + (size_t)k + (size_t)k * J.ld;
   const int tid = threadIdx.x;
@@ -74,104 +84,137 @@ __global__ void __launch_bounds__(kDiagThreads, 2) diag_inverse_kernel(const Job
     const int cc = e / kb, r = e - cc * kb;
     As[r][cc] = ldc(Fk + r + (size_t)cc * J.ld);
   }
-  __syncthreads();
-  const int c = tid % NB, g = tid / NB;
-  double2 a[kRq];
-#pragma unroll
-  for (int q = 0; q < kRq; ++q) {
-    const int r = g + kRg * q;
-    a[q] = (r < kb && c < kb) ? As[r][c] : make_double2(0.0, 0.0);
-  }
-  unsigned long long used = 0;  // rows already pivoted on (the same in every thread)
-  bool singular = false;
   if (tid < NB) s_inv[tid] = tid;  // every entry in range whatever the pivots
+  __syncthreads();
+  const int w = tid >> 5, l = tid & 31;
+  double2 a[2][8];
+#pragma unroll
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int r = l + 32 * i, c = 8 * w + j;
+      a[i][j] = (r < kb && c < kb) ? As[r][c] : make_double2(0.0, 0.0);
+    }
+  // rows already pivoted on (rows past kb count as used, so they are never chosen)
+  bool used0 = l >= kb, used1 = l + 32 >= kb;
+  bool singular = false;
+#pragma unroll 1
   for (int p = 0; p < kb; ++p) {
     const int par = p & 1;
-    if (c == p) {  // this row group's candidate, and the multipliers
-      // the first unused row is the candidate until a larger one is seen, so that a NaN column
-      // still yields an unused row in range (NaN compares false)
+    if (w == (p >> 3)) {
+      // column p & 7 of this warp's registers (opaque copies: the compiler otherwise turns the
+      // selection into an indexed local-memory load)
+      double2 x0 = make_double2(0.0, 0.0), x1 = x0;
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        double2 t0 = a[0][j], t1 = a[1][j];
+        asm volatile("" : "+d"(t0.x), "+d"(t0.y), "+d"(t1.x), "+d"(t1.y));
+        if (j == (p & 7)) {
+          x0 = t0;
+          x1 = t1;
+        }
+      }
+      s_f[l] = x0;
+      s_f[l + 32] = x1;
+      // this lane's candidate: the first unused row until a larger one is seen, so that a NaN
+      // column still yields an unused row in range (NaN compares false)
       double best = -1.0;
       int bi = NB;
-#pragma unroll
-      for (int q = 0; q < kRq; ++q) {
-        const int r = g + kRg * q;
-        const double v = cabs1(a[q]);
-        if (r < kb && !((used >> r) & 1ull) && (bi == NB || v > best)) {
+      if (!used0) {
+        best = cabs1(x0);
+        bi = l;
+      }
+      if (!used1) {
+        const double v = cabs1(x1);
+        if (bi == NB || v > best) {
           best = v;
-          bi = r;
+          bi = l + 32;
         }
-        s_f[par][r] = a[q];
       }
-      s_cval[par][g] = best;
-      s_cidx[par][g] = bi;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (oi != NB && (bi == NB || ob > best || (ob == best && oi < bi))) {
+          best = ob;
+          bi = oi;
+        }
+      }
+      // lane 0's result for all (the lanes agree unless the column holds NaNs); kb - p unused
+      // rows remain, so it is a row < kb
+      const int pv = min(__shfl_sync(0xffffffffu, bi, 0), kb - 1);
+      __syncwarp();
+      if (l == 0) {  // 1/d = conj(d) / |d|^2 (pivots of these blocks are far from the FP64 range limits)
+        const double2 d = s_f[pv];
+        const bool zero = d.x == 0.0 && d.y == 0.0;
+        double2 dinv = make_double2(0.0, 0.0);
+        if (!zero) {
+          const double rr = 1.0 / (d.x * d.x + d.y * d.y);
+          dinv = make_double2(d.x * rr, -d.y * rr);
+        }
+        s_dinv = dinv;
+        s_pvp[par] = pv;
+        s_sing[par] = zero ? 1 : 0;
+        s_pv[p] = pv;
+      }
+      __syncwarp();
+      // the column is read back from shared memory: keeping it live across the reduction costs
+      // registers the update needs
+      const double2 dinv = s_dinv;
+      s_g[par][l] = (l == pv) ? make_double2(1.0 - dinv.x, -dinv.y) : cmul(s_f[l], dinv);
+      s_g[par][l + 32] = (l + 32 == pv) ? make_double2(1.0 - dinv.x, -dinv.y) : cmul(s_f[l + 32], dinv);
     }
     __syncthreads();
-    double best = s_cval[par][0];
-    int pv = s_cidx[par][0];
+    const int pv = s_pvp[par];
+    if (s_sing[par]) singular = true;
+    const int pl = pv & 31, pi = pv >> 5;
+    if (l == pl) {  // publish u over this warp's columns, then mark row pv used
 #pragma unroll
-    for (int i = 1; i < kRg; ++i) {
-      const double v = s_cval[par][i];
-      const int ix = s_cidx[par][i];
-      if (ix != NB && (pv == NB || v > best || (v == best && ix < pv))) {
-        best = v;
-        pv = ix;
+      for (int jj = 0; jj < 8; ++jj) {
+        double2 v = pi ? a[1][jj] : a[0][jj];
+        if (8 * w + jj == p) v.x += 1.0;
+        s_row[w][jj] = v;
       }
+      if (pi) used1 = true;
+      else used0 = true;
     }
-    // kb - p unused rows remain, so some group has one: pv < kb
-    pv = min(pv, kb - 1);
-    used |= 1ull << pv;
-    const double2 d = s_f[par][pv];
-    double2 dinv = make_double2(0.0, 0.0);
-    if (d.x == 0.0 && d.y == 0.0) {
-      singular = true;
-    } else {  // conj(d) / |d|^2 (pivots of these blocks are far from the FP64 range limits)
-      const double rr = 1.0 / (d.x * d.x + d.y * d.y);
-      dinv = make_double2(d.x * rr, -d.y * rr);
-    }
-    if (g == pv % kRg) {  // the warps holding row pv publish it, scaled
-      double2 v = make_double2(0.0, 0.0);
+    __syncwarp();
+    const double2 g0 = s_g[par][l], g1 = s_g[par][l + 32];
 #pragma unroll
-      for (int q = 0; q < kRq; ++q) {
-        double2 t = a[q];
-        asm volatile("" : "+d"(t.x), "+d"(t.y));  // an opaque copy: the compiler otherwise turns the
-                                                  // selection into an indexed local-memory load
-        if (q == pv / kRg) v = t;
-      }
-      s_rp[par][c] = (c == p) ? make_double2(dinv.x + 1.0, dinv.y) : cmul(v, dinv);
-    }
-    if (tid == 0) s_pv[p] = pv;
-    __syncthreads();
-    const double2 rp = s_rp[par][c];
-#pragma unroll
-    for (int q = 0; q < kRq; ++q) {
-      const int r = g + kRg * q;
-      if (r == pv) {
-        a[q] = (c == p) ? dinv : cmul(a[q], dinv);
-      } else {
-        const double2 f = s_f[par][r];
-        a[q].x = fma(-f.x, rp.x, a[q].x);
-        a[q].x = fma(f.y, rp.y, a[q].x);
-        a[q].y = fma(-f.x, rp.y, a[q].y);
-        a[q].y = fma(-f.y, rp.x, a[q].y);
-      }
+    for (int jj = 0; jj < 8; ++jj) {
+      const double2 u = s_row[w][jj];
+      a[0][jj].x = fma(-g0.x, u.x, a[0][jj].x);
+      a[0][jj].x = fma(g0.y, u.y, a[0][jj].x);
+      a[0][jj].y = fma(-g0.x, u.y, a[0][jj].y);
+      a[0][jj].y = fma(-g0.y, u.x, a[0][jj].y);
+      a[1][jj].x = fma(-g1.x, u.x, a[1][jj].x);
+      a[1][jj].x = fma(g1.y, u.y, a[1][jj].x);
+      a[1][jj].y = fma(-g1.x, u.y, a[1][jj].y);
+      a[1][jj].y = fma(-g1.y, u.x, a[1][jj].y);
     }
   }
+  __syncthreads();
   if (tid < kb) s_inv[s_pv[tid]] = tid;
   __syncthreads();
-  if (c < kb) {
-    const int col = s_pv[c];
 #pragma unroll
-    for (int q = 0; q < kRq; ++q) {
-      const int r = g + kRg * q;
-      if (r < kb) As[s_inv[r]][col] = a[q];
+  for (int i = 0; i < 2; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int r = l + 32 * i, c = 8 * w + j;
+      if (r < kb && c < kb) As[s_inv[r]][s_pv[c]] = a[i][j];
     }
-  }
   __syncthreads();
   for (int e = tid; e < kb * kb; e += kDiagThreads) {
     const int cc = e / kb, r = e - cc * kb;
     stc(Fk + r + (size_t)cc * J.ld, As[r][cc]);
   }
   if (singular && tid == 0) atomicCAS(&info[blockIdx.x], 0, k + 1);
+}
+
+template <typename T>
+void launch_diag_inverse(bool packed, const JobDev *jobs, int njobs, int k, int *info, int smem, cudaStream_t s) {
+  if (packed) diag_inverse_kernel<T, 2><<<njobs, kDiagThreads, smem, s>>>(jobs, k, info);
+  else diag_inverse_kernel<T, 1><<<njobs, kDiagThreads, smem, s>>>(jobs, k, info);
 }
 
 // ---------------------------------------------------------------------------------------------
@@ -624,7 +667,7 @@ cudaError_t eliminate_lookahead(const JobDev *jobs, int njobs, int max_n, int ma
   // SM) runs first on the second stream, in waves over the SMs left to it, and the inverses then
   // pack at their occupancy: one wave of those is enough, and the update keeps more SMs.
   int per_sm = 1;
-  if (panel && (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, diag_inverse_kernel<T>, kDiagThreads,
+  if (panel && (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, diag_inverse_kernel<T, 2>, kDiagThreads,
                                                                smem_diag) != cudaSuccess ||
                 per_sm < 1)) {
     cudaGetLastError();
@@ -636,7 +679,7 @@ cudaError_t eliminate_lookahead(const JobDev *jobs, int njobs, int max_n, int ma
     if ((e = launch_panel_select(fk, jobs, njobs, 0, max_n, s, launches)) != cudaSuccess) return e;
     if ((e = launch_row_moves(fk, jobs, njobs, 0, 0, max_N, max_N, s, launches)) != cudaSuccess) return e;
   }
-  diag_inverse_kernel<T><<<njobs, kDiagThreads, smem_diag, s>>>(jobs, 0, info);
+  launch_diag_inverse<T>(panel, jobs, njobs, 0, info, smem_diag, s);
   if (launches) *launches += 1;
   for (int k = 0; k < max_n; k += kNb) {
     const int rest = max_N - k - 1;
@@ -662,7 +705,7 @@ cudaError_t eliminate_lookahead(const JobDev *jobs, int njobs, int max_n, int ma
           if ((e = launch_row_moves(fk, jobs, njobs, k + kNb, 0, split, max_N, la.s2, launches)) != cudaSuccess)
             return e;
         }
-        diag_inverse_kernel<T><<<njobs, kDiagThreads, smem_diag, la.s2>>>(jobs, k + kNb, info);
+        launch_diag_inverse<T>(panel, jobs, njobs, k + kNb, info, smem_diag, la.s2);
         if ((e = cudaEventRecord(la.diag, la.s2)) != cudaSuccess) return e;
       }
       if ((e = launch_tc_update(tc, jobs, njobs, k, max_N, err, s, panel ? 4 : 2,
@@ -679,7 +722,7 @@ cudaError_t eliminate_lookahead(const JobDev *jobs, int njobs, int max_n, int ma
         if ((e = launch_panel_select(fk, jobs, njobs, k + kNb, max_n, s, launches)) != cudaSuccess) return e;
         if ((e = launch_row_moves(fk, jobs, njobs, k + kNb, 0, max_N, max_N, s, launches)) != cudaSuccess) return e;
       }
-      diag_inverse_kernel<T><<<njobs, kDiagThreads, smem_diag, s>>>(jobs, k + kNb, info);
+      launch_diag_inverse<T>(panel, jobs, njobs, k + kNb, info, smem_diag, s);
       if (launches) *launches += 1;
     }
   }
@@ -695,7 +738,9 @@ cudaError_t eliminate_impl(const JobDev *jobs, int njobs, int max_n, int max_N, 
   const int smem_diag = kNb * (kNb + 1) * (int)sizeof(double2);
   const int smem_gemm = 4 * kKc * kTile * (int)sizeof(T);
   cudaError_t e;
-  if ((e = ensure_smem(diag_inverse_kernel<T>, smem_diag)) != cudaSuccess)
+  if ((e = ensure_smem(diag_inverse_kernel<T, 1>, smem_diag)) != cudaSuccess)
+    return e;
+  if ((e = ensure_smem(diag_inverse_kernel<T, 2>, smem_diag)) != cudaSuccess)
     return e;
   if ((e = ensure_smem(zgemm_tile_kernel<S, kOverwrite>, smem_gemm)) != cudaSuccess)
     return e;
@@ -713,7 +758,7 @@ cudaError_t eliminate_impl(const JobDev *jobs, int njobs, int max_n, int max_N, 
       if ((e = launch_panel_select(fk, jobs, njobs, k, max_n, s, launches)) != cudaSuccess) return e;
       if ((e = launch_row_moves(fk, jobs, njobs, k, 0, max_N, max_N, s, launches)) != cudaSuccess) return e;
     }
-    diag_inverse_kernel<T><<<njobs, kDiagThreads, smem_diag, s>>>(jobs, k, info);
+    launch_diag_inverse<T>(panel, jobs, njobs, k, info, smem_diag, s);
     const int rest = max_N - k - 1;
     const int tiles = (rest + kTile - 1) / kTile;
     if (launches) *launches += 1;
