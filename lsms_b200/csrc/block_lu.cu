@@ -932,6 +932,7 @@ cudaError_t launch_eliminate(FactorKind fk, const JobDev *jobs, int njobs, int m
                                            sparse_jobs, nullptr, panel);
   if (tc) {
     cudaError_t e = tc_prepare();
+    if (e == cudaSuccess) e = launch_tc_counters_reset(*tc, s);
     if (e != cudaSuccess) return e;
   }
   return eliminate_impl<float2, float>(jobs, njobs, max_n, max_N, info, s, launches, timer, tc, err, sparse_jobs,

@@ -433,7 +433,11 @@ int ensure_tc(b200tau_ctx *ctx, int ld, int slots) {
   ld = std::max(ld, ctx->tc_ld);
   slots = std::max(slots, ctx->tc_slots);
   const size_t a_slot = (size_t)2 * ld * 128, b_slot = (size_t)ld * 128;
-  CK(cudaMalloc(&ctx->d_pack, sizeof(float) * 2 * (a_slot + b_slot) * slots));
+  const int counter_slots = (ld / kNb + 1) * kTcCountersPerStep;
+  const size_t pack_bytes = sizeof(float) * 2 * (a_slot + b_slot) * slots;
+  CK(cudaMalloc(&ctx->d_pack, pack_bytes + sizeof(int) * counter_slots));
+  // pack rows past a step's trailing block feed only F's padding, but must be finite numbers
+  CK(cudaMemset(ctx->d_pack, 0, pack_bytes + sizeof(int) * counter_slots));
   TcMaps &t = ctx->tc;
   t.a_slot = a_slot;
   t.b_slot = b_slot;
@@ -441,6 +445,8 @@ int ensure_tc(b200tau_ctx *ctx, int ld, int slots) {
   t.a_lo = t.a_hi + a_slot * slots;
   t.b_hi = t.a_lo + a_slot * slots;
   t.b_lo = t.b_hi + b_slot * slots;
+  t.counters = reinterpret_cast<int *>(t.b_lo + b_slot * slots);
+  t.counter_slots = counter_slots;
   void *fn = nullptr;
   cudaDriverEntryPointQueryResult q;
   CK(cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q));
@@ -451,6 +457,8 @@ int ensure_tc(b200tau_ctx *ctx, int ld, int slots) {
   if ((rc = encode_pack_map(ctx, enc, &t.tA_lo, t.a_lo, 2 * ld, slots, 128))) return rc;
   if ((rc = encode_pack_map(ctx, enc, &t.tB_hi, t.b_hi, ld, slots, 256))) return rc;
   if ((rc = encode_pack_map(ctx, enc, &t.tB_lo, t.b_lo, ld, slots, 256))) return rc;
+  if ((rc = encode_pack_map(ctx, enc, &t.tB2_hi, t.b_hi, ld, slots, 128))) return rc;
+  if ((rc = encode_pack_map(ctx, enc, &t.tB2_lo, t.b_lo, ld, slots, 128))) return rc;
   ctx->tc_ld = ld;
   ctx->tc_slots = slots;
   return B200TAU_OK;
@@ -472,6 +480,11 @@ int encode_factor_map(b200tau_ctx *ctx, int ld, int slots) {
                    CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                    CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return fail(ctx, B200TAU_ERR_CUDA, "cuTensorMapEncodeTiled (F) failed (%d)", (int)r);
+  const cuuint32_t wbox[3] = {32, (cuuint32_t)kTcPieceCols, 1};
+  r = enc(&ctx->tc.tFw, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, ctx->d_F, dims, strides, wbox, estr,
+          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return fail(ctx, B200TAU_ERR_CUDA, "cuTensorMapEncodeTiled (F, warp box) failed (%d)", (int)r);
   // the sweeps' operand units: 32 real rows x 32 columns per box, in the tensor core's MN-major
   // TF32 layout (128-byte swizzle on 32-byte atoms)
   const cuuint32_t ubox[3] = {32, 32, 1};

@@ -149,11 +149,16 @@ struct KernelTimer {
 // Per wave slot: A pack 2 ld rows x 128 floats (hi and lo), B pack ld rows x 128 floats.
 struct TcMaps {
   CUtensorMap tA_hi, tA_lo, tB_hi, tB_lo;
+  CUtensorMap tB2_hi, tB2_lo;  // the B packs in 128-column boxes: one CTA's half of a pair tile
   CUtensorMap tF;   // the wave's FP32 factor slots as floats {2 ld, ld, slots}, box {128, kTcPieceCols, 1}
+  CUtensorMap tFw;  // the same slots, box {32, kTcPieceCols, 1}: one epilogue warp's rows of a piece
   CUtensorMap tFu;  // the same slots, box {32, 32, 1}, MN-major TF32 swizzle: a quarter of a sweep unit
   float *a_hi = nullptr, *a_lo = nullptr, *b_hi = nullptr, *b_lo = nullptr;
   size_t a_slot = 0, b_slot = 0;  // floats per slot
+  int *counters = nullptr;        // tile counters of the pair update, kTcCountersPerStep per step
+  int counter_slots = 0;
 };
+constexpr int kTcCountersPerStep = 8;
 // K floats per TMA box of the operand packs (128-byte rows, 128-byte swizzle)
 constexpr int kTcChunk = 32;
 // columns of F per TMA reduce-add of the update's epilogue
@@ -165,13 +170,16 @@ cudaError_t tc_prepare();
 cudaError_t launch_tc_step(const TcMaps &maps, const JobDev *jobs, int njobs, int k, int max_N, int *err,
                            cudaStream_t s);
 // The two halves: the hi/lo operand packs of step k (A21, and W unless the W = D A12 tiles wrote
-// theirs), and the update of the tiles of `part` (0 all, 1 the tile holding the next diagonal
-// block, 2 the others; 3 the first tile column, which holds the next step's whole panel, 4 the
-// other tile columns) on at most max_grid SMs (0: all).
+// theirs), and the update of the tiles of `part` (0 all, 1 the first 256 rows of the first tile
+// column, which hold the next diagonal block, 2 the others; 3 the first tile column, which holds
+// the next step's whole panel, 4 the other tile columns) on at most max_grid SMs (0: all).
+// Parts 0, 2 and 4 run on CTA pairs and take their tiles from maps.counters, which the
+// elimination zeroes before its first step (launch_tc_counters_reset).
 cudaError_t launch_tc_pack(const TcMaps &maps, const JobDev *jobs, int njobs, int k, int max_N, cudaStream_t s,
                            bool pack_b);
 cudaError_t launch_tc_update(const TcMaps &maps, const JobDev *jobs, int njobs, int k, int max_N, int *err,
                              cudaStream_t s, int part, int max_grid);
+cudaError_t launch_tc_counters_reset(const TcMaps &maps, cudaStream_t s);
 // A second stream and two events for the elimination's look-ahead (all null: none).
 struct Lookahead {
   cudaStream_t s2 = nullptr;
