@@ -249,6 +249,14 @@ int b200tau_set_mixed_fallback(b200tau_ctx *ctx, int enable);
  * reference. */
 int b200tau_set_graphs(b200tau_ctx *ctx, int enable);
 
+/* Paired elimination steps (MIXED with BLOCK pivoting): while the trailing block after the second
+ * of two 64-column steps has at least min_rest columns, both steps' updates of it are applied in
+ * one tensor-core pass (K = 128 complex), so its FP32 read-modify-write, which bounds the update,
+ * happens once per two steps; the strips the second step needs first are updated separately.
+ * The factors, and so the refinement and tau00, are those of single steps.  min_rest = 0 turns
+ * it off; default 768.  No counterpart in the reference. */
+int b200tau_set_paired_steps(b200tau_ctx *ctx, int min_rest);
+
 /* Row pivoting of the block elimination (B200TAU_PIVOT_*), both precisions.  BLOCK pivots inside
  * each 64 x 64 diagonal block, as the reference's GPU solver inverts its diagonal blocks
  * (zblock_lu_cuda_c.cu:218-259).  PANEL picks each 64-column step's rows from the whole

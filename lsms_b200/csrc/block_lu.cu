@@ -231,10 +231,15 @@ enum { kOverwrite = 0, kSubtract = 1 };
 
 // Optional second output of the W = D A12 tiles (FP32, tensor-core path): W's hi/lo TF32 split in
 // the K-major operand layout of the trailing update (column c of the trailing block at
-// b + z * slot + c * 2 kNb floats, (re, im) of row p at 2 p), job z = the launch's job index.
+// b + z * slot + c * kTcKMax + k_off floats, (re, im) of row p at 2 p), job z = the launch's job
+// index.  With shift_k >= 0 the trailing block is that of the next step shift_k (its columns
+// start kb(shift_k) further right; W's columns left of it are not packed), and this step's rows
+// go to K offset k_off: the first half of a two-step update's operand.
 struct PackB {
   float *hi = nullptr, *lo = nullptr;
   size_t slot = 0;
+  int shift_k = -1;
+  int k_off = 0;
 };
 
 __device__ __forceinline__ float tf32_round(float x) {
@@ -244,8 +249,8 @@ __device__ __forceinline__ float tf32_round(float x) {
 }
 
 template <typename S, int MODE>
-__device__ __forceinline__ void zgemm_tile_body(const JobDev &J, int k, int bx, int by, const PackB &pk = PackB(),
-                                                int z = 0) {
+__device__ __forceinline__ void zgemm_tile_body(const JobDev &J, int k, int bx, int by, int bx0, int by0,
+                                                const PackB &pk = PackB(), int z = 0) {
   using T = typename Vec2<S>::t;
   const int N = J.N, ld = J.ld;
   if (k >= J.n || J.inactive) return;
@@ -254,7 +259,7 @@ __device__ __forceinline__ void zgemm_tile_body(const JobDev &J, int k, int bx, 
   T *__restrict__ F = static_cast<T *>(J.F);
   int row0, m;
   const T *Ab;
-  const int col0 = k + kb + bx * kTile;
+  const int col0 = k + kb + (bx + bx0) * kTile;
   int n = N - col0;
   if (n <= 0) return;
   if (MODE == kOverwrite) {
@@ -263,7 +268,7 @@ __device__ __forceinline__ void zgemm_tile_body(const JobDev &J, int k, int bx, 
     m = kb;
     Ab = F + (size_t)k + (size_t)k * ld;  // D (kb x kb)
   } else {
-    row0 = k + kb + by * kTile;
+    row0 = k + kb + (by + by0) * kTile;
     m = N - row0;
     if (m <= 0) return;
     Ab = F + (size_t)row0 + (size_t)k * ld;  // A21
@@ -345,11 +350,15 @@ __device__ __forceinline__ void zgemm_tile_body(const JobDev &J, int k, int bx, 
       const int r = tx + 16 * i;
       if (MODE == kOverwrite && sizeof(S) == 4 && pk.hi != nullptr) {
         // rows past kb pack as zero
-        const float wr = r < m ? (float)acc[i][j].x : 0.f, wi = r < m ? (float)acc[i][j].y : 0.f;
-        const float hr = tf32_round(wr), hi = tf32_round(wi);
-        const size_t o = (size_t)z * pk.slot + (size_t)(bx * kTile + c) * (2 * kNb);
-        reinterpret_cast<float2 *>(pk.hi + o)[r] = make_float2(hr, hi);
-        reinterpret_cast<float2 *>(pk.lo + o)[r] = make_float2(wr - hr, wi - hi);
+        const int shift = pk.shift_k >= 0 ? min(kNb, J.n - pk.shift_k) : 0;
+        const int prow = (bx + bx0) * kTile + c - shift;
+        if (prow >= 0) {
+          const float wr = r < m ? (float)acc[i][j].x : 0.f, wi = r < m ? (float)acc[i][j].y : 0.f;
+          const float hr = tf32_round(wr), hi = tf32_round(wi);
+          const size_t o = (size_t)z * pk.slot + (size_t)prow * kTcKMax + pk.k_off;
+          reinterpret_cast<float2 *>(pk.hi + o)[r] = make_float2(hr, hi);
+          reinterpret_cast<float2 *>(pk.lo + o)[r] = make_float2(wr - hr, wi - hi);
+        }
       }
       if (r >= m) continue;
       T *dst = Cb + (size_t)r + (size_t)c * ld;
@@ -368,11 +377,12 @@ __device__ __forceinline__ void zgemm_tile_body(const JobDev &J, int k, int bx, 
 // inactive and a full grid would spend its time launching CTAs that exit at once).
 // Two resident CTAs per SM: with K = 64 per step each CTA runs only four K-chunks, so its operand
 // prologue and C read-modify-write latencies are hidden by the other CTA's FMAs.
+// Tiles start at column tile bx0 and row tile by0 of the step's trailing block.
 template <typename S, int MODE>
 __global__ void __launch_bounds__(256, 2) zgemm_tile_kernel(const JobDev *__restrict__ jobs, int k, int tx, int ty,
-                                                            int nj, PackB pk) {
+                                                            int nj, PackB pk, int bx0, int by0 = 0) {
   if (gridDim.z == (unsigned)nj && gridDim.x == (unsigned)tx && gridDim.y == (unsigned)ty) {
-    zgemm_tile_body<S, MODE>(jobs[blockIdx.z], k, blockIdx.x, blockIdx.y, pk, blockIdx.z);
+    zgemm_tile_body<S, MODE>(jobs[blockIdx.z], k, blockIdx.x, blockIdx.y, bx0, by0, pk, blockIdx.z);
     return;
   }
   // looping grid: jobs one after another (an inactive job costs one check), its tiles spread
@@ -382,7 +392,7 @@ __global__ void __launch_bounds__(256, 2) zgemm_tile_kernel(const JobDev *__rest
   for (int bz = 0; bz < nj; ++bz) {
     const JobDev &J = jobs[bz];
     if (J.inactive || k >= J.n) continue;
-    for (int vb = b0; vb < tx * ty; vb += nblk) zgemm_tile_body<S, MODE>(J, k, vb % tx, vb / tx);
+    for (int vb = b0; vb < tx * ty; vb += nblk) zgemm_tile_body<S, MODE>(J, k, vb % tx, vb / tx, bx0, by0);
   }
 }
 
@@ -685,15 +695,74 @@ cudaError_t eliminate_lookahead(const JobDev *jobs, int njobs, int max_n, int ma
     const int rest = max_N - k - 1;
     const int tiles = (rest + kTile - 1) / kTile;
     const bool next = k + kNb < max_n;
+    const int k2 = k + kNb;
+    // Paired steps k and k2: the update of the trailing block after k2 by both steps in one pass
+    // (its FP32 read-modify-write, which bounds the update, once per two steps).  Step k's update
+    // of the strips that step k2 needs first (block column k2, which holds the next diagonal
+    // block, and block row k2) runs as SIMT tiles; the factors left in F are those of two
+    // single steps.
+    if (!panel && la.pair_min_rest > 0 && k2 < la.min_n && k2 + kNb < max_n &&
+        max_N - k2 - kNb >= la.pair_min_rest) {
+      const int tiles2 = (max_N - k2 - 1 + kTile - 1) / kTile;
+      const bool next2 = k2 + kNb < max_n;
+      PackB pk0;  // W(k): its columns right of block column k2 -> K half 0 of the pair's B operand
+      pk0.hi = tc.b_hi;
+      pk0.lo = tc.b_lo;
+      pk0.slot = tc.b_slot;
+      pk0.shift_k = k2;
+      zgemm_tile_kernel<S, kOverwrite><<<dim3(tiles, 1, njobs), 256, smem_gemm, s>>>(jobs, k, tiles, 1, njobs, pk0, 0);
+      // step k on block column k2 (all rows below step k) and on block row k2 (right of it): first
+      // the diagonal block of k2, whose inverse then runs on the second stream beside the rest of
+      // the two strips
+      zgemm_tile_kernel<S, kSubtract><<<dim3(1, 1, njobs), 256, smem_gemm, s>>>(jobs, k, 1, 1, njobs, PackB(), 0, 0);
+      if ((e = cudaEventRecord(la.panel, s)) != cudaSuccess) return e;
+      if ((e = cudaStreamWaitEvent(la.s2, la.panel, 0)) != cudaSuccess) return e;
+      launch_diag_inverse<T>(false, jobs, njobs, k2, info, smem_diag, la.s2);
+      if ((e = cudaEventRecord(la.diag, la.s2)) != cudaSuccess) return e;
+      if (tiles > 1) {
+        zgemm_tile_kernel<S, kSubtract><<<dim3(1, tiles - 1, njobs), 256, smem_gemm, s>>>(jobs, k, 1, tiles - 1, njobs,
+                                                                                         PackB(), 0, 1);
+        zgemm_tile_kernel<S, kSubtract><<<dim3(tiles - 1, 1, njobs), 256, smem_gemm, s>>>(jobs, k, tiles - 1, 1,
+                                                                                         njobs, PackB(), 1, 0);
+      }
+      if ((e = cudaStreamWaitEvent(s, la.diag, 0)) != cudaSuccess) return e;
+      PackB pk1;  // W(k2) -> K half 1
+      pk1.hi = tc.b_hi;
+      pk1.lo = tc.b_lo;
+      pk1.slot = tc.b_slot;
+      pk1.k_off = 2 * kNb;
+      zgemm_tile_kernel<S, kOverwrite><<<dim3(tiles2, 1, njobs), 256, smem_gemm, s>>>(jobs, k2, tiles2, 1, njobs,
+                                                                                     pk1, 0);
+      const bool timed = timer && timer->used + 2 <= timer->cap;
+      if (timed) cudaEventRecord(timer->ev[timer->used++], s);
+      if ((e = launch_tc_pack(tc, jobs, njobs, k, 2, k2, max_N, s, false)) != cudaSuccess) return e;
+      if ((e = launch_tc_update(tc, jobs, njobs, k2, max_N, err, s, 1, 0, 2)) != cudaSuccess) return e;
+      if (next2) {
+        if ((e = cudaEventRecord(la.panel, s)) != cudaSuccess) return e;
+        if ((e = cudaStreamWaitEvent(la.s2, la.panel, 0)) != cudaSuccess) return e;
+        launch_diag_inverse<T>(false, jobs, njobs, k2 + kNb, info, smem_diag, la.s2);
+        if ((e = cudaEventRecord(la.diag, la.s2)) != cudaSuccess) return e;
+      }
+      if ((e = launch_tc_update(tc, jobs, njobs, k2, max_N, err, s, 2, next2 ? tc_num_sms() - free_sms : 0, 2)) !=
+          cudaSuccess)
+        return e;
+      if (timed) cudaEventRecord(timer->ev[timer->used++], s);
+      if (next2 && (e = cudaStreamWaitEvent(s, la.diag, 0)) != cudaSuccess) return e;
+      // W(k), the diagonal block, its inverse, W(k2), the pack, the two update launches (+ the
+      // two strips, + the next inverse)
+      if (launches) *launches += 7 + (tiles > 1 ? 2 : 0) + (next2 ? 1 : 0);
+      k = k2;  // the loop's increment moves past k2
+      continue;
+    }
     if (tiles > 0) {
       PackB pk;
       pk.hi = tc.b_hi;
       pk.lo = tc.b_lo;
       pk.slot = tc.b_slot;
-      zgemm_tile_kernel<S, kOverwrite><<<dim3(tiles, 1, njobs), 256, smem_gemm, s>>>(jobs, k, tiles, 1, njobs, pk);
+      zgemm_tile_kernel<S, kOverwrite><<<dim3(tiles, 1, njobs), 256, smem_gemm, s>>>(jobs, k, tiles, 1, njobs, pk, 0);
       const bool timed = timer && timer->used + 2 <= timer->cap;
       if (timed) cudaEventRecord(timer->ev[timer->used++], s);
-      if ((e = launch_tc_pack(tc, jobs, njobs, k, max_N, s, false)) != cudaSuccess) return e;
+      if ((e = launch_tc_pack(tc, jobs, njobs, k, 1, k, max_N, s, false)) != cudaSuccess) return e;
       if ((e = launch_tc_update(tc, jobs, njobs, k, max_N, err, s, panel ? 3 : 1, 0)) != cudaSuccess) return e;
       // the next step's columns left of the tiles still being updated: [0, k + 64 + one tile)
       const int split = k + kNb + kTcTileCols;
@@ -764,7 +833,7 @@ cudaError_t eliminate_impl(const JobDev *jobs, int njobs, int max_n, int max_N, 
     if (launches) *launches += 1;
     if (tiles > 0) {
       zgemm_tile_kernel<S, kOverwrite><<<dim3(tiles, 1, njobs), 256, smem_gemm, s>>>(jobs, k, tiles, 1, njobs,
-                                                                                   PackB());
+                                                                                   PackB(), 0);
       const bool timed = timer && timer->used + 2 <= timer->cap;
       if (timed) cudaEventRecord(timer->ev[timer->used++], s);
       if (tc != nullptr) {
@@ -773,10 +842,10 @@ cudaError_t eliminate_impl(const JobDev *jobs, int njobs, int max_n, int max_N, 
       } else {
         if (sparse_jobs)
           zgemm_tile_kernel<S, kSubtract><<<std::min(tiles * tiles * njobs, kSparseGrid), 256, smem_gemm, s>>>(
-              jobs, k, tiles, tiles, njobs, PackB());
+              jobs, k, tiles, tiles, njobs, PackB(), 0);
         else
           zgemm_tile_kernel<S, kSubtract><<<dim3(tiles, tiles, njobs), 256, smem_gemm, s>>>(jobs, k, tiles, tiles,
-                                                                                           njobs, PackB());
+                                                                                           njobs, PackB(), 0);
       }
       if (timed) cudaEventRecord(timer->ev[timer->used++], s);
       if (launches) *launches += 2;

@@ -151,6 +151,7 @@ struct b200tau_ctx {
   std::vector<FallbackGraph> fb;  // most recently used last
   std::vector<WaveGraph> wg;      // captured wave pipelines, most recently used last
   bool graphs_on = true;          // b200tau_set_graphs
+  int pair_min_rest = kPairMinRest;  // b200tau_set_paired_steps
   // b200tau_set_keep_factors: the last FP64 solve's wave (factors F, KKR matrix M, refined X, slots
   // in `kept_order` order), reusable once by b200tau_solve_vjp on the same jobs
   bool keep_factors = false;
@@ -410,12 +411,12 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t
                                   const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
                                   CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
 
-// 3-D float tensor (128 floats per row, `rows` rows per slot, `slots` slots) read in
+// 3-D float tensor (kTcKMax floats per row, `rows` rows per slot, `slots` slots) read in
 // kTcChunk x box_rows boxes with 128-byte swizzle; out-of-range rows read as zero.
 int encode_pack_map(b200tau_ctx *ctx, EncodeTiledFn enc, CUtensorMap *map, float *base, int rows, int slots,
                     int box_rows) {
-  const cuuint64_t dims[3] = {128, (cuuint64_t)rows, (cuuint64_t)slots};
-  const cuuint64_t strides[2] = {128 * sizeof(float), (cuuint64_t)rows * 128 * sizeof(float)};
+  const cuuint64_t dims[3] = {(cuuint64_t)kTcKMax, (cuuint64_t)rows, (cuuint64_t)slots};
+  const cuuint64_t strides[2] = {kTcKMax * sizeof(float), (cuuint64_t)rows * kTcKMax * sizeof(float)};
   const cuuint32_t box[3] = {(cuuint32_t)kTcChunk, (cuuint32_t)box_rows, 1};
   const cuuint32_t estr[3] = {1, 1, 1};
   const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 3, base, dims, strides, box, estr,
@@ -432,7 +433,7 @@ int ensure_tc(b200tau_ctx *ctx, int ld, int slots) {
   ctx->d_pack = nullptr;
   ld = std::max(ld, ctx->tc_ld);
   slots = std::max(slots, ctx->tc_slots);
-  const size_t a_slot = (size_t)2 * ld * 128, b_slot = (size_t)ld * 128;
+  const size_t a_slot = (size_t)2 * ld * kTcKMax, b_slot = (size_t)ld * kTcKMax;
   const int counter_slots = (ld / kNb + 1) * kTcCountersPerStep;
   const size_t pack_bytes = sizeof(float) * 2 * (a_slot + b_slot) * slots;
   CK(cudaMalloc(&ctx->d_pack, pack_bytes + sizeof(int) * counter_slots));
@@ -511,11 +512,24 @@ int drain_timer(b200tau_ctx *ctx) {
 
 // Algorithmic FLOPs of the trailing updates of one wave: sum over steps and jobs of
 // 8 (N - k - kb)^2 kb (complex multiply-add = 8 real FLOPs).
-double trailing_flops(const std::vector<JobDev> &h) {
+// Algorithmic complex FLOPs of the tensor-core update launches (the ones the profiler times): per
+// single step 8 rest^2 kb; per paired step (the elimination's schedule, block_lu.cu) only the
+// combined pass over the trailing block after the second step, 8 rest2^2 (kb + kb2) -- the strips
+// of the first step run as SIMT tiles outside the timed launches.
+double trailing_flops(const std::vector<JobDev> &h, const Lookahead &la, bool panel, int max_n, int max_N) {
   double f = 0.0;
   for (const JobDev &J : h)
     for (int k = 0; k < J.n; k += kNb) {
+      const int k2 = k + kNb;
       const double kb = std::min(kNb, J.n - k);
+      if (!panel && la.pair_min_rest > 0 && k2 < la.min_n && k2 + kNb < max_n &&
+          max_N - k2 - kNb >= la.pair_min_rest) {
+        const double kb2 = std::min(kNb, J.n - k2);
+        const double rest2 = J.N - k2 - kb2;
+        f += 8.0 * rest2 * rest2 * (kb + kb2);
+        k = k2;
+        continue;
+      }
       const double rest = J.N - k - kb;
       f += 8.0 * rest * rest * kb;
     }
@@ -754,7 +768,7 @@ int wave_graph(b200tau_ctx *ctx, int nw, int maxL, int maxn, int maxN, int ld, c
       ctx->tmat_ld, ctx->group_size, ctx->table_polls, (long long)(uintptr_t)ctx->d_jobs,
       (long long)(uintptr_t)ctx->d_info, (long long)(uintptr_t)ctx->d_active, (long long)(uintptr_t)ctx->d_err,
       (long long)(uintptr_t)ctx->d_tmat, (long long)(uintptr_t)ctx->d_tdiag, (long long)(uintptr_t)ctx->d_F,
-      (long long)(uintptr_t)ctx->d_pack, ctx->tc_ld, ctx->tc_slots};
+      (long long)(uintptr_t)ctx->d_pack, ctx->tc_ld, ctx->tc_slots, ctx->la.min_n, ctx->la.pair_min_rest};
   for (size_t i = 0; i < ctx->wg.size(); ++i)
     if (ctx->wg[i].key == key) {
       const WaveGraph g = ctx->wg[i];  // most recently used last
@@ -863,6 +877,9 @@ int run_wave(b200tau_ctx *ctx, const b200tau_job *jobs, const int *idx, int nw, 
     maxN = std::max(maxN, a.N);
     maxn = std::max(maxn, a.N - a.b);
   }
+  ctx->la.min_n = maxn;
+  for (int w = 0; w < nw; ++w) ctx->la.min_n = std::min(ctx->la.min_n, h[w].n);
+  ctx->la.pair_min_rest = ctx->pair_min_rest;
   CK(cudaMemcpyAsync(ctx->d_jobs, h.data(), sizeof(JobDev) * nw, cudaMemcpyHostToDevice, ctx->stream));
   if (reuse_factors) {
     // the forward solve of these jobs left M, its FP64 block factors and the refined X in these
@@ -901,7 +918,7 @@ int run_wave(b200tau_ctx *ctx, const b200tau_job *jobs, const int *idx, int nw, 
   if (rc || (rc = phase_begin(ctx))) return rc;
   CK(launch_kkr_build(ctx->d_jobs, nw, maxL, build_params(ctx, p), ctx->d_err, ctx->stream, &ctx->launches));
   if ((rc = phase_end(ctx, 0))) return rc;
-  if (ctx->profiling) ctx->prof_flops += trailing_flops(h);
+  if (ctx->profiling) ctx->prof_flops += trailing_flops(h, ctx->la, panel, maxn, maxN);
   if ((rc = run_pipeline(ctx, h, nw, maxn, maxN, ld, ctx->ns, ctx->kkrsz, ctx->b, p, panel))) return rc;
   if (!adj) return B200TAU_OK;
   // adjoint: G into M's storage (M is no longer needed once X is refined), M^-1 from the factors,
@@ -1209,6 +1226,13 @@ int b200tau_set_keep_factors(b200tau_ctx *ctx, int enable) {
   if (!ctx) return B200TAU_ERR_ARG;
   ctx->keep_factors = enable != 0;
   if (!enable) ctx->kept_valid = false;
+  return B200TAU_OK;
+}
+
+int b200tau_set_paired_steps(b200tau_ctx *ctx, int min_rest) {
+  if (!ctx) return B200TAU_ERR_ARG;
+  if (min_rest < 0) return fail(ctx, B200TAU_ERR_ARG, "paired steps: min_rest must be >= 0");
+  ctx->pair_min_rest = min_rest;
   return B200TAU_OK;
 }
 

@@ -146,7 +146,7 @@ struct KernelTimer {
 };
 
 // Operand packs and TMA descriptors of the tensor-core trailing update (tc_update.cu).
-// Per wave slot: A pack 2 ld rows x 128 floats (hi and lo), B pack ld rows x 128 floats.
+// Per wave slot: A pack 2 ld rows x kTcKMax floats (hi and lo), B pack ld rows x kTcKMax floats.
 struct TcMaps {
   CUtensorMap tA_hi, tA_lo, tB_hi, tB_lo;
   CUtensorMap tB2_hi, tB2_lo;  // the B packs in 128-column boxes: one CTA's half of a pair tile
@@ -161,6 +161,9 @@ struct TcMaps {
 constexpr int kTcCountersPerStep = 8;
 // K floats per TMA box of the operand packs (128-byte rows, 128-byte swizzle)
 constexpr int kTcChunk = 32;
+// floats per operand-pack row: the real K of up to two 64-column elimination steps, whose updates
+// of the trailing block the tensor-core kernels can apply in one pass
+constexpr int kTcKMax = 4 * kNb;
 // columns of F per TMA reduce-add of the update's epilogue
 constexpr int kTcPieceCols = 32;
 size_t tc_smem_bytes();
@@ -169,22 +172,37 @@ cudaError_t tc_prepare();
 // Pack + tensor-core update A22 -= A21 W for step k of every job in the wave (FP32 factors).
 cudaError_t launch_tc_step(const TcMaps &maps, const JobDev *jobs, int njobs, int k, int max_N, int *err,
                            cudaStream_t s);
+// The operand packs of an update of the trailing block of step k_last by the steps kA, kA + 64,
+// ... (nblk of them, k_last the last): A = the columns of those steps below row k_last + kb,
+// B (if pack_b) = their rows right of column k_last + kb.  nblk = 1 is a single step (kA = k_last).
 // The two halves: the hi/lo operand packs of step k (A21, and W unless the W = D A12 tiles wrote
 // theirs), and the update of the tiles of `part` (0 all, 1 the first 256 rows of the first tile
 // column, which hold the next diagonal block, 2 the others; 3 the first tile column, which holds
 // the next step's whole panel, 4 the other tile columns) on at most max_grid SMs (0: all).
 // Parts 0, 2 and 4 run on CTA pairs and take their tiles from maps.counters, which the
 // elimination zeroes before its first step (launch_tc_counters_reset).
-cudaError_t launch_tc_pack(const TcMaps &maps, const JobDev *jobs, int njobs, int k, int max_N, cudaStream_t s,
-                           bool pack_b);
+cudaError_t launch_tc_pack(const TcMaps &maps, const JobDev *jobs, int njobs, int kA, int nblk, int k_last,
+                           int max_N, cudaStream_t s, bool pack_b);
+// The update of the trailing block of step k by the last nblk steps (their packs from
+// launch_tc_pack and the W = D A12 tiles), restricted to the tiles of `part`.
 cudaError_t launch_tc_update(const TcMaps &maps, const JobDev *jobs, int njobs, int k, int max_N, int *err,
-                             cudaStream_t s, int part, int max_grid);
+                             cudaStream_t s, int part, int max_grid, int nblk = 1);
 cudaError_t launch_tc_counters_reset(const TcMaps &maps, cudaStream_t s);
 // A second stream and two events for the elimination's look-ahead (all null: none).
 struct Lookahead {
   cudaStream_t s2 = nullptr;
   cudaEvent_t panel = nullptr, diag = nullptr;
+  // Paired steps (FP32 factors with block pivoting): while the trailing block after the second of
+  // two steps has at least pair_min_rest columns, the two steps' updates of it are applied in one
+  // tensor-core pass of K = 128 complex (0: never).  min_n: the smallest n of the wave's jobs
+  // (every job must have both steps).
+  int pair_min_rest = 0;
+  int min_n = 0;
 };
+// default pair_min_rest: paired steps pay for their strip updates once the trailing block's
+// read-modify-write they save is larger (on the 31-point N = 2160 contour 768 measured best of
+// 0, 768, 1024 and 1400)
+constexpr int kPairMinRest = 768;
 
 // cudaFuncSetAttribute(fn, MaxDynamicSharedMemorySize, bytes) on the current device, skipped when
 // an earlier call on this device already allowed at least `bytes` (a per-launch host call costs

@@ -37,8 +37,7 @@ namespace {
 constexpr int kTM = 128;          // real rows per tile (64 complex rows)
 constexpr int kTN = kTcTileCols;  // columns per tile
 constexpr int kTK = kTcChunk;     // floats per K chunk (128 bytes: one 128-byte swizzle span)
-constexpr int kKReal = 2 * kNb;   // 128 real K per step
-constexpr int kChunks = kKReal / kTK;
+constexpr int kStepChunks = 2 * kNb / kTK;  // K chunks of one 64-column step (128 real K)
 // Two 96 KB stages.  A box row is one TMA request, so 128-byte rows move twice the bytes per
 // request of 64-byte ones; the TMA request rate, not L2 bandwidth, bounds the operand stream.
 constexpr int kStages = 2;
@@ -190,7 +189,7 @@ __global__ void __launch_bounds__(192, 1)
     tc_update_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_constant__ CUtensorMap tA_lo,
                      const __grid_constant__ CUtensorMap tB_hi, const __grid_constant__ CUtensorMap tB_lo,
                      const __grid_constant__ CUtensorMap tF, const JobDev *__restrict__ jobs, int k, TileSpace ts,
-                     int *err) {
+                     int nch, int *err) {
   extern __shared__ __align__(1024) unsigned char tc_raw[];
   // the dynamic window is 1024-aligned by the launch (extra 1 KB requested)
   TcSmem &sm = *reinterpret_cast<TcSmem *>((reinterpret_cast<uintptr_t>(tc_raw) + 1023) & ~uintptr_t(1023));
@@ -227,7 +226,7 @@ __global__ void __launch_bounds__(192, 1)
       for (int t = blockIdx.x; t < ts.total && !sm.abort; t += gridDim.x) {
         int z, row0, col0, kb;
         if (!tile_of(jobs, ts, k, t, z, row0, col0, kb)) continue;
-        for (int c = 0; c < kChunks; ++c, ++g) {
+        for (int c = 0; c < nch; ++c, ++g) {
           const int s = (int)(g % kStages);
           if (g >= kStages && !mbar_wait(&sm.empty[s], (unsigned)(((g / kStages) - 1) & 1))) {
             atomicOr(err, kErrUpdateWait);
@@ -266,7 +265,7 @@ __global__ void __launch_bounds__(192, 1)
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         const uint32_t d = tmem + (uint32_t)(a * kAccCols);
         bool ok = true;
-        for (int c = 0; c < kChunks; ++c, ++g) {
+        for (int c = 0; c < nch; ++c, ++g) {
           const int s = (int)(g % kStages);
           if (!mbar_wait(&sm.full[s], (unsigned)((g / kStages) & 1))) {
             atomicOr(err, kErrUpdateWait);
@@ -512,7 +511,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
     tc_update2_kernel(const __grid_constant__ CUtensorMap tA_hi, const __grid_constant__ CUtensorMap tA_lo,
                       const __grid_constant__ CUtensorMap tB_hi, const __grid_constant__ CUtensorMap tB_lo,
                       const __grid_constant__ CUtensorMap tFw, const JobDev *__restrict__ jobs, int k, TileSpace2 ts,
-                      int *counter, int *err) {
+                      int nch, int *counter, int *err) {
   extern __shared__ __align__(1024) unsigned char tc2_raw[];
   Tc2Smem &sm = *reinterpret_cast<Tc2Smem *>((reinterpret_cast<uintptr_t>(tc2_raw) + 1023) & ~uintptr_t(1023));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -556,7 +555,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
         int z, row0, col0, kb;
         tile_of2(jobs, ts, k, t, z, row0, col0, kb);
         const int ra = row0 + (int)rank * kHalf, cb = col0 + (int)rank * kHalf;
-        for (int c = 0; c < kChunks; ++c, ++g) {
+        for (int c = 0; c < nch; ++c, ++g) {
           const int s = (int)(g % kStages2);
           if (g >= kStages2 && !mbar_wait(&sm.empty[s], (unsigned)(((g / kStages2) - 1) & 1))) {
             atomicOr(err, kErrUpdateWait);
@@ -662,7 +661,7 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
           const uint32_t d = tmem + (uint32_t)(a * kAccCols);
           bool ok = true;
-          for (int c = 0; c < kChunks; ++c, ++g) {
+          for (int c = 0; c < nch; ++c, ++g) {
             const int s = (int)(g % kStages2);
             if (!mbar_wait(&sm.full[s], (unsigned)((g / kStages2) & 1))) {
               atomicOr(err, kErrUpdateWait);
@@ -785,46 +784,54 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(192, 1)
   }
 }
 
-// Pack the step's operands K-major with hi/lo TF32 split:
-//   A (blocks [0, nA)): Atil rows 2r, 2r+1 for complex rows r of A21 = F[k+kb+r, k:k+kb]
-//   B (blocks [nA, ..)): Bhat row c = W column F[k:k+kb, k+kb+c]
-// Entries with K index >= 2 kb are zero (short last step).
-__global__ void __launch_bounds__(256) tc_pack_kernel(const JobDev *__restrict__ jobs, int k, int nA,
-                                                      float *__restrict__ a_hi, float *__restrict__ a_lo,
+// Pack the operands K-major with hi/lo TF32 split, for the update of the trailing block of step
+// k_last (rows and columns from R0 = k_last + kb_last) by nblk consecutive steps kA, kA + 64, ...:
+//   A (blocks [0, nA)): Atil rows 2r, 2r+1 for complex rows r of [A21_kA | A21_kA+64 | ...],
+//                       A21_q = F[R0 + r, q : q + kb_q]
+//   B (blocks [nA, ..)): Bhat row c = [W_kA ; W_kA+64 ; ...] column R0 + c (W stored in F's rows)
+// K index 2 (64 q + p) + {0, 1} holds step q's column p; entries with p >= kb_q are zero.  Rows are
+// kTcKMax floats; the update reads the first nblk * 128 of them.
+__global__ void __launch_bounds__(256) tc_pack_kernel(const JobDev *__restrict__ jobs, int kA, int nblk, int k_last,
+                                                      int nA, float *__restrict__ a_hi, float *__restrict__ a_lo,
                                                       float *__restrict__ b_hi, float *__restrict__ b_lo,
                                                       size_t a_slot, size_t b_slot) {
   const JobDev &J = jobs[blockIdx.y];
-  if (k >= J.n) return;
-  const int kb = min(kNb, J.n - k);
-  const int rest = J.N - k - kb;
+  if (k_last >= J.n) return;
+  const int R0 = k_last + min(kNb, J.n - k_last);
+  const int rest = J.N - R0;
   const float2 *F = static_cast<const float2 *>(J.F);
   const int ld = J.ld;
   const int tid = threadIdx.x;
+  const int kw = kNb * nblk;  // complex K of the update
   if ((int)blockIdx.x < nA) {
-    // 4 complex rows per block, 64 threads (one per complex K index) per row
+    // 4 complex rows per block, 64 threads per row, each over the row's K in steps of 64
     const int r = blockIdx.x * 4 + (tid >> 6);
-    const int p = tid & 63;
     if (r >= rest) return;
-    float2 a = make_float2(0.f, 0.f);
-    if (p < kb) a = F[(size_t)(k + kb + r) + (size_t)(k + p) * ld];
-    const float hr = tf32_hi(a.x), hi_ = tf32_hi(a.y);
-    const float lr = a.x - hr, li = a.y - hi_;
-    float *h0 = a_hi + blockIdx.y * a_slot + (size_t)(2 * r) * kKReal;
-    float *l0 = a_lo + blockIdx.y * a_slot + (size_t)(2 * r) * kKReal;
-    // row 2r: (ar, -ai); row 2r+1: (ai, ar)
-    reinterpret_cast<float2 *>(h0)[p] = make_float2(hr, -hi_);
-    reinterpret_cast<float2 *>(l0)[p] = make_float2(lr, -li);
-    reinterpret_cast<float2 *>(h0 + kKReal)[p] = make_float2(hi_, hr);
-    reinterpret_cast<float2 *>(l0 + kKReal)[p] = make_float2(li, lr);
+    float *h0 = a_hi + blockIdx.y * a_slot + (size_t)(2 * r) * kTcKMax;
+    float *l0 = a_lo + blockIdx.y * a_slot + (size_t)(2 * r) * kTcKMax;
+    for (int p = tid & 63; p < kw; p += 64) {
+      const int kq = kA + p;  // column of F
+      float2 a = make_float2(0.f, 0.f);
+      if (kq < J.n) a = F[(size_t)(R0 + r) + (size_t)kq * ld];
+      const float hr = tf32_hi(a.x), hi_ = tf32_hi(a.y);
+      const float lr = a.x - hr, li = a.y - hi_;
+      // row 2r: (ar, -ai); row 2r+1: (ai, ar)
+      reinterpret_cast<float2 *>(h0)[p] = make_float2(hr, -hi_);
+      reinterpret_cast<float2 *>(l0)[p] = make_float2(lr, -li);
+      reinterpret_cast<float2 *>(h0 + kTcKMax)[p] = make_float2(hi_, hr);
+      reinterpret_cast<float2 *>(l0 + kTcKMax)[p] = make_float2(li, lr);
+    }
   } else {
     const int c = (blockIdx.x - nA) * 4 + (tid >> 6);
-    const int p = tid & 63;
     if (c >= rest) return;
-    float2 w = make_float2(0.f, 0.f);
-    if (p < kb) w = F[(size_t)(k + p) + (size_t)(k + kb + c) * ld];
-    const float hr = tf32_hi(w.x), hi_ = tf32_hi(w.y);
-    reinterpret_cast<float2 *>(b_hi + blockIdx.y * b_slot + (size_t)c * kKReal)[p] = make_float2(hr, hi_);
-    reinterpret_cast<float2 *>(b_lo + blockIdx.y * b_slot + (size_t)c * kKReal)[p] = make_float2(w.x - hr, w.y - hi_);
+    for (int p = tid & 63; p < kw; p += 64) {
+      const int kq = kA + p;  // row of F
+      float2 w = make_float2(0.f, 0.f);
+      if (kq < J.n) w = F[(size_t)kq + (size_t)(R0 + c) * ld];
+      const float hr = tf32_hi(w.x), hi_ = tf32_hi(w.y);
+      reinterpret_cast<float2 *>(b_hi + blockIdx.y * b_slot + (size_t)c * kTcKMax)[p] = make_float2(hr, hi_);
+      reinterpret_cast<float2 *>(b_lo + blockIdx.y * b_slot + (size_t)c * kTcKMax)[p] = make_float2(w.x - hr, w.y - hi_);
+    }
   }
 }
 
@@ -847,20 +854,22 @@ int tc_num_sms() {
   return n;
 }
 
-cudaError_t launch_tc_pack(const TcMaps &maps, const JobDev *jobs, int njobs, int k, int max_N, cudaStream_t s,
-                           bool pack_b) {
-  const int rest = max_N - k - 1;  // upper bound of the trailing size over the wave
+cudaError_t launch_tc_pack(const TcMaps &maps, const JobDev *jobs, int njobs, int kA, int nblk, int k_last,
+                           int max_N, cudaStream_t s, bool pack_b) {
+  const int rest = max_N - k_last - 1;  // upper bound of the trailing size over the wave
   if (rest <= 0) return cudaSuccess;
   const int nA = (rest + 3) / 4, nB = pack_b ? (rest + 3) / 4 : 0;
-  tc_pack_kernel<<<dim3(nA + nB, njobs), 256, 0, s>>>(jobs, k, nA, maps.a_hi, maps.a_lo, maps.b_hi, maps.b_lo,
-                                                      maps.a_slot, maps.b_slot);
+  tc_pack_kernel<<<dim3(nA + nB, njobs), 256, 0, s>>>(jobs, kA, nblk, k_last, nA, maps.a_hi, maps.a_lo, maps.b_hi,
+                                                      maps.b_lo, maps.a_slot, maps.b_slot);
   return cudaGetLastError();
 }
 
 cudaError_t launch_tc_update(const TcMaps &maps, const JobDev *jobs, int njobs, int k, int max_N, int *err,
-                             cudaStream_t s, int part, int max_grid) {
+                             cudaStream_t s, int part, int max_grid, int nblk) {
   const int rest = max_N - k - 1;
   if (rest <= 0) return cudaSuccess;
+  if (nblk < 1 || nblk * 2 * kNb > kTcKMax) return cudaErrorInvalidValue;
+  const int nch = nblk * kStepChunks;
   const int sms = max_grid > 0 ? std::min(max_grid, tc_num_sms()) : tc_num_sms();
   if (part == 0 || part == 2 || part == 4) {
     // the interior on CTA pairs, tiles handed out from the launch's counter
@@ -877,7 +886,7 @@ cudaError_t launch_tc_update(const TcMaps &maps, const JobDev *jobs, int njobs, 
     if (maps.counters == nullptr || slot >= maps.counter_slots) return cudaErrorInvalidValue;
     const int pairs = std::max(1, std::min(ts.total, sms / 2));
     tc_update2_kernel<<<2 * pairs, 192, tc2_smem_bytes(), s>>>(maps.tA_hi, maps.tA_lo, maps.tB2_hi, maps.tB2_lo,
-                                                               maps.tFw, jobs, k, ts, maps.counters + slot, err);
+                                                               maps.tFw, jobs, k, ts, nch, maps.counters + slot, err);
     return cudaGetLastError();
   }
   TileSpace ts;
@@ -889,13 +898,13 @@ cudaError_t launch_tc_update(const TcMaps &maps, const JobDev *jobs, int njobs, 
   if (ts.total <= 0) return cudaSuccess;
   const int grid = std::min(ts.total, sms);
   tc_update_kernel<<<grid, 192, tc_smem_bytes(), s>>>(maps.tA_hi, maps.tA_lo, maps.tB_hi, maps.tB_lo, maps.tF, jobs,
-                                                      k, ts, err);
+                                                      k, ts, nch, err);
   return cudaGetLastError();
 }
 
 cudaError_t launch_tc_step(const TcMaps &maps, const JobDev *jobs, int njobs, int k, int max_N, int *err,
                            cudaStream_t s) {
-  cudaError_t e = launch_tc_pack(maps, jobs, njobs, k, max_N, s, true);
+  cudaError_t e = launch_tc_pack(maps, jobs, njobs, k, 1, k, max_N, s, true);
   if (e != cudaSuccess) return e;
   return launch_tc_update(maps, jobs, njobs, k, max_N, err, s, 0, 0);
 }

@@ -54,7 +54,7 @@ EXPORTS = (
     "b200tau_profile_phases", "b200tau_set_mixed_sweep", "b200tau_solve_vjp",
     "b200tau_last_fallback_count", "b200tau_set_mixed_fallback", "b200tau_set_build_wait",
     "b200tau_set_pivoting", "b200tau_solve_tau_full", "b200tau_set_graphs",
-    "b200tau_set_keep_factors",
+    "b200tau_set_keep_factors", "b200tau_set_paired_steps",
 )
 
 
@@ -114,6 +114,7 @@ def load_library():
     lib.b200tau_set_pivoting.argtypes = [P, I]
     lib.b200tau_solve_tau_full.argtypes = [P, P, P, I]
     lib.b200tau_set_graphs.argtypes = [P, I]
+    lib.b200tau_set_paired_steps.argtypes = [P, I]
     lib.b200tau_set_keep_factors.argtypes = [P, I]
     _lib = lib
     return lib
@@ -208,6 +209,11 @@ class TauSolver:
     def set_graphs(self, enable: bool):
         """Each wave as one captured CUDA graph (default) or as separate launches."""
         self._check(self.lib.b200tau_set_graphs(self.ctx, int(bool(enable))))
+
+    def set_paired_steps(self, min_rest: int):
+        """Paired elimination steps (one tensor-core pass for two steps' trailing updates) while the
+        trailing block has at least min_rest columns; 0 turns them off (default 768)."""
+        self._check(self.lib.b200tau_set_paired_steps(self.ctx, int(min_rest)))
 
     def set_pivoting(self, mode: int):
         """Row pivoting of the elimination: PIVOT_AUTO (default), PIVOT_BLOCK or PIVOT_PANEL."""

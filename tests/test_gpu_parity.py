@@ -376,3 +376,29 @@ def test_wave_graphs_match_separate_launches(solver_factory):
             assert max(tau_err(prob, i, 0, m_g[i], m_sep[i]) for i in range(6)) <= 1e-12
     finally:
         s.set_graphs(True)
+
+
+@pytest.mark.parametrize("min_rest", [0, 1, 768])
+def test_paired_steps_match_reference(solver_factory, ref, min_rest):
+    """MIXED at N = 2160 with paired elimination steps everywhere they fit (min_rest = 1), at the
+    default threshold (768) and off: every job converges without the FP64 re-solve and matches the
+    reference's calculateTauMatrix; paired and single steps leave the same factors, so their
+    results agree to the refinement's tolerance."""
+    prob = W.config_n2160(npts=8)
+    s = _solver(solver_factory, prob)
+    jobs = T.make_jobs([(0, i, 0, prob.energies[i]) for i in range(8)])
+    try:
+        s.set_paired_steps(0)
+        single = s.solve_jobs(jobs, T.PREC_MIXED)
+        s.set_paired_steps(min_rest)
+        for graphs in (False, True):
+            s.set_graphs(graphs)
+            mixed = s.solve_jobs(jobs, T.PREC_MIXED)
+            assert s.last_fallback_count == 0
+            for i in range(8):
+                want = ref.calculate_tau(prob, i, 0, ref.ZBLOCKLU_CPP)
+                assert tau_err(prob, i, 0, mixed[i], want) <= TOL_MIXED, (i, tau_err(prob, i, 0, mixed[i], want))
+                assert tau_err(prob, i, 0, mixed[i], single[i]) <= 1e-11
+    finally:
+        s.set_paired_steps(768)
+        s.set_graphs(True)
