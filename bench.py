@@ -42,12 +42,13 @@ N_ENERGIES = 31
 DATA = "synthetic (seeded phase-shift t-matrices, fcc LIZ)"
 CONFIG = {"workload": "fcc LIZ 135 sites a=6.82, lmax 3, N=2160, kkrsz_ns 16, 31-point semicircle contour "
                       "-0.3..0.7 Ry, one atom per GPU"}
-# DRAM bytes (read + write) of the trailing update per elimination step of this workload (the
-# update of the next diagonal tile plus the interior launch): an ncu capture of the trailing-update
-# kernel on a 24-job interior launch at k = 192 measured 17.4 B per trailing-block entry; scaled to
-# 31 jobs and the average trailing block over the 34 steps (1.476e6 entries).  Not measured by
-# this run (a kernel under ncu is not timed).
-TRAFFIC_PER_LAUNCH = 796.1e6
+# DRAM bytes (read + write) of the trailing update per elimination step of this workload: ncu
+# captures measured 18.7 B per trailing-block entry for a paired-step pass (24 jobs, trailing block
+# 1776^2, K = 128 complex; the FP32 read-modify-write of the block once for two steps) and 17.4 B
+# for a single-step pass; over the default schedule (pairs while the block after the second step
+# has >= 768 columns: 10 pairs, 14 single steps) that is 434.9 MB per step on average at 31 jobs.
+# Not measured by this run (a kernel under ncu is not timed).
+TRAFFIC_PER_LAUNCH = 434.9e6
 
 
 def algorithmic_flops(N: int, b: int, L: int) -> float:
@@ -405,6 +406,9 @@ def main():
                     help="contour2160 = the headline line; the others print their own line")
     ap.add_argument("--energies", type=int, default=N_ENERGIES,
                     help="contour points solved per step (31 = the benchmark; fewer for small profiling cases)")
+    ap.add_argument("--no-graphs", action="store_true",
+                    help="launch each wave's kernels one by one instead of replaying its CUDA graph "
+                         "(for profilers, which do not see into graphs with conditional nodes)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup()
@@ -439,6 +443,8 @@ def main():
     flops_per_solve = algorithmic_flops(N, b, L)
     s = T.TauSolver(prob.lmax, prob.n_spin_cant, prob.n_spin_pola, device=local)
     s.load_problem(prob)
+    if args.no_graphs:
+        s.set_graphs(False)
     jobs = T.make_jobs([(0, i, 0, prob.energies[i]) for i in range(ne)])
     out = torch.empty(ne * b * b * 2, dtype=torch.float64, device=f"cuda:{local}")
     stream = torch.cuda.ExternalStream(s.stream, device=f"cuda:{local}")
