@@ -489,11 +489,13 @@ __device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(s), "l"(gmem) : "memory");
 }
 
-// R = B - M X with B = [0; t0] (rows n..N-1 hold t0), FP64.  The product is FP64-FMA bound
-// (b complex multiply-adds per 16-byte element of M), so each thread keeps one row x 16 columns of
-// accumulators and every M element it loads feeds 16 complex FMAs.  M and X stream through a
-// three-stage cp.async ring in shared memory (kResK columns of M and rows of X per stage), so two
-// stages of loads are in flight while one is multiplied; X is read as broadcasts.
+// R = B - M X with B = [0; t0] (rows n..N-1 hold t0), FP64.  The product is FP64 bound (b complex
+// multiply-adds per 16-byte element of M) and runs on the FP64 tensor cores (mma.sync m8n8k4
+// f64): as real products, [Rr | Ri] = Mr [Xr | Xi] + Mi [-Xi | Xr], four 8 x 8 x 4 MMAs per row
+// tile and 8-column block per K step of 4, a few instructions per 1024 FMAs where DFMAs take 32.
+// Each warp owns ROWS / 4 rows (8-row tiles) x BC columns of accumulators.  M and X stream
+// through a three-stage cp.async ring in shared memory (kResK columns of M and rows of X per
+// stage), so two stages of loads are in flight while one is multiplied.
 // BC = 16 or 32 is the padded column count (b <= BC).
 constexpr int kResK = 8;       // K per stage
 constexpr int kResStages = 3;
@@ -508,9 +510,13 @@ __host__ __device__ constexpr int residual_smem_bytes() {
   return kResStages * kResK * (residual_rows<BC>() + BC) * (int)sizeof(double2);
 }
 
-// Register tile of a residual thread: RPT rows (ROWS / RPT apart) x NCT columns, 10 shared-memory
-// loads per 16 complex FMAs.
-template <int BC> struct ResTile { static constexpr int RPT = 2, NCT = 8; };
+// D (8 x 8) += A (8 x 4) B (4 x 8) in FP64 on the tensor cores, per warp: lane l holds
+// a = A[l / 4][l % 4], b = B[l % 4][l / 4] and D[l / 4][2 (l % 4) + i] in d_i.
+__device__ __forceinline__ void dmma_884(double &d0, double &d1, double a, double b) {
+  asm("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};"
+      : "+d"(d0), "+d"(d1)
+      : "d"(a), "d"(b));
+}
 
 // The jobs of a wave still refining: list[0] = their number, list[1..] their indices in order.
 // One warp.
@@ -533,10 +539,10 @@ __global__ void active_list_kernel(const JobDev *__restrict__ jobs, int njobs, i
 template <int BC>
 __global__ void __launch_bounds__(kResThreads, 4) residual_kernel(const JobDev *__restrict__ jobs,
                                                                   const int *__restrict__ active, int rowblocks) {
-  constexpr int RPT = ResTile<BC>::RPT, NCT = ResTile<BC>::NCT;
   constexpr int ROWS = residual_rows<BC>();  // rows per CTA
-  constexpr int RG = ROWS / RPT;             // row groups
-  static_assert(RG * (BC / NCT) == kResThreads, "residual thread layout");
+  constexpr int RT = ROWS / 32;              // 8-row tiles per warp (four warps)
+  constexpr int NB = BC / 8;                 // 8-column blocks
+  static_assert(kResThreads == 128 && RT * 32 == ROWS && NB * 8 == BC && kResK % 4 == 0, "residual layout");
   int jw = blockIdx.x, rb = blockIdx.y;
   if (active != nullptr) {
     const int cnt = active[0], i = blockIdx.x;
@@ -554,7 +560,8 @@ __global__ void __launch_bounds__(kResThreads, 4) residual_kernel(const JobDev *
   double2(*Xs)[kResK][BC] =
       reinterpret_cast<double2(*)[kResK][BC]>(rsm + sizeof(double2) * kResStages * kResK * ROWS);
   const int tid = threadIdx.x;
-  const int rg = tid % RG, cg = tid / RG;
+  const int lane = tid & 31, g = lane >> 2, t = lane & 3;
+  const int wrow = (tid >> 5) * (8 * RT);  // the warp's first row within the CTA's rows
   const double2 *__restrict__ M = J.M;
   const double2 *__restrict__ X = J.X;
   const double2 zero = make_double2(0.0, 0.0);
@@ -575,11 +582,11 @@ __global__ void __launch_bounds__(kResThreads, 4) residual_kernel(const JobDev *
     }
     asm volatile("cp.async.commit_group;" ::: "memory");
   };
-  double2 acc[RPT][NCT];
+  double ar[RT][NB][2], ai[RT][NB][2];  // M X, real and imaginary parts
 #pragma unroll
-  for (int i = 0; i < RPT; ++i)
+  for (int r = 0; r < RT; ++r)
 #pragma unroll
-    for (int j = 0; j < NCT; ++j) acc[i][j] = zero;
+    for (int j = 0; j < NB; ++j) ar[r][j][0] = ar[r][j][1] = ai[r][j][0] = ai[r][j][1] = 0.0;
   const int nst = (N + kResK - 1) / kResK;
 #pragma unroll
   for (int q = 0; q < kResStages - 1; ++q) {
@@ -594,15 +601,20 @@ __global__ void __launch_bounds__(kResThreads, 4) residual_kernel(const JobDev *
     else asm volatile("cp.async.commit_group;" ::: "memory");
     const int st = q % kResStages;
 #pragma unroll
-    for (int kk = 0; kk < kResK; ++kk) {
-      double2 a[RPT];
+    for (int ks = 0; ks < kResK; ks += 4) {
+      double2 xv[NB];
 #pragma unroll
-      for (int i = 0; i < RPT; ++i) a[i] = Ms[st][kk][rg + i * RG];
+      for (int j = 0; j < NB; ++j) xv[j] = Xs[st][ks + t][8 * j + g];
 #pragma unroll
-      for (int j = 0; j < NCT; ++j) {
-        const double2 x = Xs[st][kk][cg * NCT + j];
+      for (int r = 0; r < RT; ++r) {
+        const double2 mv = Ms[st][ks + t][wrow + 8 * r + g];
 #pragma unroll
-        for (int i = 0; i < RPT; ++i) acc[i][j] = cfma(a[i], x, acc[i][j]);
+        for (int j = 0; j < NB; ++j) {
+          dmma_884(ar[r][j][0], ar[r][j][1], mv.x, xv[j].x);
+          dmma_884(ar[r][j][0], ar[r][j][1], mv.y, -xv[j].y);
+          dmma_884(ai[r][j][0], ai[r][j][1], mv.x, xv[j].y);
+          dmma_884(ai[r][j][0], ai[r][j][1], mv.y, xv[j].x);
+        }
       }
     }
   }
@@ -610,17 +622,19 @@ __global__ void __launch_bounds__(kResThreads, 4) residual_kernel(const JobDev *
   // with panel pivoting the factors are those of P M: row gr of R goes to its physical row
   const int *__restrict__ rowpos = J.piv != nullptr ? J.piv + ld : nullptr;
 #pragma unroll
-  for (int i = 0; i < RPT; ++i) {
-    const int gr = row0 + rg + i * RG;
+  for (int r = 0; r < RT; ++r) {
+    const int gr = row0 + wrow + 8 * r + g;
     if (gr >= N) continue;
     const int dst = rowpos != nullptr ? rowpos[gr] : gr;
 #pragma unroll
-    for (int j = 0; j < NCT; ++j) {
-      const int c = cg * NCT + j;
-      if (c >= b) continue;
-      const double2 bv = (gr >= J.n) ? J.t0[(gr - J.n) + (size_t)c * J.t0_ld] : zero;
-      J.R[(size_t)dst + (size_t)c * ld] = csub(bv, acc[i][j]);
-    }
+    for (int j = 0; j < NB; ++j)
+#pragma unroll
+      for (int i = 0; i < 2; ++i) {
+        const int c = 8 * j + 2 * t + i;
+        if (c >= b) continue;
+        const double2 bv = (gr >= J.n) ? J.t0[(gr - J.n) + (size_t)c * J.t0_ld] : zero;
+        J.R[(size_t)dst + (size_t)c * ld] = make_double2(bv.x - ar[r][j][i], bv.y - ai[r][j][i]);
+      }
   }
 }
 
