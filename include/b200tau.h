@@ -249,7 +249,7 @@ int b200tau_set_mixed_fallback(b200tau_ctx *ctx, int enable);
  * reference. */
 int b200tau_set_graphs(b200tau_ctx *ctx, int enable);
 
-/* Paired elimination steps (MIXED with BLOCK pivoting): while the trailing block after the second
+/* Paired elimination steps (MIXED, either pivoting): while the trailing block after the second
  * of two 64-column steps has at least min_rest columns, both steps' updates of it are applied in
  * one tensor-core pass (K = 128 complex), so its FP32 read-modify-write, which bounds the update,
  * happens once per two steps; the strips the second step needs first are updated separately.

@@ -715,6 +715,66 @@ cudaError_t eliminate_lookahead(const JobDev *jobs, int njobs, int max_n, int ma
     // of the strips that step k2 needs first (block column k2, which holds the next diagonal
     // block, and block row k2) runs as SIMT tiles; the factors left in F are those of two
     // single steps.
+    // With panel pivoting the pair keeps every row's pending update the same when step k2's rows
+    // move: block column k2 is updated by step k (all rows) before step k2's selection, and block
+    // row k2 only after its row moves, so that at the moves every row below step k still owes
+    // step k's update right of block column k2 (done for all of them by the combined pass) and
+    // the moves carry A21_k's rows with them.
+    if (panel && la.pair_min_rest > 0 && k2 < la.min_n && k2 + kNb < max_n &&
+        max_N - k2 - kNb >= la.pair_min_rest) {
+      const int tiles2 = (max_N - k2 - 1 + kTile - 1) / kTile;
+      const int split2 = k2 + kNb + kTcTileCols;
+      PackB pk0;  // W(k): its columns right of block column k2 -> K half 0 of the pair's B operand
+      pk0.hi = tc.b_hi;
+      pk0.lo = tc.b_lo;
+      pk0.slot = tc.b_slot;
+      pk0.shift_k = k2;
+      zgemm_tile_kernel<S, kOverwrite><<<dim3(tiles, 1, njobs), 256, smem_gemm, s>>>(jobs, k, tiles, 1, njobs, pk0, 0);
+      // step k on block column k2, every row below step k (the diagonal block included)
+      zgemm_tile_kernel<S, kSubtract><<<dim3(1, tiles, njobs), 256, smem_gemm, s>>>(jobs, k, 1, tiles, njobs,
+                                                                                   PackB(), 0, 0);
+      if ((e = launch_panel_select(fk, jobs, njobs, k2, max_n, s, launches)) != cudaSuccess) return e;
+      if ((e = launch_row_moves(fk, jobs, njobs, k2, 0, max_N, max_N, s, launches)) != cudaSuccess) return e;
+      // the inverse of the moved diagonal block beside step k's update of block row k2
+      if ((e = cudaEventRecord(la.panel, s)) != cudaSuccess) return e;
+      if ((e = cudaStreamWaitEvent(la.s2, la.panel, 0)) != cudaSuccess) return e;
+      launch_diag_inverse<T>(true, jobs, njobs, k2, info, smem_diag, la.s2);
+      if ((e = cudaEventRecord(la.diag, la.s2)) != cudaSuccess) return e;
+      if (tiles > 1)
+        zgemm_tile_kernel<S, kSubtract><<<dim3(tiles - 1, 1, njobs), 256, smem_gemm, s>>>(jobs, k, tiles - 1, 1,
+                                                                                         njobs, PackB(), 1, 0);
+      if ((e = cudaStreamWaitEvent(s, la.diag, 0)) != cudaSuccess) return e;
+      PackB pk1;  // W(k2) -> K half 1
+      pk1.hi = tc.b_hi;
+      pk1.lo = tc.b_lo;
+      pk1.slot = tc.b_slot;
+      pk1.k_off = 2 * kNb;
+      zgemm_tile_kernel<S, kOverwrite><<<dim3(tiles2, 1, njobs), 256, smem_gemm, s>>>(jobs, k2, tiles2, 1, njobs,
+                                                                                     pk1, 0);
+      const bool timed = timer && timer->used + 2 <= timer->cap;
+      if (timed) cudaEventRecord(timer->ev[timer->used++], s);
+      if ((e = launch_tc_pack(tc, jobs, njobs, k, 2, k2, max_N, s, false)) != cudaSuccess) return e;
+      if ((e = launch_tc_update(tc, jobs, njobs, k2, max_N, err, s, 3, 0, 2)) != cudaSuccess) return e;
+      // the next step's selection, its moves left of the tiles still being updated, its inverse
+      if ((e = cudaEventRecord(la.panel, s)) != cudaSuccess) return e;
+      if ((e = cudaStreamWaitEvent(la.s2, la.panel, 0)) != cudaSuccess) return e;
+      if ((e = launch_panel_select(fk, jobs, njobs, k2 + kNb, max_n, la.s2, launches)) != cudaSuccess) return e;
+      if ((e = launch_row_moves(fk, jobs, njobs, k2 + kNb, 0, split2, max_N, la.s2, launches)) != cudaSuccess)
+        return e;
+      launch_diag_inverse<T>(true, jobs, njobs, k2 + kNb, info, smem_diag, la.s2);
+      if ((e = cudaEventRecord(la.diag, la.s2)) != cudaSuccess) return e;
+      if ((e = launch_tc_update(tc, jobs, njobs, k2, max_N, err, s, 4, tc_num_sms() - free_sms, 2)) != cudaSuccess)
+        return e;
+      if (timed) cudaEventRecord(timer->ev[timer->used++], s);
+      if ((e = cudaStreamWaitEvent(s, la.diag, 0)) != cudaSuccess) return e;
+      if ((e = launch_row_moves(fk, jobs, njobs, k2 + kNb, split2, max_N, max_N, s, launches)) != cudaSuccess)
+        return e;
+      // W(k), the column strip, the row strip, k2's inverse, W(k2), the pack, the two update
+      // launches, the next inverse (selections and moves count themselves)
+      if (launches) *launches += 7 + (tiles > 1 ? 1 : 0);
+      k = k2;  // the loop's increment moves past k2
+      continue;
+    }
     if (!panel && la.pair_min_rest > 0 && k2 < la.min_n && k2 + kNb < max_n &&
         max_N - k2 - kNb >= la.pair_min_rest) {
       const int tiles2 = (max_N - k2 - 1 + kTile - 1) / kTile;

@@ -516,14 +516,13 @@ int drain_timer(b200tau_ctx *ctx) {
 // single step 8 rest^2 kb; per paired step (the elimination's schedule, block_lu.cu) only the
 // combined pass over the trailing block after the second step, 8 rest2^2 (kb + kb2) -- the strips
 // of the first step run as SIMT tiles outside the timed launches.
-double trailing_flops(const std::vector<JobDev> &h, const Lookahead &la, bool panel, int max_n, int max_N) {
+double trailing_flops(const std::vector<JobDev> &h, const Lookahead &la, int max_n, int max_N) {
   double f = 0.0;
   for (const JobDev &J : h)
     for (int k = 0; k < J.n; k += kNb) {
       const int k2 = k + kNb;
       const double kb = std::min(kNb, J.n - k);
-      if (!panel && la.pair_min_rest > 0 && k2 < la.min_n && k2 + kNb < max_n &&
-          max_N - k2 - kNb >= la.pair_min_rest) {
+      if (la.pair_min_rest > 0 && k2 < la.min_n && k2 + kNb < max_n && max_N - k2 - kNb >= la.pair_min_rest) {
         const double kb2 = std::min(kNb, J.n - k2);
         const double rest2 = J.N - k2 - kb2;
         f += 8.0 * rest2 * rest2 * (kb + kb2);
@@ -918,7 +917,7 @@ int run_wave(b200tau_ctx *ctx, const b200tau_job *jobs, const int *idx, int nw, 
   if (rc || (rc = phase_begin(ctx))) return rc;
   CK(launch_kkr_build(ctx->d_jobs, nw, maxL, build_params(ctx, p), ctx->d_err, ctx->stream, &ctx->launches));
   if ((rc = phase_end(ctx, 0))) return rc;
-  if (ctx->profiling) ctx->prof_flops += trailing_flops(h, ctx->la, panel, maxn, maxN);
+  if (ctx->profiling) ctx->prof_flops += trailing_flops(h, ctx->la, maxn, maxN);
   if ((rc = run_pipeline(ctx, h, nw, maxn, maxN, ld, ctx->ns, ctx->kkrsz, ctx->b, p, panel))) return rc;
   if (!adj) return B200TAU_OK;
   // adjoint: G into M's storage (M is no longer needed once X is refined), M^-1 from the factors,

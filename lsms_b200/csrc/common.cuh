@@ -192,7 +192,7 @@ cudaError_t launch_tc_counters_reset(const TcMaps &maps, cudaStream_t s);
 struct Lookahead {
   cudaStream_t s2 = nullptr;
   cudaEvent_t panel = nullptr, diag = nullptr;
-  // Paired steps (FP32 factors with block pivoting): while the trailing block after the second of
+  // Paired steps (FP32 factors, either pivoting): while the trailing block after the second of
   // two steps has at least pair_min_rest columns, the two steps' updates of it are applied in one
   // tensor-core pass of K = 128 complex (0: never).  min_n: the smallest n of the wave's jobs
   // (every job must have both steps).
