@@ -15,8 +15,10 @@
 //    shared memory), then arrives on each CTA's `full` barrier of the slot.  A CTA starts step j
 //    as soon as its slot is full, turns the block into the step's tensor-core operand and
 //    releases the slot on its `empty` barrier in the CTA that produces the slot's next use.
-//    Slot s of an ns-deep ring is always produced by the same rank (cs divides ns), so both
-//    barriers count plain phases.
+//    Blocks are produced in turn by the cluster's ranks, so a rank produces every cs-th block and
+//    its `empty` barrier of a slot completes one phase per block it produces into that slot: with
+//    ns >= cs (cs divides ns) every use of the slot, with ns = 4 < cs = 8 (the ring shrunk so
+//    that larger matrices fit shared memory) every other use.
 //  * Operand panels (A21, D or W) stream through a ring of shared-memory stages several units
 //    ahead: a unit is 64 complex rows x 32 columns of the factor, loaded by a producer warp as
 //    four TMA boxes of 32 real rows x 32 columns in the 128-byte/32-byte-atom swizzle, which is
@@ -78,9 +80,15 @@ struct FlowLayout {
   int ring, lo, bstep, bd, slots, tiles, bars, tmem, total;
 };
 __host__ __device__ constexpr int kBars(int ns) { return 2 * ns + 2 * kStages + 9; }
+__host__ __device__ inline FlowLayout flow_layout(int cs, int own, bool forward, int ns);
+// ns = max(cs, 4) block slots, or 4 for cs = 8 when that does not fit shared memory (N = 4320)
 __host__ __device__ inline FlowLayout flow_layout(int cs, int own, bool forward) {
+  const FlowLayout L = flow_layout(cs, own, forward, cs > 4 ? cs : 4);
+  return (L.total > kMaxSmem && cs > 4) ? flow_layout(cs, own, forward, 4) : L;
+}
+__host__ __device__ inline FlowLayout flow_layout(int cs, int own, bool forward, int ns) {
   FlowLayout L;
-  L.ns = cs > 4 ? cs : 4;
+  L.ns = ns;
   L.own = own;
   L.ring = 0;
   L.lo = L.ring + kStages * kUnitBytes;
@@ -631,7 +639,8 @@ __global__ void __launch_bounds__(kBlock, 1)
           acc_read(S, tmem, me & 1, v);
           // Y_(j+1) = D_(j+1) R_(j+1): into J.Y and into slot (j + 1) % ns of every CTA
           const int jd = j + 1, kd = 64 * jd, kbd = min(64, n - kd), slot = jd & nsm;
-          if (jd >= ns) ok = cta_wait<true>(S.empty + slot, ((jd >> lns) - 1) & 1, conv);
+          // this rank's phases of the slot's empty barrier: one per block it produced into the slot
+          if (jd >= ns) ok = cta_wait<true>(S.empty + slot, ((jd - ns) >> max(lns, lcs)) & 1, conv);
           if (!ok) break;
           const float *dst = reinterpret_cast<const float *>(S.slots + slot * kTileElems);
           const bool live = r < kbd;
@@ -775,7 +784,7 @@ __global__ void __launch_bounds__(kBlock, 1)
           // the rows of block s + 1 are final: X (+)= Y there, and the block to every CTA
           const int kn = 64 * tnext, kbn = min(64, n - kn), slot = (s + 1) & nsm;
           if (s + 1 >= ns)
-            ok = cta_wait<true>(S.empty + slot, (((s + 1) >> lns) - 1) & 1, conv);
+            ok = cta_wait<true>(S.empty + slot, (((s + 1) - ns) >> max(lns, lcs)) & 1, conv);
           else
             compute_sync();
           if (!ok) break;
