@@ -42,13 +42,26 @@ N_ENERGIES = 31
 DATA = "synthetic (seeded phase-shift t-matrices, fcc LIZ)"
 CONFIG = {"workload": "fcc LIZ 135 sites a=6.82, lmax 3, N=2160, kkrsz_ns 16, 31-point semicircle contour "
                       "-0.3..0.7 Ry, one atom per GPU"}
-# DRAM bytes (read + write) of the trailing update per elimination step of this workload: ncu
-# captures measured 18.7 B per trailing-block entry for a paired-step pass (24 jobs, trailing block
-# 1776^2, K = 128 complex; the FP32 read-modify-write of the block once for two steps) and 17.4 B
-# for a single-step pass; over the default schedule (pairs while the block after the second step
-# has >= 768 columns: 10 pairs, 14 single steps) that is 434.9 MB per step on average at 31 jobs.
-# Not measured by this run (a kernel under ncu is not timed).
-TRAFFIC_PER_LAUNCH = 434.9e6
+# DRAM bytes (read + write) of the trailing update per trailing-block entry and pass, from ncu
+# captures on this workload: 18.7 B for a paired-step pass (24 jobs, trailing block 1776^2, K = 128
+# complex; the FP32 read-modify-write of the block once for two steps) and 17.4 B for a single-step
+# pass.  Not measured by this run (a kernel under ncu is not timed).
+BYTES_PER_ENTRY_PAIR = 18.7
+BYTES_PER_ENTRY_SINGLE = 17.4
+
+
+def update_traffic_per_step(n, b, jobs, min_rest):
+    """Average DRAM bytes of the trailing update per 64-column elimination step, over the schedule
+    the library runs at paired-steps threshold min_rest (pairs while the block after the second
+    step keeps >= min_rest columns): 434.9 MB at N = 2160, 31 jobs and the default 768."""
+    nelim, k, total, steps = n - b, 0, 0.0, 0
+    while k < nelim:
+        k2 = k + 64
+        if min_rest > 0 and k2 + 64 < nelim and n - k2 - 64 >= min_rest:
+            total, k, steps = total + (n - k2 - 64) ** 2 * BYTES_PER_ENTRY_PAIR * jobs, k + 128, steps + 2
+        else:
+            total, k, steps = total + max(0, n - k - 64) ** 2 * BYTES_PER_ENTRY_SINGLE * jobs, k + 64, steps + 1
+    return total / steps
 
 
 def algorithmic_flops(N: int, b: int, L: int) -> float:
@@ -299,11 +312,11 @@ def run_comparators(args, local):
 def run_workload(args, world, rank, local):
     """The other configurations of the benchmark's table, one JSON line each (not the headline):
     one step = every job of the configuration in one batched call."""
-    line = workload_line(args.workload, args.steps, args.warmup, world, rank, local)
+    line = workload_line(args.workload, args.steps, args.warmup, world, rank, local, args.autotune_by_size)
     print(json.dumps(line))
 
 
-def workload_line(kind, steps, warmup, world, rank, local):
+def workload_line(kind, steps, warmup, world, rank, local, autotune=False):
     import torch
     from lsms_b200 import tau as T
     from lsms_b200 import workloads as W
@@ -363,6 +376,13 @@ def workload_line(kind, steps, warmup, world, rank, local):
     res = {}
     fallbacks = 0
     phases = {}
+    tune = None
+    if autotune:
+        # untimed: the paired-steps threshold per size bucket, timed on a sample of each bucket's jobs
+        mixed_default_ms = timed(lambda: s.solve_jobs_device(jobs, out.data_ptr(), T.PREC_MIXED))
+        table = s.autotune_paired_steps_by_size(jobs)
+        tune = {"paired_steps_min_rest_by_n": {str(k): v[0] for k, v in table.items()},
+                "mixed_at_default_768": {"value": nj / (mixed_default_ms * 1e-3), "ms_per_step": mixed_default_ms}}
     for name, prec in (("fp64", T.PREC_FP64), ("mixed", T.PREC_MIXED)):
         ms = timed(lambda: s.solve_jobs_device(jobs, out.data_ptr(), prec))
         s.sync()
@@ -388,7 +408,8 @@ def workload_line(kind, steps, warmup, world, rank, local):
                  "err_mixed_vs_fp64_on_tau00_l": err,
                  "mixed_jobs_resolved_in_fp64": fallbacks,
                  "phase_ms_per_step": phases,
-                 "algorithmic_flops_per_step": flops})
+                 "algorithmic_flops_per_step": flops,
+                 "autotune": tune or "off (paired-steps threshold 768)"})
     s.close()
     return line
 
@@ -409,6 +430,12 @@ def main():
     ap.add_argument("--no-graphs", action="store_true",
                     help="launch each wave's kernels one by one instead of replaying its CUDA graph "
                          "(for profilers, which do not see into graphs with conditional nodes)")
+    ap.add_argument("--no-autotune", action="store_true",
+                    help="keep the default paired-steps threshold instead of timing the candidates "
+                         "on the headline workload before the warm-up")
+    ap.add_argument("--autotune-by-size", action="store_true",
+                    help="batched / non-collinear lines: tune the threshold per size bucket on a "
+                         "64-job sample of each before timing (off: the default threshold)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = dist_setup()
@@ -446,6 +473,11 @@ def main():
     if args.no_graphs:
         s.set_graphs(False)
     jobs = T.make_jobs([(0, i, 0, prob.energies[i]) for i in range(ne)])
+    # untimed: the paired-steps threshold that is fastest on this workload becomes the setting
+    tune = None
+    if not args.no_autotune:
+        chosen, tune_ms = s.autotune_paired_steps(jobs, reps=2)
+        tune = {"paired_steps_min_rest": chosen, "ms_per_candidate": tune_ms}
     out = torch.empty(ne * b * b * 2, dtype=torch.float64, device=f"cuda:{local}")
     stream = torch.cuda.ExternalStream(s.stream, device=f"cuda:{local}")
 
@@ -562,9 +594,9 @@ def main():
     if rank == 0 and world == 1 and not args.no_extras:
         extras["cusolver_zgesv"] = cusolver_comparator(s, prob, ne, local)
         for kind in ("batched", "noncollinear"):
-            wlne = workload_line(kind, 1, 1, world, rank, local)
+            wlne = workload_line(kind, 1, 1, world, rank, local, args.autotune_by_size)
             extras[kind] = {k: wlne[k] for k in ("config", "value", "fp64", "mixed", "err_mixed_vs_fp64_on_tau00_l",
-                                                 "mixed_jobs_resolved_in_fp64", "phase_ms_per_step")}
+                                                 "mixed_jobs_resolved_in_fp64", "phase_ms_per_step", "autotune")}
 
     value = world * ne / (ms_mixed * 1e-3)
     fp64_value = world * ne / (ms_fp64 * 1e-3)
@@ -578,7 +610,8 @@ def main():
                        "solves_per_step": ne, "l2": "inputs larger than L2 "
                        f"({ne} x {N * N * 16 / 1e6:.0f} MB KKR matrices per step)",
                        "refinement_steps_mixed": "up to 10, per job until the correction estimate < 1e-12",
-                       "refinement_steps_fp64": 1},
+                       "refinement_steps_fp64": 1,
+                       "autotune": tune or "off (paired-steps threshold 768)"},
             "fp64": {"value": fp64_value, "unit": "solves/s", "ms_per_step": ms_fp64,
                      "mixed_over_fp64": value / fp64_value},
             "fp64_one_energy_per_call": {"value": world / (one_ms * 1e-3), "unit": "solves/s",
@@ -596,7 +629,8 @@ def main():
                          "achieved": achieved, "unit": "TFLOP/s",
                          "peak": tf32_peak, "frac": (achieved / tf32_peak) if achieved else None,
                          "executed_frac": (3.0 * achieved / tf32_peak) if achieved else None,
-                         "traffic": TRAFFIC_PER_LAUNCH, "traffic_unit": "bytes per elimination step",
+                         "traffic": update_traffic_per_step(N, b, ne, tune["paired_steps_min_rest"] if tune else 768),
+                         "traffic_unit": "bytes per elimination step",
                          "traffic_source": "ncu capture of the trailing-update kernel (dram__bytes_read.sum + "
                                            "dram__bytes_write.sum), scaled to this workload; not measured in "
                                            "this run",

@@ -257,6 +257,21 @@ int b200tau_set_graphs(b200tau_ctx *ctx, int enable);
  * it off; default 768.  No counterpart in the reference. */
 int b200tau_set_paired_steps(b200tau_ctx *ctx, int min_rest);
 
+/* Autotuner of that threshold for a workload: solves `jobs` (MIXED) with each candidate min_rest
+ * (NULL candidates: 0, 512, 768, 1024, 1280, 1536; at most 16), one untimed solve and then `reps`
+ * timed ones (1..16) per candidate, each timed on the context's stream from the first launch to
+ * the last of the call, and keeps the candidate with the fastest of its timed solves for the jobs'
+ * size bucket (their largest N rounded up to 64): later waves whose largest N falls in that bucket
+ * use it, other sizes keep b200tau_set_paired_steps' value (which also clears every tuned bucket).
+ * The threshold in force for the bucket before the call stays unless a candidate is at least 2%
+ * faster than it.  The choice goes to *chosen (if non-NULL) and the per-candidate ms (fastest
+ * timed solve) to ms_out[ncand] (if non-NULL).  Outputs of the solves are discarded.  On an error
+ * nothing is recorded.  No counterpart in the reference, whose tuning knob is the block size of
+ * its block LU (zblockLUSize, calculateTauMatrix.cpp:726-736). */
+int b200tau_autotune_paired_steps(b200tau_ctx *ctx, const b200tau_job *jobs, int njobs,
+                                  const int *candidates, int ncand, int reps, int *chosen,
+                                  float *ms_out);
+
 /* Row pivoting of the block elimination (B200TAU_PIVOT_*), both precisions.  BLOCK pivots inside
  * each 64 x 64 diagonal block, as the reference's GPU solver inverts its diagonal blocks
  * (zblock_lu_cuda_c.cu:218-259).  PANEL picks each 64-column step's rows from the whole

@@ -152,6 +152,10 @@ struct b200tau_ctx {
   std::vector<WaveGraph> wg;      // captured wave pipelines, most recently used last
   bool graphs_on = true;          // b200tau_set_graphs
   int pair_min_rest = kPairMinRest;  // b200tau_set_paired_steps
+  // (N rounded up to 64, min_rest) from b200tau_autotune_paired_steps: a wave whose largest N
+  // falls in a tuned bucket uses that bucket's threshold; the autotuner's trials set pair_trial
+  std::vector<std::pair<int, int>> pair_table;
+  int pair_trial = -1;
   // b200tau_set_keep_factors: the last FP64 solve's wave (factors F, KKR matrix M, refined X, slots
   // in `kept_order` order), reusable once by b200tau_solve_vjp on the same jobs
   bool keep_factors = false;
@@ -828,6 +832,16 @@ struct AdjointBufs {
   const long *site_off;    // host: first output block of each job
 };
 
+// The paired-steps threshold of a wave whose largest N is max_N: the autotuner's trial value while
+// it runs, else the tuned value of max_N's 64-bucket, else the context's setting.
+int pair_min_rest_for(const b200tau_ctx *ctx, int max_N) {
+  if (ctx->pair_trial >= 0) return ctx->pair_trial;
+  const int bucket = round_up(max_N, 64);
+  for (const auto &e : ctx->pair_table)
+    if (e.first == bucket) return e.second;
+  return ctx->pair_min_rest;
+}
+
 int run_wave(b200tau_ctx *ctx, const b200tau_job *jobs, const int *idx, int nw, int ld, const Plan &p,
              double2 *out_base, const AdjointBufs *adj = nullptr, bool reuse_factors = false) {
   std::vector<JobDev> h(nw);
@@ -878,7 +892,7 @@ int run_wave(b200tau_ctx *ctx, const b200tau_job *jobs, const int *idx, int nw, 
   }
   ctx->la.min_n = maxn;
   for (int w = 0; w < nw; ++w) ctx->la.min_n = std::min(ctx->la.min_n, h[w].n);
-  ctx->la.pair_min_rest = ctx->pair_min_rest;
+  ctx->la.pair_min_rest = pair_min_rest_for(ctx, maxN);
   CK(cudaMemcpyAsync(ctx->d_jobs, h.data(), sizeof(JobDev) * nw, cudaMemcpyHostToDevice, ctx->stream));
   if (reuse_factors) {
     // the forward solve of these jobs left M, its FP64 block factors and the refined X in these
@@ -1232,6 +1246,7 @@ int b200tau_set_paired_steps(b200tau_ctx *ctx, int min_rest) {
   if (!ctx) return B200TAU_ERR_ARG;
   if (min_rest < 0) return fail(ctx, B200TAU_ERR_ARG, "paired steps: min_rest must be >= 0");
   ctx->pair_min_rest = min_rest;
+  ctx->pair_table.clear();
   return B200TAU_OK;
 }
 
@@ -1442,6 +1457,88 @@ int b200tau_sync(b200tau_ctx *ctx) {
     return rc;
   }
   return check_host_info(ctx);
+}
+
+namespace {
+struct EventPair {
+  cudaEvent_t a = nullptr, b = nullptr;
+  ~EventPair() {
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+  }
+};
+}  // namespace
+
+int b200tau_autotune_paired_steps(b200tau_ctx *ctx, const b200tau_job *jobs, int njobs,
+                                  const int *candidates, int ncand, int reps, int *chosen,
+                                  float *ms_out) {
+  if (!ctx) return B200TAU_ERR_ARG;
+  static const int kDefault[] = {0, 512, 768, 1024, 1280, 1536};
+  if (!candidates) {
+    candidates = kDefault;
+    ncand = (int)(sizeof(kDefault) / sizeof(kDefault[0]));
+  }
+  if (njobs <= 0 || !jobs || ncand < 1 || ncand > 16 || reps < 1 || reps > 16)
+    return fail(ctx, B200TAU_ERR_ARG, "autotune: bad arguments");
+  for (int c = 0; c < ncand; ++c)
+    if (candidates[c] < 0) return fail(ctx, B200TAU_ERR_ARG, "autotune: candidate %d is negative", c);
+  int rc = check_prec(ctx, B200TAU_PREC_MIXED);
+  if (rc) return rc;
+  CK(cudaSetDevice(ctx->device));
+  const size_t outn = (size_t)njobs * ctx->b * ctx->b;
+  if ((rc = ensure_out(ctx, outn))) return rc;
+  EventPair ev;
+  CK(cudaEventCreate(&ev.a));
+  CK(cudaEventCreate(&ev.b));
+  int maxN = 0;
+  for (int j = 0; j < njobs; ++j)
+    if (jobs[j].atom >= 0 && jobs[j].atom < (int)ctx->atoms.size()) maxN = std::max(maxN, ctx->atoms[jobs[j].atom].N);
+  const int incumbent = pair_min_rest_for(ctx, maxN);
+  float incumbent_ms = -1.0f;
+  struct TrialReset {
+    b200tau_ctx *c;
+    ~TrialReset() { c->pair_trial = -1; }
+  } trial_reset{ctx};
+  int best = -1;
+  float best_ms = 0.0f;
+  for (int c = 0; c < ncand; ++c) {
+    ctx->pair_trial = candidates[c];
+    float cand_ms = 0.0f;
+    // one untimed solve (a new threshold is a new wave graph: its capture is not timed), then the
+    // fastest of `reps` timed ones
+    for (int r = 0; r <= reps; ++r) {
+      CK(cudaEventRecord(ev.a, ctx->stream));
+      rc = solve_impl(ctx, jobs, njobs, B200TAU_PREC_MIXED, ctx->d_out);
+      if (!rc) {
+        const cudaError_t e = cudaEventRecord(ev.b, ctx->stream);
+        if (e != cudaSuccess) rc = fail(ctx, B200TAU_ERR_CUDA, "autotune: %s", cudaGetErrorString(e));
+      }
+      if (!rc) rc = b200tau_sync(ctx);
+      if (rc) return rc;
+      float ms = 0.0f;
+      CK(cudaEventElapsedTime(&ms, ev.a, ev.b));
+      if (r > 0 && (r == 1 || ms < cand_ms)) cand_ms = ms;
+    }
+    if (ms_out) ms_out[c] = cand_ms;
+    if (candidates[c] == incumbent) incumbent_ms = cand_ms;
+    if (c == 0 || cand_ms < best_ms) {
+      best_ms = cand_ms;
+      best = candidates[c];
+    }
+  }
+  ctx->pair_trial = -1;
+  // run-to-run noise of a solve is a few per cent: the setting in force stays unless beaten by 2%
+  if (incumbent_ms >= 0.0f && best_ms > 0.98f * incumbent_ms) best = incumbent;
+  const int bucket = round_up(maxN, 64);
+  bool found = false;
+  for (auto &e : ctx->pair_table)
+    if (e.first == bucket) {
+      e.second = best;
+      found = true;
+    }
+  if (!found) ctx->pair_table.emplace_back(bucket, best);
+  if (chosen) *chosen = best;
+  return B200TAU_OK;
 }
 
 int b200tau_solve_dense(b200tau_ctx *ctx, const double *m, int n, int ldm, const double *t0, int b,

@@ -55,6 +55,7 @@ EXPORTS = (
     "b200tau_last_fallback_count", "b200tau_set_mixed_fallback", "b200tau_set_build_wait",
     "b200tau_set_pivoting", "b200tau_solve_tau_full", "b200tau_set_graphs",
     "b200tau_set_keep_factors", "b200tau_set_paired_steps",
+    "b200tau_autotune_paired_steps",
 )
 
 
@@ -115,6 +116,7 @@ def load_library():
     lib.b200tau_solve_tau_full.argtypes = [P, P, P, I]
     lib.b200tau_set_graphs.argtypes = [P, I]
     lib.b200tau_set_paired_steps.argtypes = [P, I]
+    lib.b200tau_autotune_paired_steps.argtypes = [P, P, I, P, I, I, P, P]
     lib.b200tau_set_keep_factors.argtypes = [P, I]
     _lib = lib
     return lib
@@ -160,6 +162,7 @@ class TauSolver:
         self.lmax, self.n_spin_cant, self.n_spin_pola = lmax, n_spin_cant, n_spin_pola
         self.kkrsz = (lmax + 1) ** 2
         self.kkrsz_ns = n_spin_cant * self.kkrsz
+        self.atom_n = {}  # atom index -> N of its KKR matrix (from set_atom)
 
     # -- plumbing -------------------------------------------------------------------------
     def close(self):
@@ -215,6 +218,32 @@ class TauSolver:
         trailing block has at least min_rest columns; 0 turns them off (default 768)."""
         self._check(self.lib.b200tau_set_paired_steps(self.ctx, int(min_rest)))
 
+    def autotune_paired_steps(self, jobs, candidates=None, reps: int = 2):
+        """Time mixed solves of `jobs` at each paired-steps threshold (default 0, 512, 768, 1024,
+        1280, 1536), keep the fastest as the setting; returns (chosen, {candidate: ms})."""
+        cand = [0, 512, 768, 1024, 1280, 1536] if candidates is None else [int(c) for c in candidates]
+        ca = np.ascontiguousarray(cand, np.int32)
+        ms = np.zeros(len(cand), np.float32)
+        chosen = ctypes.c_int()
+        self._check(self.lib.b200tau_autotune_paired_steps(self.ctx, ctypes.cast(jobs, ctypes.c_void_p), len(jobs),
+                                                           _ptr(ca), len(cand), int(reps),
+                                                           ctypes.byref(chosen), _ptr(ms)))
+        return chosen.value, {c: float(t) for c, t in zip(cand, ms)}
+
+    def autotune_paired_steps_by_size(self, jobs, sample: int = 64, candidates=(0, 768, 1280), reps: int = 2):
+        """Tune the paired-steps threshold per size bucket (N rounded up to 64) of a mixed batch:
+        for each bucket, autotune_paired_steps on up to `sample` of its jobs; waves whose largest N
+        falls in a tuned bucket then use its threshold.  Returns {bucket: (chosen, {candidate: ms})}."""
+        buckets = {}
+        for j in jobs:
+            n = self.atom_n[j.atom]
+            buckets.setdefault((n + 63) // 64 * 64, []).append(j)
+        table = {}
+        for bucket in sorted(buckets, reverse=True):
+            sub = buckets[bucket][:sample]
+            table[bucket] = self.autotune_paired_steps((Job * len(sub))(*sub), candidates, reps)
+        return table
+
     def set_pivoting(self, mode: int):
         """Row pivoting of the elimination: PIVOT_AUTO (default), PIVOT_BLOCK or PIVOT_PANEL."""
         self._check(self.lib.b200tau_set_pivoting(self.ctx, mode))
@@ -259,6 +288,7 @@ class TauSolver:
         self._check(self.lib.b200tau_set_atom(self.ctx, atom, pos.shape[0], _ptr(pos), _ptr(lm), _ptr(si),
                                               None if u is None else _ptr(u),
                                               None if ud is None else _ptr(ud)))
+        self.atom_n[atom] = self.n_spin_cant * int(sum((int(l) + 1) ** 2 for l in lm))
 
     def load_problem(self, prob: workloads.Problem, atom: int = 0, upload_tmat: bool = True):
         if upload_tmat:

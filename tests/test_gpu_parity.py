@@ -402,3 +402,54 @@ def test_paired_steps_match_reference(solver_factory, ref, min_rest):
     finally:
         s.set_paired_steps(768)
         s.set_graphs(True)
+
+
+def test_autotune_paired_steps(solver_factory, ref):
+    """The paired-steps autotuner times each candidate threshold on the caller's jobs, keeps the
+    fastest, and the solves that follow at that setting still match the reference; bad candidates
+    are refused without touching the setting."""
+    prob = W.config_n2160(npts=8)
+    s = _solver(solver_factory, prob)
+    jobs = T.make_jobs([(0, i, 0, prob.energies[i]) for i in range(8)])
+    try:
+        with pytest.raises(T.B200TauError):
+            s.autotune_paired_steps(jobs, candidates=[768, -1])
+        chosen, ms = s.autotune_paired_steps(jobs, candidates=[0, 768, 1400], reps=1)
+        assert chosen in ms and all(t > 0 for t in ms.values())
+        fastest = min(ms, key=ms.get)
+        # the setting in force (768) stays unless beaten by 2%
+        assert chosen == (fastest if ms[fastest] <= 0.98 * ms[768] else 768)
+        mixed = s.solve_jobs(jobs, T.PREC_MIXED)
+        assert s.last_fallback_count == 0
+        for i in range(8):
+            want = ref.calculate_tau(prob, i, 0, ref.ZBLOCKLU_CPP)
+            assert tau_err(prob, i, 0, mixed[i], want) <= TOL_MIXED
+    finally:
+        s.set_paired_steps(768)
+
+
+def test_autotuned_threshold_applies_to_its_size_bucket(solver_factory):
+    """The tuned threshold is recorded for the jobs' size bucket and used by later waves of that
+    size (seen in the number of trailing-update passes the profiler times: paired steps update the
+    trailing block once for two steps); b200tau_set_paired_steps clears it."""
+    prob = W.config_n2160(npts=4)
+    s = _solver(solver_factory, prob)
+    jobs = T.make_jobs([(0, i, 0, prob.energies[i]) for i in range(4)])
+    try:
+        def launches(min_rest=None):
+            if min_rest is not None:
+                s.set_paired_steps(min_rest)
+            s.set_profiling(True)
+            s.solve_jobs(jobs, T.PREC_MIXED)
+            n = s.profile_read()[1]
+            s.set_profiling(False)
+            return n
+        n_off, n_on = launches(0), launches(768)
+        assert n_off != n_on
+        chosen, _ = s.autotune_paired_steps(jobs, candidates=[0], reps=1)
+        assert chosen == 0
+        assert launches() == n_off
+        assert launches(768) == n_on
+    finally:
+        s.set_profiling(False)
+        s.set_paired_steps(768)
