@@ -569,13 +569,19 @@ def main():
     for i in range(ne):
         s.solve_jobs_device(one[i], out.data_ptr(), T.PREC_FP64)
     s.sync()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for i in range(ne):
-        s.solve_jobs_device(one[i], out.data_ptr() + 16 * b * b * i, T.PREC_FP64)
-    e1.record(stream)
-    s.sync()
-    one_ms = max_over_ranks(e0.elapsed_time(e1) / ne)
+    # the fastest of three windows of ne host-enqueued calls (a host stall while enqueuing idles
+    # the device and would otherwise land in the figure)
+    one_ms = None
+    for _ in range(3):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for i in range(ne):
+            s.solve_jobs_device(one[i], out.data_ptr() + 16 * b * b * i, T.PREC_FP64)
+        e1.record(stream)
+        s.sync()
+        w_ms = e0.elapsed_time(e1) / ne
+        one_ms = w_ms if one_ms is None else min(one_ms, w_ms)
+    one_ms = max_over_ranks(one_ms)
 
     cpu, ref_outs = None, []
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -617,7 +623,8 @@ def main():
             "fp64_one_energy_per_call": {"value": world / (one_ms * 1e-3), "unit": "solves/s",
                                          "ms_per_solve": one_ms,
                                          "note": "the reference's calling pattern: one b200tau call per "
-                                                 "(atom, energy), FP64, inputs resident"},
+                                                 "(atom, energy), FP64, inputs resident; fastest of three "
+                                                 "windows of the 31 calls"},
             "err_mixed_vs_fp64": err,
             "err_vs_reference": err_ref,
             "phase_ms_per_step_mixed": phases,

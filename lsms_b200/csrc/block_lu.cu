@@ -55,6 +55,14 @@ template <> struct Vec2<float> { using t = float2; };
 // the step, in every warp the lane holding row pv publishes u over the warp's columns (a per-warp
 // slot in shared memory, read only by that warp) and all lanes apply the update.
 // ---------------------------------------------------------------------------------------------
+// Pivot search key of a row: |re| + |im| (non-negative doubles order as their bit patterns; NaN
+// counts as 0) with its 6 low mantissa bits replaced by 63 - row, so that the largest key is the
+// largest value, ties - and values within 2^-46 relative of each other - going to the lowest row.
+__device__ __forceinline__ unsigned long long pivot_key(double v, int row) {
+  v = (v == v) ? v : 0.0;
+  return ((unsigned long long)__double_as_longlong(v) & ~63ull) | (unsigned long long)(63 - row);
+}
+
 constexpr int kDiagThreads = 256;
 constexpr int kDiagWarps = kDiagThreads / 32;
 static_assert(kDiagWarps * 8 == kNb && kNb == 64, "diagonal inverse layout: 8 columns per warp, 2 rows per lane");
@@ -71,10 +79,8 @@ __global__ void __launch_bounds__(kDiagThreads, PER_SM) diag_inverse_kernel(cons
   const int kb = min(NB, J.n - k);
   extern __shared__ __align__(16) double2 dyn_smem[];
   double2(*As)[NB + 1] = reinterpret_cast<double2(*)[NB + 1]>(dyn_smem);  // staging As[row][col]
-  __shared__ double2 s_f[NB];                 // column p before the step (the pivot warp's scratch)
   __shared__ double2 s_g[2][NB];              // the step's row factors g, by step parity
   __shared__ double2 s_row[kDiagWarps][8];    // per warp: u over the warp's columns
-  __shared__ double2 s_dinv;                  // 1 / d (the pivot warp's scratch)
   __shared__ int s_pvp[2];
   __shared__ int s_sing[2];
   __shared__ int s_pv[NB], s_inv[NB];
@@ -114,55 +120,34 @@ __global__ void __launch_bounds__(kDiagThreads, PER_SM) diag_inverse_kernel(cons
           x1 = t1;
         }
       }
-      s_f[l] = x0;
-      s_f[l + 32] = x1;
-      // this lane's candidate: the first unused row until a larger one is seen, so that a NaN
-      // column still yields an unused row in range (NaN compares false)
-      double best = -1.0;
-      int bi = NB;
-      if (!used0) {
-        best = cabs1(x0);
-        bi = l;
+      // the pivot: the unused row of largest |re| + |im| as the largest 64-bit key (pivot_key),
+      // two warp max-reductions (high word, then the low word among the lanes holding the high max)
+      const unsigned long long k0 = used0 ? 0ull : pivot_key(cabs1(x0), l);
+      const unsigned long long k1 = used1 ? 0ull : pivot_key(cabs1(x1), l + 32);
+      const unsigned long long kl = k0 > k1 ? k0 : k1;
+      const unsigned hi = (unsigned)(kl >> 32);
+      const unsigned mhi = __reduce_max_sync(0xffffffffu, hi);
+      const unsigned mlo = __reduce_max_sync(0xffffffffu, hi == mhi ? (unsigned)kl : 0u);
+      // kb - p unused rows remain, so the key names one of them (a row < kb)
+      const int pv = min(63 - (int)(mlo & 63u), kb - 1);
+      const double2 xs = (pv >> 5) ? x1 : x0;
+      double2 d;
+      d.x = __shfl_sync(0xffffffffu, xs.x, pv & 31);
+      d.y = __shfl_sync(0xffffffffu, xs.y, pv & 31);
+      // 1/d = conj(d) / |d|^2 in every lane (pivots of these blocks are far from the FP64 range limits)
+      const bool zero = d.x == 0.0 && d.y == 0.0;
+      double2 dinv = make_double2(0.0, 0.0);
+      if (!zero) {
+        const double rr = 1.0 / (d.x * d.x + d.y * d.y);
+        dinv = make_double2(d.x * rr, -d.y * rr);
       }
-      if (!used1) {
-        const double v = cabs1(x1);
-        if (bi == NB || v > best) {
-          best = v;
-          bi = l + 32;
-        }
-      }
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-        const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-        if (oi != NB && (bi == NB || ob > best || (ob == best && oi < bi))) {
-          best = ob;
-          bi = oi;
-        }
-      }
-      // lane 0's result for all (the lanes agree unless the column holds NaNs); kb - p unused
-      // rows remain, so it is a row < kb
-      const int pv = min(__shfl_sync(0xffffffffu, bi, 0), kb - 1);
-      __syncwarp();
-      if (l == 0) {  // 1/d = conj(d) / |d|^2 (pivots of these blocks are far from the FP64 range limits)
-        const double2 d = s_f[pv];
-        const bool zero = d.x == 0.0 && d.y == 0.0;
-        double2 dinv = make_double2(0.0, 0.0);
-        if (!zero) {
-          const double rr = 1.0 / (d.x * d.x + d.y * d.y);
-          dinv = make_double2(d.x * rr, -d.y * rr);
-        }
-        s_dinv = dinv;
+      s_g[par][l] = (l == pv) ? make_double2(1.0 - dinv.x, -dinv.y) : cmul(x0, dinv);
+      s_g[par][l + 32] = (l + 32 == pv) ? make_double2(1.0 - dinv.x, -dinv.y) : cmul(x1, dinv);
+      if (l == 0) {
         s_pvp[par] = pv;
         s_sing[par] = zero ? 1 : 0;
         s_pv[p] = pv;
       }
-      __syncwarp();
-      // the column is read back from shared memory: keeping it live across the reduction costs
-      // registers the update needs
-      const double2 dinv = s_dinv;
-      s_g[par][l] = (l == pv) ? make_double2(1.0 - dinv.x, -dinv.y) : cmul(s_f[l], dinv);
-      s_g[par][l + 32] = (l + 32 == pv) ? make_double2(1.0 - dinv.x, -dinv.y) : cmul(s_f[l + 32], dinv);
     }
     __syncthreads();
     const int pv = s_pvp[par];
