@@ -382,6 +382,17 @@ __global__ void __launch_bounds__(256, 2) zgemm_tile_kernel(const JobDev *__rest
 }
 
 
+// Step k's update of the two strips a paired step k2 = k + 64 needs before its own W (block
+// pivoting): block column k2 below its diagonal block (CTAs x < t1: row tiles 1 .. t1) and block
+// row k2 right of it (x >= t1: column tiles 1 .. t1), one grid of 2 t1 x njobs CTAs, so that the
+// last wave of one strip shares the GPU with the other.
+template <typename S>
+__global__ void __launch_bounds__(256, 2) zgemm_strips_kernel(const JobDev *__restrict__ jobs, int k, int t1) {
+  const int x = blockIdx.x;
+  if (x < t1) zgemm_tile_body<S, kSubtract>(jobs[blockIdx.z], k, 0, x, 0, 1);
+  else zgemm_tile_body<S, kSubtract>(jobs[blockIdx.z], k, x - t1, 0, 1, 0);
+}
+
 // out = tau00 (out_mode 1) or rotate(tau00 - t0) (out_mode 0), tau00 in A[r][b + c].
 __device__ void write_out(const JobDev &J, double2 (*A)[2 * kMaxB + 1], int ns, int kkrsz) {
   const int tid = threadIdx.x;
@@ -778,12 +789,7 @@ cudaError_t eliminate_lookahead(const JobDev *jobs, int njobs, int max_n, int ma
       if ((e = cudaStreamWaitEvent(la.s2, la.panel, 0)) != cudaSuccess) return e;
       launch_diag_inverse<T>(false, jobs, njobs, k2, info, smem_diag, la.s2);
       if ((e = cudaEventRecord(la.diag, la.s2)) != cudaSuccess) return e;
-      if (tiles > 1) {
-        zgemm_tile_kernel<S, kSubtract><<<dim3(1, tiles - 1, njobs), 256, smem_gemm, s>>>(jobs, k, 1, tiles - 1, njobs,
-                                                                                         PackB(), 0, 1);
-        zgemm_tile_kernel<S, kSubtract><<<dim3(tiles - 1, 1, njobs), 256, smem_gemm, s>>>(jobs, k, tiles - 1, 1,
-                                                                                         njobs, PackB(), 1, 0);
-      }
+      if (tiles > 1) zgemm_strips_kernel<S><<<dim3(2 * (tiles - 1), 1, njobs), 256, smem_gemm, s>>>(jobs, k, tiles - 1);
       if ((e = cudaStreamWaitEvent(s, la.diag, 0)) != cudaSuccess) return e;
       PackB pk1;  // W(k2) -> K half 1
       pk1.hi = tc.b_hi;
@@ -808,8 +814,8 @@ cudaError_t eliminate_lookahead(const JobDev *jobs, int njobs, int max_n, int ma
       if (timed) cudaEventRecord(timer->ev[timer->used++], s);
       if (next2 && (e = cudaStreamWaitEvent(s, la.diag, 0)) != cudaSuccess) return e;
       // W(k), the diagonal block, its inverse, W(k2), the pack, the two update launches (+ the
-      // two strips, + the next inverse)
-      if (launches) *launches += 7 + (tiles > 1 ? 2 : 0) + (next2 ? 1 : 0);
+      // two strips in one launch, + the next inverse)
+      if (launches) *launches += 7 + (tiles > 1 ? 1 : 0) + (next2 ? 1 : 0);
       k = k2;  // the loop's increment moves past k2
       continue;
     }
@@ -873,6 +879,8 @@ cudaError_t eliminate_impl(const JobDev *jobs, int njobs, int max_n, int max_N, 
   if ((e = ensure_smem(zgemm_tile_kernel<S, kOverwrite>, smem_gemm)) != cudaSuccess)
     return e;
   if ((e = ensure_smem(zgemm_tile_kernel<S, kSubtract>, smem_gemm)) != cudaSuccess)
+    return e;
+  if ((e = ensure_smem(zgemm_strips_kernel<S>, smem_gemm)) != cudaSuccess)
     return e;
   // Look-ahead (tensor-core path): the update of step k first covers the tile holding the next
   // step's diagonal block; the next diagonal inverse then runs on the second stream while the other
