@@ -60,3 +60,23 @@ def test_no_gpu_means_error_not_fallback():
         pytest.skip("a GPU is present")
     with pytest.raises(tau.B200TauError):
         tau.TauSolver()
+
+
+def test_autotune_by_size_groups_jobs_per_bucket(monkeypatch):
+    """TauSolver.autotune_paired_steps_by_size (host logic only; the timed library call is
+    replaced): jobs go to the bucket of their atom's N rounded up to 64, each bucket is tuned on
+    at most `sample` of its jobs in their order, the largest bucket first."""
+    s = object.__new__(tau.TauSolver)
+    s.atom_n = {0: 2160, 1: 2144, 2: 688, 3: 700}
+    seen = []
+
+    def fake(jobs, candidates=None, reps=2):
+        seen.append([(j.atom, j.iie) for j in jobs])
+        return 768, {c: 1.0 for c in candidates}
+    monkeypatch.setattr(s, "autotune_paired_steps", fake, raising=False)
+    specs = [(a, i, 0, 0.5 + 0.1j) for i in range(5) for a in (0, 1, 2, 3)]
+    table = s.autotune_paired_steps_by_size(tau.make_jobs(specs), sample=3)
+    assert list(table) == [2176, 704]
+    assert seen[0] == [(0, 0), (1, 0), (0, 1)]   # N 2160 and 2144 share the 2176 bucket
+    assert seen[1] == [(2, 0), (3, 0), (2, 1)]   # N 688 and 700 share 704
+    assert all(v[0] == 768 for v in table.values())
