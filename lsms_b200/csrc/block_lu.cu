@@ -86,9 +86,26 @@ __global__ void __launch_bounds__(kDiagThreads, PER_SM) diag_inverse_kernel(cons
   __shared__ int s_pv[NB], s_inv[NB];
   T *__restrict__ Fk = static_cast<T *>(J.F) + (size_t)k + (size_t)k * J.ld;
   const int tid = threadIdx.x;
-  for (int e = tid; e < kb * kb; e += kDiagThreads) {
-    const int cc = e / kb, r = e - cc * kb;
-    As[r][cc] = ldc(Fk + r + (size_t)cc * J.ld);
+  constexpr int kPer = NB * NB / kDiagThreads;  // entries per thread of a full block
+  if (kb == NB) {
+    // all of a thread's loads in flight at once (a loop over them waits out one DRAM round trip
+    // per entry)
+    double2 v[kPer];
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+      const int e = tid + i * kDiagThreads;
+      v[i] = ldc(Fk + (e % NB) + (size_t)(e / NB) * J.ld);
+    }
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+      const int e = tid + i * kDiagThreads;
+      As[e % NB][e / NB] = v[i];
+    }
+  } else {
+    for (int e = tid; e < kb * kb; e += kDiagThreads) {
+      const int cc = e / kb, r = e - cc * kb;
+      As[r][cc] = ldc(Fk + r + (size_t)cc * J.ld);
+    }
   }
   if (tid < NB) s_inv[tid] = tid;  // every entry in range whatever the pivots
   __syncthreads();
@@ -189,9 +206,17 @@ __global__ void __launch_bounds__(kDiagThreads, PER_SM) diag_inverse_kernel(cons
       if (r < kb && c < kb) As[s_inv[r]][s_pv[c]] = a[i][j];
     }
   __syncthreads();
-  for (int e = tid; e < kb * kb; e += kDiagThreads) {
-    const int cc = e / kb, r = e - cc * kb;
-    stc(Fk + r + (size_t)cc * J.ld, As[r][cc]);
+  if (kb == NB) {
+#pragma unroll
+    for (int i = 0; i < kPer; ++i) {
+      const int e = tid + i * kDiagThreads;
+      stc(Fk + (e % NB) + (size_t)(e / NB) * J.ld, As[e % NB][e / NB]);
+    }
+  } else {
+    for (int e = tid; e < kb * kb; e += kDiagThreads) {
+      const int cc = e / kb, r = e - cc * kb;
+      stc(Fk + r + (size_t)cc * J.ld, As[r][cc]);
+    }
   }
   if (singular && tid == 0) atomicCAS(&info[blockIdx.x], 0, k + 1);
 }
