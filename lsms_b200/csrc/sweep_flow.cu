@@ -63,6 +63,8 @@ constexpr unsigned kUnitBytes = kUnitFloats * 4;
 constexpr int kBoxFloats = 32 * kUnit;     // one TMA box: 32 real rows x 32 columns
 constexpr int kStages = 3;                 // operand ring depth (units)
 constexpr int kTileElems = 64 * kCols;     // one 64-row tile of the right-hand side (float2)
+constexpr int kPerThread = kTileElems / kThreads;  // a tile's entries per compute thread
+static_assert(kTileElems % kThreads == 0, "tile entries spread evenly over the compute threads");
 constexpr int kBFloats = 64 * 64;          // B operand of a 64-row block: N = 64 rows x K = 64
 constexpr int kAccCols = 64;               // TMEM columns per accumulator (two of them)
 constexpr int kMaxSmem = 227 * 1024;
@@ -572,11 +574,14 @@ __global__ void __launch_bounds__(kBlock, 1)
   if (tid < kThreads)
     for (int i = 0; q + i * cs < T; ++i) {
       const int t = q + i * cs;
-      for (int e = tid; e < kTileElems; e += kThreads) {
-        const int c = e >> 6, rr = e & 63, gr = 64 * t + rr;
-        S.tiles[i * kTileElems + e] = (c < b && gr < N) ? to_v<float2>(__ldcg(Rb + (size_t)gr + (size_t)c * ld))
-                                                        : make_float2(0.f, 0.f);
+      float2 v[kPerThread];  // a tile's loads in flight together, then its stores
+#pragma unroll
+      for (int j = 0; j < kPerThread; ++j) {
+        const int e = tid + j * kThreads, c = e >> 6, rr = e & 63, gr = 64 * t + rr;
+        v[j] = (c < b && gr < N) ? to_v<float2>(__ldcg(Rb + (size_t)gr + (size_t)c * ld)) : make_float2(0.f, 0.f);
       }
+#pragma unroll
+      for (int j = 0; j < kPerThread; ++j) S.tiles[i * kTileElems + tid + j * kThreads] = v[j];
     }
   cluster_sync();  // barriers and tensor memory set up in every CTA before any remote arrival or store
   um::fence_after();
@@ -709,11 +714,14 @@ __global__ void __launch_bounds__(kBlock, 1)
     // own tiles of Y (rows < n) in FP32
     for (int i = 0; q + i * cs < Tn; ++i) {
       const int t = q + i * cs;
-      for (int e = tid; e < kTileElems; e += kThreads) {
-        const int c = e >> 6, gr = 64 * t + (e & 63);
-        S.tiles[i * kTileElems + e] = (c < b && gr < n) ? to_v<float2>(__ldcg(Yb + (size_t)gr + (size_t)c * ld))
-                                                        : make_float2(0.f, 0.f);
+      float2 v[kPerThread];  // a tile's loads in flight together, then its stores
+#pragma unroll
+      for (int j = 0; j < kPerThread; ++j) {
+        const int e = tid + j * kThreads, c = e >> 6, gr = 64 * t + (e & 63);
+        v[j] = (c < b && gr < n) ? to_v<float2>(__ldcg(Yb + (size_t)gr + (size_t)c * ld)) : make_float2(0.f, 0.f);
       }
+#pragma unroll
+      for (int j = 0; j < kPerThread; ++j) S.tiles[i * kTileElems + tid + j * kThreads] = v[j];
     }
     // step 0, the central block from the Schur solve: every CTA fills its own slot 0 (column-major)
     for (int e = tid; e < kTileElems; e += kThreads) {
@@ -790,32 +798,39 @@ __global__ void __launch_bounds__(kBlock, 1)
           if (!ok) break;
           const float4 *src = reinterpret_cast<const float4 *>(Yt);
           const float4 *dst = reinterpret_cast<const float4 *>(S.slots + slot * kTileElems);
+          float4 yv[2];
 #pragma unroll
           for (int i = 0; i < 2; ++i) {
             // float4 f: column c = f / 32, complex rows 2 (f % 32) and 2 (f % 32) + 1
-            const int f = tid + kThreads * i, c = f >> 5, r0 = 2 * (f & 31);
+            const int f = tid + kThreads * i, r0 = 2 * (f & 31);
             float4 y = src[f];
             if (r0 >= kbn) y.x = y.y = 0.f;
             if (r0 + 1 >= kbn) y.z = y.w = 0.f;
-            if (c < b) {
-#pragma unroll
-              for (int e = 0; e < 2; ++e) {
-                if (r0 + e >= kbn) continue;
-                const size_t idx = (size_t)(kn + r0 + e) + (size_t)c * ld;
-                const double2 yd = make_double2(e ? y.z : y.x, e ? y.w : y.y);
-                if (mode == 0) {
-                  Xb[idx] = yd;
-                } else {
-                  const double2 x = Xb[idx];
-                  Xb[idx] = make_double2(x.x + yd.x, x.y + yd.y);
-                }
-              }
-            }
+            yv[i] = y;
             for (int pc = 0; pc < cs; ++pc) st_remote(remote_u32(dst + f, pc), y);
           }
           __syncwarp();
           if ((tid & 31) == 0)
             for (int pc = 0; pc < cs; ++pc) mbar_arrive_cluster(S.full + slot, pc);
+          // X (+)= Y on the block's rows once the block is out: the read of X (mode 1) then
+          // stays off the chain of steps
+#pragma unroll
+          for (int i = 0; i < 2; ++i) {
+            const int f = tid + kThreads * i, c = f >> 5, r0 = 2 * (f & 31);
+            if (c >= b) continue;
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+              if (r0 + e >= kbn) continue;
+              const size_t idx = (size_t)(kn + r0 + e) + (size_t)c * ld;
+              const double2 yd = make_double2(e ? yv[i].z : yv[i].x, e ? yv[i].w : yv[i].y);
+              if (mode == 0) {
+                Xb[idx] = yd;
+              } else {
+                const double2 x = Xb[idx];
+                Xb[idx] = make_double2(x.x + yd.x, x.y + yd.y);
+              }
+            }
+          }
         }
       }
     }
