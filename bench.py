@@ -143,6 +143,23 @@ def dist_setup():
     return world, rank, local
 
 
+def rank_max(x, dist=None, device="cpu"):
+    """The largest of every rank's x (one all-reduce over the process group `dist`; x itself
+    without one): per-step times are reported as the slowest rank's."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank, world, ms_max):
+    """Units per second of the whole job: every rank processes units_per_rank (replicas over
+    independent atoms) in the slowest rank's ms_max."""
+    return world * units_per_rank / (ms_max * 1e-3)
+
+
 def measured_peaks():
     path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(path):
@@ -486,11 +503,7 @@ def main():
             pg.barrier()
 
     def max_over_ranks(x: float) -> float:
-        if pg is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        return float(t.item())
+        return rank_max(x, pg, f"cuda:{local}")
 
     def timed(prec, steps, warmup, sampler=None):
         cm = sampler if sampler is not None else _Null()
@@ -604,8 +617,8 @@ def main():
             extras[kind] = {k: wlne[k] for k in ("config", "value", "fp64", "mixed", "err_mixed_vs_fp64_on_tau00_l",
                                                  "mixed_jobs_resolved_in_fp64", "phase_ms_per_step", "autotune")}
 
-    value = world * ne / (ms_mixed * 1e-3)
-    fp64_value = world * ne / (ms_fp64 * 1e-3)
+    value = whole_job_rate(ne, world, ms_mixed)
+    fp64_value = whole_job_rate(ne, world, ms_fp64)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
